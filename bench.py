@@ -1,0 +1,412 @@
+#!/usr/bin/env python
+"""Triangle-count throughput (edges/s) of the B200 counting path.
+
+Workload: plain triangle count of a seeded RMAT graph, scale 22 (4,194,304
+vertices), edge factor 16, (a,b,c,d) = (0.57,0.19,0.19,0.05), symmetrised,
+deduplicated, self-loops dropped, int32 ids / int64 offsets (the
+graph.meta/vertex/edge layout).  One step = one pass of the counting path
+over the device-resident symmetric CSR: degree-ordered orientation, owner
+lists and task queues built on the device, then the counting kernels, then
+the uint64 count copied back.  value = undirected edges / step time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference path's CPU restatement (the oracle's
+orientation of graph.cc:196-235 plus the merge-intersection count) on the
+host cores, on a bounded hash-sampled fraction of the source vertices per
+step, extrapolated to the whole graph.  Under torchrun (N > 1) each rank
+holds the whole graph, counts its shard of the tasks and the partial counts
+are summed with an NCCL all-reduce; time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+LEAF_MAX_OUT = 64  # owners with d+ <= this go to the warp kernel (dgraph.cuh)
+
+
+def parse_args():
+    p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--scale", type=int, default=22)
+    p.add_argument("--edge-factor", type=int, default=16)
+    p.add_argument("--seed", type=int, default=1)
+    p.add_argument("--e2e-steps", type=int, default=5)
+    p.add_argument("--cpu-seconds", type=float, default=12.0,
+                   help="target CPU time of the bounded CPU-baseline sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def workload_config(a):
+    return {
+        "workload": f"plain TC, RMAT scale {a.scale} edge factor {a.edge_factor} "
+                    f"(0.57,0.19,0.19,0.05) seed {a.seed}, device orientation + count",
+        "scale": a.scale, "edge_factor": a.edge_factor, "seed": a.seed,
+        "l2": "no flush: inputs larger than L2 (symmetric CSR > 126 MB per step)",
+    }
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms in the background."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.3)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self, sm_max_default=None):
+        if self.proc is None or not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": sm_max_default, "reasons": ["unsampled"]}
+        rows = []
+        with open(self.path) as f:
+            for r in csv.reader(f):
+                if len(r) >= 9:
+                    rows.append([x.strip() for x in r])
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": sm_max_default, "reasons": ["unsampled"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        smax = [num(r[2]) for r in rows if num(r[2]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        top = max(sm) if sm else None
+        loaded = [s for s in sm if top and s >= 0.5 * top] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(smax) if smax else sm_max_default,
+                "samples": len(rows), "reasons": reasons}
+
+
+# ---------------------------------------------------------------- roofline
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_from_profile():
+    """DRAM bytes per launch of tc_hub_kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "tc_hub_kernel_rmat22.txt")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        for line in f:
+            if line.startswith("dram_bytes_per_launch"):
+                try:
+                    return float(line.split("=")[1].split()[0])
+                except (IndexError, ValueError):
+                    return None
+    return None
+
+
+def algorithmic_bytes(n, drp, dcol):
+    """Per-launch algorithmic bytes of the count phase and of the hub kernel.
+
+    Per unit (one DAG edge u->v): 12 B (its id plus the far row's offsets) +
+    4 B x (d+u + d+v) (both operand lists), plus 8 B per row offset -- the
+    edge-iterator merge volume.  The "min" variant streams only the shorter
+    list per edge (each owner's list read once into shared memory).
+    """
+    dplus = np.diff(drp).astype(np.int64)
+    src = np.repeat(np.arange(n, dtype=np.int64), dplus)
+    dst = dcol.astype(np.int64)
+    ds, dd = dplus[src], dplus[dst]
+    m = len(dcol)
+    b_tc = 8.0 * (n + 1) + 12.0 * m + 4.0 * float((ds + dd).sum())
+    valid = (ds >= 1) & (dd >= 1)
+    src_owns = (ds > dd) | ((ds == dd) & (src > dst))
+    owner_deg = np.where(src_owns, ds, dd)
+    hub = valid & (owner_deg > LEAF_MAX_OUT)
+    hub_owners = np.unique(np.where(src_owns, src, dst)[hub]).size
+    b_hub = 8.0 * hub_owners + 12.0 * float(hub.sum()) + 4.0 * float((ds + dd)[hub].sum())
+    b_min = 8.0 * (n + 1) + 20.0 * m + 4.0 * float(np.minimum(ds, dd).sum())
+    return {"b_tc": b_tc, "b_hub": b_hub, "b_min": b_min, "hub_edges": int(hub.sum()),
+            "merge_volume": float((ds + dd).sum())}
+
+
+# ---------------------------------------------------------------- CPU side
+def cpu_baseline(g, drp=None, dcol=None, target_s=12.0):
+    """Oracle on the host cores: orientation of the whole graph plus a count
+    over a hash-sampled 1/k of the sources, extrapolated by edges."""
+    from oracle import oracle as orc
+    rp, col = np.asarray(g.rowptr), np.asarray(g.col)
+    t0 = time.perf_counter()
+    drp, dcol = orc.orient(rp, col)
+    t_orient = time.perf_counter() - t0
+    m_dag = len(dcol)
+    k = 4096
+    while True:
+        t0 = time.perf_counter()
+        _, e = orc.tc_sample(drp, dcol, k)
+        dt = time.perf_counter() - t0
+        if dt > 0.5 or k == 1:
+            break
+        k = max(1, k // 8)
+    # scale the modulus so one sample takes about target_s seconds
+    k = max(1, int(k * dt / target_s)) if dt < target_s else k
+    t0 = time.perf_counter()
+    _, e = orc.tc_sample(drp, dcol, k)
+    t_sample = time.perf_counter() - t0
+    t_count = t_sample * (m_dag / max(e, 1))
+    m = len(col) // 2
+    return {
+        "value": m / (t_orient + t_count), "unit": "edges/s", "cores": orc.num_threads(),
+        "kind": "port",
+        "sample": f"oracle orientation of the whole graph ({t_orient:.2f} s) + merge count over "
+                  f"a hash-sampled 1/{k} of the sources ({e} of {m_dag} DAG edges, "
+                  f"{t_sample:.2f} s), count time extrapolated by edges",
+        "orient_s": t_orient, "count_s_extrapolated": t_count,
+    }
+
+
+def run_reference(a, rank, world):
+    if rank != 0:
+        return 0
+    from mercury_b200 import Graph
+    from oracle import oracle as orc
+    g = Graph.rmat(a.scale, a.edge_factor, seed=a.seed)
+    rp, col = np.asarray(g.rowptr), np.asarray(g.col)
+    m = len(col) // 2
+    # Size the per-step sample so W+K steps take a few minutes in total.
+    steps_total = a.steps + a.warmup
+    per_step_s = max(1.0, min(8.0, 150.0 / max(steps_total, 1)))
+    t0 = time.perf_counter()
+    drp, dcol = orc.orient(rp, col)
+    t_or = time.perf_counter() - t0
+    k = 4096
+    while True:
+        t0 = time.perf_counter()
+        orc.tc_sample(drp, dcol, k)
+        dt = time.perf_counter() - t0
+        if dt > 0.3 or k == 1:
+            break
+        k = max(1, k // 8)
+    budget = max(per_step_s - t_or, 0.3)
+    k = max(1, int(k * dt / budget)) if dt < budget else k
+    times = []
+    for i in range(steps_total):
+        t0 = time.perf_counter()
+        drp, dcol = orc.orient(rp, col)
+        t1 = time.perf_counter()
+        _, e = orc.tc_sample(drp, dcol, k, seed=0x5EED + i)
+        t2 = time.perf_counter()
+        if i >= a.warmup:
+            times.append((t1 - t0) + (t2 - t1) * (len(dcol) / max(e, 1)))
+    step_s = statistics.mean(times)
+    value = m / step_s
+    line = {
+        "metric": "TC edges/s", "value": value, "unit": "edges/s", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": step_s * 1e3,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic", "config": workload_config(a), "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "edges/s", "cores": orc.num_threads(),
+                         "kind": "port",
+                         "sample": f"per step: oracle orientation of the whole graph + merge "
+                                   f"count over a hash-sampled 1/{k} of the sources, count "
+                                   f"time extrapolated by DAG edges"},
+        "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- GPU side
+def run_ours(a, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from mercury_b200 import DeviceGraph, Graph, Timing, tc_count_host
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    g = Graph.rmat(a.scale, a.edge_factor, seed=a.seed)
+    n, nnz = g.n, g.nnz
+    m = nnz // 2
+    dg = DeviceGraph(g)
+    stream = torch.cuda.ExternalStream(dg.stream)
+
+    def step():
+        if world == 1:
+            return dg.tc_count(), dg.last_timing
+        part = dg.tc_count_shard(rank, world)
+        t = dg.last_timing
+        buf = torch.tensor([part], dtype=torch.int64, device="cuda")
+        dist.all_reduce(buf)
+        return int(buf.item()), t
+
+    first = None
+    for _ in range(a.warmup):
+        c, _ = step()
+        first = c if first is None else first
+        assert c == first, "count changed between warm-up steps"
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+    hub_ms, count_ms, orient_ms, launches = [], [], [], 0
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clocks:
+        ev0.record(stream)
+        for _ in range(a.steps):
+            c, t = step()
+            if first is not None:
+                assert c == first, "count changed between steps"
+            first = c
+            hub_ms.append(t.hub_ms)
+            count_ms.append(t.count_ms)
+            orient_ms.append(t.orient_ms)
+            launches += int(t.launches)
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    total_ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        tt = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+        dist.barrier()
+    ms_per_step = total_ms / a.steps
+    value = m / (ms_per_step / 1e3)
+    count = first
+
+    # ---- end to end through the public one-shot call, host buffers -------
+    e2e = None
+    if rank == 0 or world == 1:
+        rp_pin = torch.from_numpy(np.asarray(g.rowptr)).pin_memory()
+        col_pin = torch.from_numpy(np.asarray(g.col)).pin_memory()
+        rp_np, col_np = rp_pin.numpy(), col_pin.numpy()
+        tm = Timing()
+        for _ in range(2):
+            assert tc_count_host(rp_np, col_np, tm) == count
+        t0 = time.perf_counter()
+        for _ in range(a.e2e_steps):
+            assert tc_count_host(rp_np, col_np, tm) == count
+        e2e_s = (time.perf_counter() - t0) / a.e2e_steps
+        launches_e2e = int(tm.launches)
+        e2e = {"value": m / e2e_s, "unit": "edges/s", "ms_per_step": e2e_s * 1e3,
+               "h2d_bytes_per_step": int(rp_np.nbytes + col_np.nbytes),
+               "d2h_bytes_per_step": 8 + 8 * 8 + 4,
+               "timed_with": "host wall clock around each synchronous call",
+               "launches_per_step": launches_e2e}
+        del rp_pin, col_pin
+
+    if rank != 0:
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
+
+    # ---- roofline of the dominant kernel ----------------------------------
+    drp, dcol = dg.export_dag()
+    ab = algorithmic_bytes(n, drp, dcol)
+    stats = dg.tc_stats()
+    peak, peak_kind = load_peaks()
+    hub_avg = statistics.mean(hub_ms)
+    cnt_avg = statistics.mean(count_ms)
+    achieved = ab["b_hub"] / (hub_avg / 1e3) / 1e9
+    traffic = traffic_from_profile()
+    line = {
+        "metric": "TC edges/s", "value": value, "unit": "edges/s", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic", "config": {**workload_config(a), "n": n, "m": m,
+                                        "parallelism": f"task-shard x{world}" if world > 1 else "1 GPU"},
+        "triangles": count,
+        "phases_ms": {"orient": statistics.mean(orient_ms), "count": cnt_avg, "hub_kernel": hub_avg,
+                      "leaf_kernel": statistics.mean([t for t in (np.array(count_ms) - np.array(hub_ms))])},
+        "count_phase_edges_per_s": m / (cnt_avg / 1e3),
+        "roofline": {"bound": "hbm", "kernel": "tc_hub_kernel", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": f"{peak_kind} hbm_gbs",
+                     "traffic": traffic,
+                     "algorithmic_bytes_per_launch": ab["b_hub"],
+                     "per_unit": "per DAG edge owned by a hub task: 12 B + 4 B x (d+u + d+v); "
+                                 "8 B per owner row"},
+        "roofline_count_phase": {"b_tc": ab["b_tc"], "achieved_gbs": ab["b_tc"] / (cnt_avg / 1e3) / 1e9,
+                                 "b_min_stream_shorter": ab["b_min"],
+                                 "achieved_min_gbs": ab["b_min"] / (cnt_avg / 1e3) / 1e9},
+        "tc_stats": stats,
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+        "e2e": e2e,
+    }
+    if world == 1 and not a.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(g, target_s=a.cpu_seconds)
+    print(json.dumps(line), flush=True)
+    dg.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    a = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(a.gpus if a.gpus == 1 else 1)))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        return run_reference(a, rank, world)
+    return run_ours(a, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

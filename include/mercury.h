@@ -1,0 +1,165 @@
+/*
+ * mercury.h -- C ABI of the B200 (sm_100a) counting path: triangle counting
+ * and the P1..P8 pattern counts over an undirected CSR graph.
+ *
+ * Every entry point returns an int status (MC_OK == 0, negative on error)
+ * and never exits or aborts the calling process; mc_strerror() names the
+ * status.  Device buffers are owned by the handle that created them until
+ * the matching *_free call.  Calls on distinct handles may run from distinct
+ * host threads; calls on one handle must be serialised by the caller.
+ *
+ * Graph contract (the reference's input contract, graph.cc:18-35): vertex ids
+ * are int32 in [0, n), row offsets are int64 with rowptr[0] == 0 and
+ * rowptr[n] == nnz, each row is sorted strictly ascending (no duplicates), no
+ * self-loops, and the adjacency is symmetric (nnz == 2m directed entries).
+ * mc_dgraph_create() checks everything but symmetry on the device and
+ * refuses a graph that breaks it with MC_ERR_FORMAT; MC_VALIDATE_SYMMETRY
+ * adds the symmetry check.
+ */
+#ifndef MERCURY_B200_H
+#define MERCURY_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define MC_OK 0
+#define MC_ERR_ARG (-1)         /* null pointer, bad size, bad pattern id      */
+#define MC_ERR_IO (-2)          /* a file could not be opened/read/written     */
+#define MC_ERR_FORMAT (-3)      /* input breaks the CSR contract above         */
+#define MC_ERR_OOM (-4)         /* host or device allocation failed            */
+#define MC_ERR_CUDA (-5)        /* a CUDA runtime call failed                  */
+#define MC_ERR_DEVICE (-6)      /* a kernel raised its error flag              */
+#define MC_ERR_UNSUPPORTED (-7) /* size beyond a documented limit              */
+#define MC_ERR_NO_DEVICE (-8)   /* no CUDA device visible                      */
+#define MC_ERR_BUDGET (-9)      /* request refused by the HBM budget           */
+#define MC_ERR_TIMEOUT (-10)    /* a bounded wait expired                      */
+
+/* ---- flags for mc_dgraph_create ----------------------------------------- */
+#define MC_VALIDATE_SYMMETRY 0x1u
+
+/* Opaque handles. */
+typedef struct mc_graph mc_graph_t;   /* host CSR (loaded or generated)      */
+typedef struct mc_dgraph mc_dgraph_t; /* device-resident CSR + its scratch   */
+
+/* Per-call device timings in milliseconds, measured with CUDA events on the
+ * handle's stream.  Fields a call does not run are left at 0. */
+typedef struct mc_timing {
+  double h2d_ms;      /* host->device copy of the CSR (one-shot calls)       */
+  double orient_ms;   /* degree order, DAG build, partner lists, task queue  */
+  double count_ms;    /* counting kernels                                    */
+  double d2h_ms;      /* device->host copy of the result                     */
+  double total_ms;    /* first to last event of the call                     */
+  double hub_ms;      /* share of count_ms spent in the hash (hub) kernel    */
+  double leaf_ms;     /* share of count_ms spent in the warp (leaf) kernel   */
+  int64_t launches;   /* kernels this call launched                          */
+} mc_timing_t;
+
+/* Sizes of the device preprocessing, for reporting and parity tests. */
+typedef struct mc_tc_stats {
+  int64_t n;             /* vertices                                         */
+  int64_t nnz;           /* directed entries of the symmetric CSR (2m)       */
+  int64_t dag_edges;     /* m+ = edges of the degree-ordered DAG             */
+  int64_t max_out_degree;/* max d+ over the DAG                              */
+  int64_t hub_tasks;     /* tasks routed to the CTA hash kernel              */
+  int64_t leaf_tasks;    /* tasks routed to the warp kernel                  */
+  int64_t partner_edges; /* DAG edges whose two ends both have d+ >= 1       */
+  double probe_work;     /* sum over partner edges of the streamed list size */
+} mc_tc_stats_t;
+
+/* ---- status ------------------------------------------------------------- */
+const char *mc_strerror(int status);
+/* Library version string ("mercury_b200 <semver> sm_100a"). */
+const char *mc_version(void);
+
+/* ---- host graphs ---------------------------------------------------------
+ * mc_graph_load replaces the reference loader Graph::Graph(prefix)
+ * (graph.cc:6-35): reads <prefix>.meta.txt (10 whitespace fields: nv ne
+ * vid_size eid_size vlabel_size elabel_size max_degree feat_len n_vclasses
+ * n_eclasses), <prefix>.vertex.bin (int64[nv+1]) and <prefix>.edge.bin
+ * (int32[ne]).  The reference asserts the field sizes and
+ * 0 < max_degree < nv (graph.cc:24-28); this returns MC_ERR_FORMAT instead. */
+int mc_graph_load(const char *prefix, mc_graph_t **out);
+/* Writes the same three files (the layout the reference reader expects). */
+int mc_graph_write(const mc_graph_t *g, const char *prefix);
+/* Wraps caller arrays into a host graph (copied; the caller keeps its own). */
+int mc_graph_from_csr(const int64_t *rowptr, const int32_t *col, int64_t n,
+                      int64_t nnz, mc_graph_t **out);
+int mc_graph_info(const mc_graph_t *g, int64_t *n, int64_t *nnz,
+                  int64_t *max_degree);
+/* Borrowed pointers, valid until mc_graph_free. */
+const int64_t *mc_graph_rowptr(const mc_graph_t *g);
+const int32_t *mc_graph_col(const mc_graph_t *g);
+/* Host-side contract check (sorted rows, ids in range, no self-loops and,
+ * when check_symmetry != 0, symmetry).  MC_OK or MC_ERR_FORMAT. */
+int mc_graph_validate(const mc_graph_t *g, int check_symmetry);
+void mc_graph_free(mc_graph_t *g);
+
+/* Seeded synthetic graphs (the reference ships only a closed converter
+ * binary, datasets/converter.sh:5; these produce the same CSR layout).
+ * RMAT: 2^scale vertices, edge_factor*2^scale draws of (a,b,c,1-a-b-c)
+ * quadrant recursion, no noise, no relabelling; self-loops dropped,
+ * symmetrised, deduplicated, sorted. */
+int mc_gen_rmat(int scale, int edge_factor, double a, double b, double c,
+                uint64_t seed, mc_graph_t **out);
+/* Chung-Lu: weights w_i = (i+1)^(-1/(gamma-1)) scaled to mean_degree and
+ * capped at max_weight; n*mean_degree/2 endpoint pairs drawn proportional to
+ * w; self-loops and duplicates dropped. */
+int mc_gen_chung_lu(int64_t n, double gamma, double mean_degree,
+                    double max_weight, uint64_t seed, mc_graph_t **out);
+
+/* ---- device graphs -------------------------------------------------------
+ * mc_dgraph_create replaces GraphGPU::init / init_with_division
+ * (include/graph_gpu.h:87-188): copies the symmetric CSR to the current
+ * device and validates it there.  `stream` is a cudaStream_t (NULL: the
+ * handle creates its own non-blocking stream).  The orientation
+ * (Graph::orientation_with_division, graph.cc:196-321) is NOT done on the
+ * host: mc_tc_count builds it on the device. */
+int mc_dgraph_create(const int64_t *rowptr, const int32_t *col, int64_t n,
+                     int64_t nnz, void *stream, unsigned flags,
+                     mc_dgraph_t **out);
+/* Same, from a CSR that already lives in device memory (copied into the
+ * handle with device-to-device copies on the handle's stream). */
+int mc_dgraph_create_device(const int64_t *d_rowptr, const int32_t *d_col,
+                            int64_t n, int64_t nnz, void *stream,
+                            unsigned flags, mc_dgraph_t **out);
+/* The cudaStream_t every call on this handle is issued on. */
+int mc_dgraph_stream(const mc_dgraph_t *g, void **stream);
+void mc_dgraph_free(mc_dgraph_t *g);
+
+/* Triangle count.  Replaces TCSolver(Graph&, uint64_t&) (tc_challenge.cu:11,
+ * declared main.cc:3) and its two kernels hashIndex_for_large_degree and
+ * binarySearch_for_small_degree (gpu_kernels/tc_challenge.cuh:4-303).
+ * Device-side: degree-ordered DAG (u->v iff deg v > deg u, or equal degree
+ * and v > u: graph.cc:207-214), then sum over DAG edges of
+ * |N+(u) & N+(v)|.  Blocks until the count is on the host. */
+int mc_tc_count(mc_dgraph_t *g, uint64_t *count, mc_timing_t *timing);
+/* Partial triangle count over shard `shard` of `num_shards`: the counting
+ * tasks are dealt round-robin to the shards, so the partial counts of
+ * shards 0..num_shards-1 sum to mc_tc_count's result.  Each GPU of a
+ * multi-GPU run holds the whole graph and counts its own shard; the partial
+ * counts are then summed across ranks (the reference's MPI_Reduce,
+ * tc_multigpu/tc_challenge_multigpu.cu:198-206). */
+int mc_tc_count_shard(mc_dgraph_t *g, int shard, int num_shards,
+                      uint64_t *partial, mc_timing_t *timing);
+/* Preprocessing sizes of the last mc_tc_count on this handle. */
+int mc_tc_stats(const mc_dgraph_t *g, mc_tc_stats_t *stats);
+/* Copies the device-built DAG (after mc_tc_count) to host arrays of n+1
+ * and dag_edges entries, for parity checks of the orientation. */
+int mc_dgraph_export_dag(const mc_dgraph_t *g, int64_t *rowptr_out,
+                         int32_t *col_out);
+
+/* One-shot drop-in for TCSolver: host CSR in, count out.  Uploads, orients,
+ * counts and copies the result back inside the call (timing->h2d_ms etc.).
+ * Device buffers are cached in a per-thread context and reused while the
+ * graph fits, so repeated calls do not re-allocate. */
+int mc_tc_count_host(const int64_t *rowptr, const int32_t *col, int64_t n,
+                     int64_t nnz, uint64_t *count, mc_timing_t *timing);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MERCURY_B200_H */

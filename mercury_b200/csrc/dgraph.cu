@@ -1,0 +1,339 @@
+// C ABI of the device graph handle and the triangle-count entry points.
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+
+#include "dgraph.cuh"
+#include "device_common.cuh"
+#include "scan.cuh"
+
+namespace mc {
+
+namespace {
+thread_local cudaError_t t_last_cuda = cudaSuccess;
+
+__global__ void probe_work_kernel(const int32_t *prt_col, const int32_t *dplus, int64_t count,
+                                  unsigned long long *out) {
+  unsigned long long s = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+       i += (int64_t)gridDim.x * blockDim.x)
+    s += (unsigned long long)dplus[prt_col[i]];
+  s = warp_sum_u64(s);
+  if ((threadIdx.x & 31) == 0 && s) atomicAdd(out, s);
+}
+
+double elapsed(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) return 0.0;
+  return (double)ms;
+}
+
+void release(mc_dgraph *g) {
+  if (!g) return;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(g->device);
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  void *bufs[] = {g->rowptr,     g->col,        g->deg,      g->dplus,     g->dag_rowptr,
+                  g->dag_col,    g->prt_rowptr, g->prt_col,  g->tile_counts, g->tile_offsets,
+                  g->hub_cnt,    g->leaf_cnt,   g->hub_off,  g->leaf_off,  g->hub_tasks,
+                  g->leaf_tasks, g->scan_temp,  g->counters, g->err};
+  for (void *p : bufs)
+    if (p) cudaFree(p);
+  if (g->h_counters) cudaFreeHost(g->h_counters);
+  for (cudaEvent_t e : g->ev)
+    if (e) cudaEventDestroy(e);
+  if (g->own_stream && g->stream) cudaStreamDestroy(g->stream);
+  if (prev >= 0) cudaSetDevice(prev);
+  delete g;
+}
+
+int create_common(int64_t n, int64_t nnz, void *stream, mc_dgraph **out, mc_dgraph **gp) {
+  if (!out || n < 0 || nnz < 0) return MC_ERR_ARG;
+  if (n > INT32_MAX - 1) return MC_ERR_UNSUPPORTED;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MC_ERR_NO_DEVICE;
+  mc_dgraph *g = new (std::nothrow) mc_dgraph();
+  if (!g) return MC_ERR_OOM;
+  *gp = g;
+  MC_CUDA_TRY(cudaGetDevice(&g->device));
+  MC_CUDA_TRY(cudaDeviceGetAttribute(&g->num_sms, cudaDevAttrMultiProcessorCount, g->device));
+  if (stream) {
+    g->stream = static_cast<cudaStream_t>(stream);
+  } else {
+    MC_CUDA_TRY(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+    g->own_stream = true;
+  }
+  g->n = n;
+  g->nnz = nnz;
+  MC_CUDA_TRY(cudaMalloc((void **)&g->rowptr, sizeof(int64_t) * (size_t)(n + 1)));
+  MC_CUDA_TRY(cudaMalloc((void **)&g->col, sizeof(int32_t) * (size_t)std::max<int64_t>(nnz, 1)));
+  MC_CUDA_TRY(cudaMalloc((void **)&g->counters, sizeof(unsigned long long) * 8));
+  MC_CUDA_TRY(cudaMalloc((void **)&g->err, sizeof(unsigned)));
+  MC_CUDA_TRY(cudaMallocHost((void **)&g->h_counters, sizeof(unsigned long long) * 8 + 64));
+  g->h_err = reinterpret_cast<unsigned *>(g->h_counters + 8);
+  for (cudaEvent_t &e : g->ev) MC_CUDA_TRY(cudaEventCreate(&e));
+  return MC_OK;
+}
+
+int finish_create(mc_dgraph *g, unsigned flags, mc_dgraph **out, int rc) {
+  if (rc == MC_OK) rc = validate_graph(g, flags);
+  if (rc != MC_OK) {
+    release(g);
+    return rc;
+  }
+  *out = g;
+  return MC_OK;
+}
+
+// Per-thread cache for the one-shot entry point: the handle is kept and its
+// buffers reused while later graphs fit in its capacity.
+struct HostCache {
+  mc_dgraph *g = nullptr;
+  int64_t cap_n = -1, cap_nnz = -1;
+  ~HostCache() { release(g); }
+};
+thread_local HostCache t_cache;
+
+}  // namespace
+
+void set_last_cuda_error(cudaError_t e) { t_last_cuda = e; }
+
+int tc_stats(mc_dgraph *g, mc_tc_stats_t *st) {
+  std::memset(st, 0, sizeof(*st));
+  st->n = g->n;
+  st->nnz = g->nnz;
+  if (!g->tc_ready || g->n == 0) return MC_OK;
+  int64_t v[4] = {0, 0, 0, 0};
+  const int64_t *src[4] = {g->dag_rowptr + g->n, g->prt_rowptr + g->n, g->hub_off + g->n,
+                           g->leaf_off + g->n};
+  for (int i = 0; i < 4; ++i)
+    MC_CUDA_TRY(cudaMemcpyAsync(&v[i], src[i], sizeof(int64_t), cudaMemcpyDeviceToHost, g->stream));
+  MC_CUDA_TRY(cudaMemsetAsync(g->counters + 4, 0, sizeof(unsigned long long), g->stream));
+  MC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  if (v[1] > 0) {
+    probe_work_kernel<<<g->num_sms * 4, 256, 0, g->stream>>>(g->prt_col, g->dplus, v[1],
+                                                            g->counters + 4);
+    MC_CUDA_TRY(cudaGetLastError());
+  }
+  unsigned long long c[8];
+  MC_CUDA_TRY(cudaMemcpyAsync(c, g->counters, sizeof(c), cudaMemcpyDeviceToHost, g->stream));
+  MC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  st->dag_edges = v[0];
+  st->partner_edges = v[1];
+  st->hub_tasks = v[2];
+  st->leaf_tasks = v[3];
+  st->max_out_degree = (int64_t)c[3];
+  st->probe_work = (double)c[4];
+  return MC_OK;
+}
+
+}  // namespace mc
+
+using mc::release;
+
+extern "C" {
+
+const char *mc_strerror(int status) {
+  switch (status) {
+    case MC_OK: return "ok";
+    case MC_ERR_ARG: return "invalid argument";
+    case MC_ERR_IO: return "file could not be opened, read or written";
+    case MC_ERR_FORMAT: return "input breaks the CSR contract";
+    case MC_ERR_OOM: return "out of host or device memory";
+    case MC_ERR_CUDA: return "CUDA runtime error";
+    case MC_ERR_DEVICE: return "a kernel raised its error flag";
+    case MC_ERR_UNSUPPORTED: return "size beyond a documented limit";
+    case MC_ERR_NO_DEVICE: return "no CUDA device visible";
+    case MC_ERR_BUDGET: return "refused by the HBM budget";
+    case MC_ERR_TIMEOUT: return "a bounded wait expired";
+    default: return "unknown status";
+  }
+}
+
+const char *mc_version(void) { return "mercury_b200 0.1.0 sm_100a"; }
+
+int mc_dgraph_create(const int64_t *rowptr, const int32_t *col, int64_t n, int64_t nnz,
+                     void *stream, unsigned flags, mc_dgraph_t **out) {
+  if (!rowptr || (nnz > 0 && !col)) return MC_ERR_ARG;
+  mc_dgraph *g = nullptr;
+  int rc = mc::create_common(n, nnz, stream, out, &g);
+  if (rc != MC_OK) {
+    release(g);
+    return rc;
+  }
+  auto up = [&]() -> int {
+    MC_CUDA_TRY(cudaMemcpyAsync(g->rowptr, rowptr, sizeof(int64_t) * (size_t)(n + 1),
+                                cudaMemcpyHostToDevice, g->stream));
+    if (nnz > 0)
+      MC_CUDA_TRY(cudaMemcpyAsync(g->col, col, sizeof(int32_t) * (size_t)nnz,
+                                  cudaMemcpyHostToDevice, g->stream));
+    return MC_OK;
+  };
+  return mc::finish_create(g, flags, out, up());
+}
+
+int mc_dgraph_create_device(const int64_t *d_rowptr, const int32_t *d_col, int64_t n, int64_t nnz,
+                            void *stream, unsigned flags, mc_dgraph_t **out) {
+  if (!d_rowptr || (nnz > 0 && !d_col)) return MC_ERR_ARG;
+  mc_dgraph *g = nullptr;
+  int rc = mc::create_common(n, nnz, stream, out, &g);
+  if (rc != MC_OK) {
+    release(g);
+    return rc;
+  }
+  auto up = [&]() -> int {
+    MC_CUDA_TRY(cudaMemcpyAsync(g->rowptr, d_rowptr, sizeof(int64_t) * (size_t)(n + 1),
+                                cudaMemcpyDeviceToDevice, g->stream));
+    if (nnz > 0)
+      MC_CUDA_TRY(cudaMemcpyAsync(g->col, d_col, sizeof(int32_t) * (size_t)nnz,
+                                  cudaMemcpyDeviceToDevice, g->stream));
+    return MC_OK;
+  };
+  return mc::finish_create(g, flags, out, up());
+}
+
+int mc_dgraph_stream(const mc_dgraph_t *g, void **stream) {
+  if (!g || !stream) return MC_ERR_ARG;
+  *stream = (void *)g->stream;
+  return MC_OK;
+}
+
+void mc_dgraph_free(mc_dgraph_t *g) { release(g); }
+
+int mc_tc_count(mc_dgraph_t *g, uint64_t *count, mc_timing_t *timing) {
+  return mc_tc_count_shard(g, 0, 1, count, timing);
+}
+
+int mc_tc_count_shard(mc_dgraph_t *g, int shard, int num_shards, uint64_t *count,
+                      mc_timing_t *timing) {
+  if (!g || !count || num_shards < 1 || shard < 0 || shard >= num_shards) return MC_ERR_ARG;
+  MC_CUDA_TRY(cudaSetDevice(g->device));
+  int rc = mc::tc_alloc(g);
+  if (rc != MC_OK) return rc;
+  cudaStream_t s = g->stream;
+  const int64_t launches_before = g->launches;
+  MC_CUDA_TRY(cudaEventRecord(g->ev[0], s));
+  rc = mc::tc_orient(g);
+  if (rc != MC_OK) return rc;
+  MC_CUDA_TRY(cudaEventRecord(g->ev[1], s));
+  // The hub table size follows the largest DAG out-degree (load <= 1/4).
+  MC_CUDA_TRY(cudaMemcpyAsync(g->h_counters + 3, g->counters + 3, sizeof(unsigned long long),
+                              cudaMemcpyDeviceToHost, s));
+  MC_CUDA_TRY(cudaStreamSynchronize(s));
+  const long long maxd = (long long)g->h_counters[3];
+  // MERCURY_TC_TABLE_LOG2_MAX (8..15) lowers the shared-memory table cap;
+  // owners whose list no longer fits are then probed by binary search in
+  // global memory (tests use it to reach that path on small graphs).
+  int cap = mc::kHubTableLog2Max;
+  if (const char *env = std::getenv("MERCURY_TC_TABLE_LOG2_MAX")) {
+    const int v = std::atoi(env);
+    if (v >= 8 && v <= mc::kHubTableLog2Max) cap = v;
+  }
+  int lg = 8;
+  while (lg < cap && (1ll << lg) < 4 * maxd) ++lg;
+  g->hub_table_log2 = lg;
+  MC_CUDA_TRY(cudaEventRecord(g->ev[4], s));
+  rc = mc::tc_count_launch(g, g->ev[2], shard, num_shards);
+  if (rc != MC_OK) return rc;
+  MC_CUDA_TRY(cudaEventRecord(g->ev[3], s));
+  MC_CUDA_TRY(cudaMemcpyAsync(g->h_counters, g->counters, sizeof(unsigned long long) * 8,
+                              cudaMemcpyDeviceToHost, s));
+  MC_CUDA_TRY(cudaMemcpyAsync(g->h_err, g->err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  MC_CUDA_TRY(cudaStreamSynchronize(s));
+  if (*g->h_err) return MC_ERR_DEVICE;
+  *count = (uint64_t)g->h_counters[0];
+  if (timing) {
+    std::memset(timing, 0, sizeof(*timing));
+    timing->orient_ms = mc::elapsed(g->ev[0], g->ev[1]);
+    timing->hub_ms = mc::elapsed(g->ev[4], g->ev[2]);
+    timing->leaf_ms = mc::elapsed(g->ev[2], g->ev[3]);
+    timing->count_ms = mc::elapsed(g->ev[4], g->ev[3]);
+    timing->total_ms = mc::elapsed(g->ev[0], g->ev[3]);
+    timing->launches = g->launches - launches_before;
+  }
+  return MC_OK;
+}
+
+int mc_tc_stats(const mc_dgraph_t *g, mc_tc_stats_t *stats) {
+  if (!g || !stats) return MC_ERR_ARG;
+  MC_CUDA_TRY(cudaSetDevice(g->device));
+  return mc::tc_stats(const_cast<mc_dgraph *>(g), stats);
+}
+
+int mc_dgraph_export_dag(const mc_dgraph_t *g, int64_t *rowptr_out, int32_t *col_out) {
+  if (!g || !rowptr_out) return MC_ERR_ARG;
+  if (!g->tc_ready) return MC_ERR_ARG;
+  MC_CUDA_TRY(cudaSetDevice(g->device));
+  MC_CUDA_TRY(cudaMemcpyAsync(rowptr_out, g->dag_rowptr, sizeof(int64_t) * (size_t)(g->n + 1),
+                              cudaMemcpyDeviceToHost, g->stream));
+  MC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  const int64_t m = rowptr_out[g->n];
+  if (m > 0) {
+    if (!col_out) return MC_ERR_ARG;
+    MC_CUDA_TRY(cudaMemcpyAsync(col_out, g->dag_col, sizeof(int32_t) * (size_t)m,
+                                cudaMemcpyDeviceToHost, g->stream));
+    MC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  }
+  return MC_OK;
+}
+
+int mc_tc_count_host(const int64_t *rowptr, const int32_t *col, int64_t n, int64_t nnz,
+                     uint64_t *count, mc_timing_t *timing) {
+  if (!rowptr || (nnz > 0 && !col) || !count || n < 0 || nnz < 0) return MC_ERR_ARG;
+  mc::HostCache &c = mc::t_cache;
+  int dev = 0;
+  MC_CUDA_TRY(cudaGetDevice(&dev));
+  if (c.g && (c.g->device != dev || n > c.cap_n || nnz > c.cap_nnz)) {
+    release(c.g);
+    c.g = nullptr;
+  }
+  if (!c.g) {
+    mc_dgraph *g = nullptr;
+    mc_dgraph *tmp = nullptr;
+    int rc = mc::create_common(n, nnz, nullptr, &tmp, &g);
+    if (rc != MC_OK) {
+      release(g);
+      return rc;
+    }
+    c.g = g;
+    c.cap_n = n;
+    c.cap_nnz = nnz;
+    rc = mc::tc_alloc(g);
+    if (rc != MC_OK) {
+      release(g);
+      c.g = nullptr;
+      return rc;
+    }
+  }
+  mc_dgraph *g = c.g;
+  g->n = n;
+  g->nnz = nnz;
+  cudaEvent_t e0, e1;
+  MC_CUDA_TRY(cudaEventCreate(&e0));
+  MC_CUDA_TRY(cudaEventCreate(&e1));
+  MC_CUDA_TRY(cudaEventRecord(e0, g->stream));
+  MC_CUDA_TRY(cudaMemcpyAsync(g->rowptr, rowptr, sizeof(int64_t) * (size_t)(n + 1),
+                              cudaMemcpyHostToDevice, g->stream));
+  if (nnz > 0)
+    MC_CUDA_TRY(cudaMemcpyAsync(g->col, col, sizeof(int32_t) * (size_t)nnz, cudaMemcpyHostToDevice,
+                                g->stream));
+  MC_CUDA_TRY(cudaEventRecord(e1, g->stream));
+  g->launches = 0;
+  int rc = mc::validate_graph(g, 0);
+  const int64_t validate_launches = g->launches;
+  if (rc == MC_OK) rc = mc_tc_count(g, count, timing);
+  if (rc == MC_OK && timing) {
+    timing->h2d_ms = mc::elapsed(e0, e1);
+    timing->orient_ms += mc::elapsed(e1, g->ev[0]);  // validation on upload
+    timing->total_ms = mc::elapsed(e0, g->ev[3]);
+    timing->launches += validate_launches;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}
+
+}  // extern "C"

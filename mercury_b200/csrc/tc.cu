@@ -1,0 +1,258 @@
+// Triangle-count kernels.  count = sum over DAG edges {x, y} of
+// |N+(x) & N+(y)|, where x is the edge's owner (larger d+, ties to the larger
+// id) and y its partner.  Both kernels put N+(owner) into a shared-memory
+// open-addressing table once per task and stream the partners' (shorter)
+// lists through it, 32 list entries per warp step with the lanes flattened
+// across partner boundaries.
+//
+// Reference counterparts: hashIndex_for_large_degree (CTA per large vertex,
+// 1019-bin hash staged through a 256 MiB global scratch,
+// gpu_kernels/tc_challenge.cuh:4-192) and binarySearch_for_small_degree
+// (warp per small vertex, binary search in shared memory,
+// gpu_kernels/tc_challenge.cuh:195-303), each with an atomic work counter
+// (DYNAMIC_MODE, gpu_kernels/tuning_schedules.cuh:1-21).  Here the queues hold
+// bounded (owner, partner-chunk) tasks, the tables live in shared memory only,
+// and the hash needs no global scratch.
+#include <algorithm>
+
+#include "dgraph.cuh"
+#include "device_common.cuh"
+
+namespace mc {
+namespace {
+
+struct CountArgs {
+  const int64_t *__restrict__ dag_rowptr;
+  const int32_t *__restrict__ dag_col;
+  const int64_t *__restrict__ prt_rowptr;
+  const int32_t *__restrict__ prt_col;
+  const uint64_t *__restrict__ tasks;
+  const int64_t *__restrict__ ntasks;  // device scalar (end of the offsets)
+  unsigned long long *queue;
+  unsigned long long *result;
+  unsigned *err;
+  int table_log2_max;
+  int shard, num_shards;  // this call counts tasks shard, shard + num_shards, ...
+};
+
+// Tasks of this shard: queue position t maps to task t * num_shards + shard.
+__device__ __forceinline__ int64_t shard_tasks(const CountArgs &a) {
+  const int64_t total = *a.ntasks;
+  return total > a.shard ? (total - a.shard + a.num_shards - 1) / a.num_shards : 0;
+}
+__device__ __forceinline__ uint64_t shard_task(const CountArgs &a, unsigned long long t) {
+  return a.tasks[(int64_t)t * a.num_shards + a.shard];
+}
+
+// Probe of an open-addressing table (empty slot = -1, linear probing).
+struct TableProbe {
+  const int *tab;
+  unsigned mask;
+  int shift;
+  __device__ __forceinline__ int operator()(int w) const {
+    unsigned h = hash_slot(w, shift);
+#pragma unroll 1
+    for (unsigned it = 0; it <= mask; ++it) {
+      const int t = tab[h];
+      if (t == w) return 1;
+      if (t < 0) return 0;
+      h = (h + 1) & mask;
+    }
+    return 0;
+  }
+};
+
+// Binary search in a sorted global list (owners too large for the table).
+struct ListProbe {
+  const int32_t *list;
+  int len;
+  __device__ __forceinline__ int operator()(int w) const {
+    int lo = 0, hi = len - 1;
+    while (lo <= hi) {
+      int mid = (lo + hi) >> 1;
+      int m = __ldg(list + mid);
+      if (m == w) return 1;
+      if (m < w) lo = mid + 1; else hi = mid - 1;
+    }
+    return 0;
+  }
+};
+
+__device__ __forceinline__ void table_insert(int *tab, unsigned mask, int shift, int key,
+                                             unsigned *err) {
+  unsigned h = hash_slot(key, shift);
+  for (unsigned it = 0;; ++it) {
+    const int prev = atomicCAS(tab + h, -1, key);
+    if (prev == -1 || prev == key) return;
+    h = (h + 1) & mask;
+    if (it >= mask) {
+      atomicOr(err, (unsigned)kErrHashFull);
+      return;
+    }
+  }
+}
+
+// Streams the partner lists of partners [q0, q1) (batches of 32 partners
+// starting at q0 + 32*first, stepping by 32*step) through `probe`.  Within a
+// batch the 32 lanes walk the concatenated lists 32 entries at a time: lane L
+// of window F handles flat entry F + L, and the partner that entry belongs to
+// comes from the bit mask of partner starts inside the window.
+template <class Probe>
+__device__ __forceinline__ unsigned long long stream_partners(const CountArgs &a, int64_t q0,
+                                                              int64_t q1, int first, int step,
+                                                              int lane, const Probe &probe) {
+  unsigned long long hits = 0;
+  for (int64_t qb = q0 + (int64_t)kWarp * first; qb < q1; qb += (int64_t)kWarp * step) {
+    const int64_t q = qb + lane;
+    const bool valid = q < q1;
+    const int y = valid ? __ldg(a.prt_col + q) : 0;
+    const int64_t st = valid ? __ldg(a.dag_rowptr + y) : 0;
+    const int len = valid ? (int)(__ldg(a.dag_rowptr + y + 1) - st) : 0;
+    const int incl = warp_inclusive_scan(len, lane);
+    const int excl = incl - len;
+    const int total = __shfl_sync(kFull, incl, kWarp - 1);
+    const unsigned upto = lane == kWarp - 1 ? kFull : ((2u << lane) - 1u);
+    int base = 0;
+    for (int F = 0; F < total; F += kWarp) {
+      const unsigned bit =
+          (len > 0 && excl >= F && excl < F + kWarp) ? (1u << (excl - F)) : 0u;
+      const unsigned starts = __reduce_or_sync(kFull, bit);
+      const int p = max(base + __popc(starts & upto) - 1, 0);
+      const int64_t pst = __shfl_sync(kFull, st, p);
+      const int pex = __shfl_sync(kFull, excl, p);
+      const int f = F + lane;
+      if (f < total) hits += probe(__ldg(a.dag_col + pst + (f - pex)));
+      base += __popc(starts);
+    }
+  }
+  return hits;
+}
+
+__device__ __forceinline__ int ceil_log2(int v) { return v <= 1 ? 0 : 32 - __clz(v - 1); }
+
+// One CTA per hub task: N+(owner) into a table of 2^lg slots (load <= 1/4
+// when it fits, <= 1/2 at the size cap; owners beyond the cap use binary
+// search in global memory), then the 8 warps share the partner chunk.
+__global__ void __launch_bounds__(kCountThreads) tc_hub_kernel(CountArgs a) {
+  extern __shared__ int table[];
+  __shared__ unsigned long long s_task;
+  const int lane = threadIdx.x & (kWarp - 1), warp = threadIdx.x / kWarp;
+  const int nwarps = blockDim.x / kWarp;
+  const int64_t ntasks = shard_tasks(a);
+  unsigned long long hits = 0;
+  for (;;) {
+    if (threadIdx.x == 0) s_task = atomicAdd(a.queue, 1ull);
+    __syncthreads();
+    const unsigned long long t = s_task;
+    if ((int64_t)t >= ntasks) break;
+    const uint64_t task = shard_task(a, t);
+    const int x = (int)(task >> 32);
+    const int chunk = (int)(task & 0xffffffffu);
+    const int64_t a0 = a.dag_rowptr[x];
+    const int d = (int)(a.dag_rowptr[x + 1] - a0);
+    const int64_t pend = a.prt_rowptr[x + 1];
+    const int64_t q0 = a.prt_rowptr[x] + (int64_t)chunk * kHubChunk;
+    const int64_t q1 = min(q0 + kHubChunk, pend);
+    int lg = max(8, ceil_log2(4 * d));
+    if (lg > a.table_log2_max && 2 * d <= (1 << a.table_log2_max)) lg = a.table_log2_max;
+    if (lg <= a.table_log2_max) {
+      const int size = 1 << lg;
+      const unsigned mask = (unsigned)size - 1u;
+      const int shift = 32 - lg;
+      int4 *t4 = reinterpret_cast<int4 *>(table);
+      for (int i = threadIdx.x; i < size / 4; i += blockDim.x) t4[i] = make_int4(-1, -1, -1, -1);
+      __syncthreads();
+      for (int i = threadIdx.x; i < d; i += blockDim.x)
+        table_insert(table, mask, shift, __ldg(a.dag_col + a0 + i), a.err);
+      __syncthreads();
+      hits += stream_partners(a, q0, q1, warp, nwarps, lane, TableProbe{table, mask, shift});
+    } else {
+      hits += stream_partners(a, q0, q1, warp, nwarps, lane, ListProbe{a.dag_col + a0, d});
+    }
+    __syncthreads();  // table and s_task are rewritten by the next task
+  }
+  hits = warp_sum_u64(hits);
+  if (lane == 0 && hits) atomicAdd(a.result, hits);
+}
+
+// One warp per leaf task (owner d+ <= kLeafMaxOut): a private 256-slot table.
+__global__ void __launch_bounds__(kCountThreads) tc_leaf_kernel(CountArgs a) {
+  __shared__ int tables[kCountThreads / kWarp][kLeafSlots];
+  const int lane = threadIdx.x & (kWarp - 1), warp = threadIdx.x / kWarp;
+  int *tab = tables[warp];
+  constexpr int lg = 8;  // log2(kLeafSlots)
+  static_assert((1 << lg) == kLeafSlots, "leaf table size");
+  const int64_t ntasks = shard_tasks(a);
+  unsigned long long hits = 0;
+  for (;;) {
+    unsigned long long t = 0;
+    if (lane == 0) t = atomicAdd(a.queue, 1ull);
+    t = __shfl_sync(kFull, t, 0);
+    if ((int64_t)t >= ntasks) break;
+    const uint64_t task = shard_task(a, t);
+    const int x = (int)(task >> 32);
+    const int chunk = (int)(task & 0xffffffffu);
+    const int64_t a0 = a.dag_rowptr[x];
+    const int d = (int)(a.dag_rowptr[x + 1] - a0);
+    const int64_t q0 = a.prt_rowptr[x] + (int64_t)chunk * kLeafChunk;
+    const int64_t q1 = min(q0 + kLeafChunk, a.prt_rowptr[x + 1]);
+    int4 *t4 = reinterpret_cast<int4 *>(tab);
+    for (int i = lane; i < kLeafSlots / 4; i += kWarp) t4[i] = make_int4(-1, -1, -1, -1);
+    __syncwarp();
+    for (int i = lane; i < d; i += kWarp)
+      table_insert(tab, kLeafSlots - 1, 32 - lg, __ldg(a.dag_col + a0 + i), a.err);
+    __syncwarp();
+    hits += stream_partners(a, q0, q1, 0, 1, lane, TableProbe{tab, kLeafSlots - 1, 32 - lg});
+    __syncwarp();
+  }
+  hits = warp_sum_u64(hits);
+  if (lane == 0 && hits) atomicAdd(a.result, hits);
+}
+
+int resident_blocks(const void *kernel, int threads, size_t smem) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess)
+    per_sm = 1;
+  return std::max(per_sm, 1);
+}
+
+}  // namespace
+
+int tc_count_launch(mc_dgraph *g, cudaEvent_t after_hub, int shard, int num_shards) {
+  if (g->n == 0) {
+    if (after_hub) MC_CUDA_TRY(cudaEventRecord(after_hub, g->stream));
+    return MC_OK;
+  }
+  CountArgs a{};
+  a.dag_rowptr = g->dag_rowptr;
+  a.dag_col = g->dag_col;
+  a.prt_rowptr = g->prt_rowptr;
+  a.prt_col = g->prt_col;
+  a.result = g->counters + 0;
+  a.err = g->err;
+  a.table_log2_max = g->hub_table_log2;
+  a.shard = shard;
+  a.num_shards = num_shards;
+
+  const size_t hub_smem = sizeof(int) << g->hub_table_log2;
+  MC_CUDA_TRY(cudaFuncSetAttribute(tc_hub_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)hub_smem));
+  const int hub_grid = g->num_sms * resident_blocks((const void *)tc_hub_kernel, kCountThreads, hub_smem);
+  a.tasks = g->hub_tasks;
+  a.ntasks = g->hub_off + g->n;
+  a.queue = g->counters + 1;
+  g->launches += 2;
+  tc_hub_kernel<<<hub_grid, kCountThreads, hub_smem, g->stream>>>(a);
+  MC_CUDA_TRY(cudaGetLastError());
+  if (after_hub) MC_CUDA_TRY(cudaEventRecord(after_hub, g->stream));
+
+  const int leaf_grid = g->num_sms * resident_blocks((const void *)tc_leaf_kernel, kCountThreads, 0);
+  a.tasks = g->leaf_tasks;
+  a.ntasks = g->leaf_off + g->n;
+  a.queue = g->counters + 2;
+  tc_leaf_kernel<<<leaf_grid, kCountThreads, 0, g->stream>>>(a);
+  MC_CUDA_TRY(cudaGetLastError());
+  return MC_OK;
+}
+
+}  // namespace mc

@@ -1,0 +1,117 @@
+"""ORACLE -- test infrastructure, not product code.
+
+ctypes loader of the CPU restatement in oracle/oracle.cpp and
+oracle/patterns_oracle.cpp (built into oracle/_build/liboracle.so by
+``make -C oracle``).  Only tests/, the smoke check and bench.py's CPU baseline
+use it, always as the checker or the timed CPU baseline, never as a path of
+the product.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def build() -> None:
+    subprocess.run(["make", "-C", HERE, "-s"], check=True)
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        P = C.c_void_p
+        L.orc_num_threads.restype = C.c_int
+        L.orc_orient.argtypes = [C.c_int64, P, P, P, P]
+        L.orc_orient.restype = None
+        L.orc_division.argtypes = [C.c_int64, P, P, C.c_int, P]
+        L.orc_division.restype = None
+        L.orc_tc_dag.argtypes = [C.c_int64, P, P, C.c_int64, C.c_int64]
+        L.orc_tc_dag.restype = C.c_uint64
+        L.orc_tc_sample.argtypes = [C.c_int64, P, P, C.c_uint64, C.c_uint64, P]
+        L.orc_tc_sample.restype = C.c_uint64
+        L.orc_merge_volume.argtypes = [C.c_int64, P, P]
+        L.orc_merge_volume.restype = C.c_double
+        L.orc_tc.argtypes = [C.c_int64, P, P]
+        L.orc_tc.restype = C.c_uint64
+        L.orc_pattern.argtypes = [C.c_int64, P, P, C.c_int, P]
+        L.orc_pattern.restype = C.c_uint64
+        _lib = L
+    return _lib
+
+
+def _csr(rowptr, col):
+    return (np.ascontiguousarray(rowptr, dtype=np.int64),
+            np.ascontiguousarray(col, dtype=np.int32))
+
+
+def num_threads() -> int:
+    return lib().orc_num_threads()
+
+
+def orient(rowptr, col):
+    """Degree-ordered DAG (graph.cc:196-235) as (dag_rowptr, dag_col)."""
+    rowptr, col = _csr(rowptr, col)
+    n = len(rowptr) - 1
+    drp = np.zeros(n + 1, dtype=np.int64)
+    lib().orc_orient(n, rowptr.ctypes.data, col.ctypes.data, drp.ctypes.data, None)
+    dcol = np.zeros(max(int(drp[-1]), 1), dtype=np.int32)
+    lib().orc_orient(n, rowptr.ctypes.data, col.ctypes.data, drp.ctypes.data, dcol.ctypes.data)
+    return drp, dcol[: int(drp[-1])]
+
+
+def division(rowptr, col, deg_thd: int = 128) -> dict:
+    """Sizes of the reference's small/large split (graph.cc:237-312)."""
+    rowptr, col = _csr(rowptr, col)
+    out = np.zeros(4, dtype=np.int64)
+    lib().orc_division(len(rowptr) - 1, rowptr.ctypes.data, col.ctypes.data, deg_thd,
+                       out.ctypes.data)
+    return {"small_edges": int(out[0]), "large_edges": int(out[1]),
+            "small_tasks": int(out[2]), "large_tasks": int(out[3])}
+
+
+def tc(rowptr, col) -> int:
+    rowptr, col = _csr(rowptr, col)
+    return int(lib().orc_tc(len(rowptr) - 1, rowptr.ctypes.data, col.ctypes.data))
+
+
+def tc_dag(dag_rowptr, dag_col, v0: int = 0, v1: int | None = None) -> int:
+    dag_rowptr, dag_col = _csr(dag_rowptr, dag_col)
+    n = len(dag_rowptr) - 1
+    return int(lib().orc_tc_dag(n, dag_rowptr.ctypes.data, dag_col.ctypes.data, v0,
+                                n if v1 is None else v1))
+
+
+def tc_sample(dag_rowptr, dag_col, modulus: int, seed: int = 0x5EED):
+    """(count, DAG edges owned) over a hash-sampled 1/modulus of the sources."""
+    dag_rowptr, dag_col = _csr(dag_rowptr, dag_col)
+    edges = np.zeros(1, dtype=np.int64)
+    c = lib().orc_tc_sample(len(dag_rowptr) - 1, dag_rowptr.ctypes.data, dag_col.ctypes.data,
+                            modulus, seed, edges.ctypes.data)
+    return int(c), int(edges[0])
+
+
+def merge_volume(dag_rowptr, dag_col) -> float:
+    dag_rowptr, dag_col = _csr(dag_rowptr, dag_col)
+    return float(lib().orc_merge_volume(len(dag_rowptr) - 1, dag_rowptr.ctypes.data,
+                                        dag_col.ctypes.data))
+
+
+def pattern(rowptr, col, k: int, return_counters: bool = False):
+    """Reference result of pattern P<k> (1..8)."""
+    rowptr, col = _csr(rowptr, col)
+    c12 = np.zeros(2, dtype=np.uint64)
+    r = int(lib().orc_pattern(len(rowptr) - 1, rowptr.ctypes.data, col.ctypes.data, k,
+                              c12.ctypes.data))
+    if return_counters:
+        return r, int(c12[0]), int(c12[1])
+    return r

@@ -1,0 +1,150 @@
+"""Runs the reference's own programs (built from its sources into oracle/_ref/
+by oracle/ref.mk) on a GPU and records their counts and runtimes.
+
+  python tests/golden/run_reference.py [--out gpurun_out/reference_run.json]
+                                       [--scales 16,20,22] [--repeats 3]
+
+* Fixture counts: oracle/_ref/tc_challenge and oracle/_ref/sm_patterns
+  (P1..P8) on every graph in tests/golden/graphs; their
+  "total_num_triangles = N" lines are collected.  The committed result is
+  tests/golden/reference_counts.json (the oracle is pinned to it by
+  tests/test_reference_pin.py).
+* Timing: RMAT graphs of the listed scales (edge factor 16, seed 1, the
+  library's generator) are written in the reference's file layout and run
+  through the reference's tc_challenge and this repository's tc_challenge;
+  the "Runtime  = X sec" lines are collected.
+
+Before running the reference's triangle kernel on a graph this checks, on the
+CPU, the limits that kernel's fixed buffers assume
+(gpu_kernels/tc_challenge.cuh:4-192, tc_challenge.cu:93-101): DAG
+out-degree of every large-task vertex <= 4096 (shared-memory table) and at
+most 64 out-neighbours per hash bin (uid % 1019) -- a graph that breaks them
+is skipped, not run.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+REF_TC = os.path.join(ROOT, "oracle", "_ref", "tc_challenge")
+REF_SM = os.path.join(ROOT, "oracle", "_ref", "sm_patterns")
+OUR_TC = os.path.join(ROOT, "mercury_b200", "bin", "tc_challenge")
+COUNT = re.compile(r"total_num_triangles = (\d+)")
+RUNTIME = re.compile(r"^Runtime  = ([0-9.eE+-]+) sec", re.M)
+SM_RUNTIME = re.compile(r"^Total runtime  = ([0-9.eE+-]+) sec", re.M)
+
+
+def run(cmd, timeout):
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+    except subprocess.TimeoutExpired:
+        return None, "timeout"
+    if r.returncode != 0:
+        return None, f"exit {r.returncode}: {r.stderr.strip()[-300:]}"
+    return r.stdout, None
+
+
+def reference_tc_limits_ok(rowptr, col):
+    from oracle import oracle as orc
+    drp, dcol = orc.orient(rowptr, col)
+    n = len(rowptr) - 1
+    dplus = np.diff(drp)
+    if dplus.max(initial=0) > 4096:
+        return False, f"max d+ {int(dplus.max())} > 4096"
+    src = np.repeat(np.arange(n, dtype=np.int64), dplus)
+    big = dplus[src] > 128  # only vertices reaching the hash kernel matter
+    if big.any():
+        key = src[big] * 1019 + (dcol[big].astype(np.int64) % 1019)
+        _, cnt = np.unique(key, return_counts=True)
+        if cnt.max() > 64:
+            return False, f"hash bin load {int(cnt.max())} > 64"
+        return True, f"max d+ {int(dplus.max())}, max bin load {int(cnt.max())}"
+    return True, f"max d+ {int(dplus.max(initial=0))}"
+
+
+def fixture_counts(timeout):
+    out = {}
+    gdir = os.path.join(HERE, "graphs")
+    golden = json.load(open(os.path.join(HERE, "golden.json")))
+    for name in sorted(os.listdir(gdir)):
+        prefix = os.path.join(gdir, name, "graph")
+        rp = np.fromfile(prefix + ".vertex.bin", dtype=np.int64)
+        col = np.fromfile(prefix + ".edge.bin", dtype=np.int32)
+        rec = {}
+        ok, why = reference_tc_limits_ok(rp, col)
+        rec["tc_limits"] = why
+        if ok:
+            s, err = run([REF_TC, prefix], timeout)
+            rec["TC"] = int(COUNT.search(s).group(1)) if s else err
+        for k in range(1, 9):
+            if f"P{k}" not in golden[name]:
+                continue
+            s, err = run([REF_SM, prefix, f"P{k}"], timeout)
+            rec[f"P{k}"] = int(COUNT.search(s).group(1)) if s else err
+        out[name] = rec
+        print(name, rec, flush=True)
+    return out
+
+
+def timing(scales, repeats, timeout):
+    from mercury_b200 import Graph
+    res = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for sc in scales:
+            g = Graph.rmat(sc, 16, seed=1)
+            prefix = os.path.join(tmp, f"rmat{sc}", "graph")
+            os.makedirs(os.path.dirname(prefix))
+            g.write(prefix)
+            rec = {"n": g.n, "m": g.nnz // 2}
+            ok, why = reference_tc_limits_ok(np.asarray(g.rowptr), np.asarray(g.col))
+            rec["ref_limits"] = why
+            for label, exe, allowed in (("reference", REF_TC, ok), ("ours", OUR_TC, True)):
+                if not allowed:
+                    rec[label] = "skipped: " + why
+                    continue
+                runs = []
+                for _ in range(repeats):
+                    s, err = run([exe, prefix], timeout)
+                    if s is None:
+                        runs.append(err)
+                        break
+                    runs.append({"runtime_s": float(RUNTIME.search(s).group(1)),
+                                 "count": int(COUNT.search(s).group(1))})
+                rec[label] = runs
+            res[f"rmat{sc}"] = rec
+            print(f"rmat{sc}", rec, flush=True)
+    return res
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "reference_run.json"))
+    ap.add_argument("--scales", default="16,20,22")
+    ap.add_argument("--repeats", type=int, default=3)
+    ap.add_argument("--timeout", type=float, default=120.0)
+    ap.add_argument("--skip-fixtures", action="store_true")
+    a = ap.parse_args()
+    result = {}
+    if not a.skip_fixtures:
+        result["fixtures"] = fixture_counts(a.timeout)
+    scales = [int(s) for s in a.scales.split(",") if s]
+    if scales:
+        result["timing"] = timing(scales, a.repeats, a.timeout)
+    os.makedirs(os.path.dirname(a.out), exist_ok=True)
+    with open(a.out, "w") as f:
+        json.dump(result, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,85 @@
+"""The oracle pinned against brute force and the golden fixtures (CPU only)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from brute import expected_from_counts, induced_counts, random_graph, triangles
+from conftest import GOLDEN, csr_from_edges, relabel
+from oracle import oracle as orc
+
+with open(os.path.join(GOLDEN, "golden.json")) as f:
+    GOLD = json.load(f)
+
+CHEAP = ["k5", "star9", "path6", "petersen", "rand13", "isolated", "rmat8"]
+
+
+def load_fixture(name):
+    prefix = os.path.join(GOLDEN, "graphs", name, "graph")
+    rp = np.fromfile(prefix + ".vertex.bin", dtype=np.int64)
+    col = np.fromfile(prefix + ".edge.bin", dtype=np.int32)
+    return rp, col
+
+
+@pytest.mark.parametrize("name", sorted(GOLD))
+def test_oracle_tc_matches_golden(name):
+    rp, col = load_fixture(name)
+    assert orc.tc(rp, col) == GOLD[name]["TC"]
+
+
+@pytest.mark.parametrize("name", CHEAP)
+def test_oracle_patterns_match_golden(name):
+    rp, col = load_fixture(name)
+    for k in range(1, 9):
+        assert orc.pattern(rp, col, k) == GOLD[name][f"P{k}"], (name, k)
+
+
+@pytest.mark.parametrize("seed", [101, 202, 303])
+def test_oracle_formulas_are_the_induced_identities(seed):
+    n = 12
+    rp, col = csr_from_edges(n, random_graph(n, 0.4, seed))
+    exp = expected_from_counts(induced_counts(rp, col))
+    got = {"TC": orc.tc(rp, col), **{f"P{k}": orc.pattern(rp, col, k) for k in range(1, 9)}}
+    assert got == exp
+
+
+def test_oracle_tc_brute_force_rmat10():
+    rp, col = load_fixture("rmat10")
+    assert orc.tc(rp, col) == triangles(rp, col)
+
+
+def test_relabel_invariance_of_oracle():
+    rp, col = load_fixture("rmat8")
+    perm = np.random.default_rng(5).permutation(len(rp) - 1)
+    rp2, col2 = relabel(rp, col, perm)
+    assert orc.tc(rp2, col2) == orc.tc(rp, col)
+    # Pattern counts are induced-subgraph counts, so invariant too.
+    for k in (1, 4, 6):
+        assert orc.pattern(rp2, col2, k) == orc.pattern(rp, col, k)
+
+
+def test_orientation_is_a_dag_with_every_edge_once():
+    rp, col = load_fixture("cl3000")
+    drp, dcol = orc.orient(rp, col)
+    n = len(rp) - 1
+    deg = np.diff(rp)
+    assert drp[-1] * 2 == len(col)
+    src = np.repeat(np.arange(n), np.diff(drp))
+    key_s = deg[src] * (n + 1) + src
+    key_d = deg[dcol] * (n + 1) + dcol
+    assert np.all(key_d > key_s)  # strictly up the (degree, id) order
+    for v in range(n):
+        row = dcol[drp[v]:drp[v + 1]]
+        assert np.all(np.diff(row) > 0)
+
+
+def test_division_sizes_cover_the_contributing_edges():
+    rp, col = load_fixture("dense400")
+    d = orc.division(rp, col)
+    drp, _ = orc.orient(rp, col)
+    # dense400 has every out-degree >= 1 except the top vertex; every DAG
+    # edge lands in exactly one of the two lists unless an end has d+ == 0.
+    assert d["small_edges"] + d["large_edges"] <= drp[-1]
+    assert d["large_edges"] > 0
+    assert d == GOLD["dense400"]["division"]

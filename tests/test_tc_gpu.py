@@ -1,0 +1,141 @@
+"""Triangle count on the GPU vs the oracle and the golden fixtures.
+
+Every count goes through the C ABI (include/mercury.h) into the sm_100a
+kernels; counts are compared bit-exactly (uint64).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, csr_from_edges, relabel
+from mercury_b200 import DeviceGraph, Graph, McError, tc_count_host
+from mercury_b200 import _ffi
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+with open(os.path.join(GOLDEN, "golden.json")) as f:
+    GOLD = json.load(f)
+
+
+def fixture(name):
+    return Graph(os.path.join(GOLDEN, "graphs", name, "graph"))
+
+
+@pytest.mark.parametrize("name", sorted(GOLD))
+def test_tc_matches_golden(name):
+    g = fixture(name)
+    with DeviceGraph(g) as d:
+        assert d.tc_count() == GOLD[name]["TC"]
+        assert d.tc_count() == GOLD[name]["TC"]  # second call on the same handle
+
+
+@pytest.mark.parametrize("name", ["rmat10", "cl3000", "dense400", "isolated"])
+def test_device_dag_equals_oracle_orientation(name):
+    g = fixture(name)
+    rp, col = np.array(g.rowptr), np.array(g.col)
+    with DeviceGraph(g) as d:
+        d.tc_count()
+        drp, dcol = d.export_dag()
+        st = d.tc_stats()
+    orp, ocol = orc.orient(rp, col)
+    assert np.array_equal(drp, orp)
+    assert np.array_equal(dcol, ocol)
+    assert st["dag_edges"] == len(col) // 2
+    assert st["partner_edges"] <= st["dag_edges"]
+
+
+@pytest.mark.parametrize("scale,ef,seed", [(12, 16, 1), (14, 16, 2), (16, 16, 1), (16, 32, 9)])
+def test_tc_rmat_vs_oracle(scale, ef, seed):
+    g = Graph.rmat(scale, ef, seed=seed)
+    with DeviceGraph(g) as d:
+        got = d.tc_count()
+        st = d.tc_stats()
+    assert got == orc.tc(g.rowptr, g.col)
+    assert st["hub_tasks"] + st["leaf_tasks"] > 0
+
+
+@pytest.mark.parametrize("n,cap,seed", [(20000, 2000, 3), (200000, 50000, 1)])
+def test_tc_chung_lu_vs_oracle(n, cap, seed):
+    g = Graph.chung_lu(n, 2.1, 20.0, cap, seed=seed)
+    with DeviceGraph(g) as d:
+        assert d.tc_count() == orc.tc(g.rowptr, g.col)
+
+
+def test_tc_relabel_invariance():
+    g = Graph.rmat(15, 16, seed=4)
+    rp, col = np.array(g.rowptr), np.array(g.col)
+    perm = np.random.default_rng(1).permutation(len(rp) - 1)
+    rp2, col2 = relabel(rp, col, perm)
+    with DeviceGraph(rp, col) as a, DeviceGraph(rp2, col2) as b:
+        assert a.tc_count() == b.tc_count()
+
+
+def test_one_shot_host_entry_equals_handle_path():
+    g = Graph.rmat(14, 16, seed=5)
+    with DeviceGraph(g) as d:
+        want = d.tc_count()
+    t = _ffi.Timing()
+    assert tc_count_host(g.rowptr, g.col, t) == want
+    assert t.h2d_ms > 0 and t.count_ms > 0
+    # a smaller graph reuses the cached buffers
+    h = Graph.rmat(10, 8, seed=6)
+    assert tc_count_host(h.rowptr, h.col) == orc.tc(h.rowptr, h.col)
+
+
+@pytest.mark.parametrize("shards", [2, 3, 8])
+def test_shard_partials_sum_to_the_count(shards):
+    g = Graph.rmat(14, 16, seed=8)
+    with DeviceGraph(g) as d:
+        full = d.tc_count()
+        parts = [d.tc_count_shard(s, shards) for s in range(shards)]
+    assert sum(parts) == full
+    assert all(p > 0 for p in parts)
+
+
+def test_global_memory_fallback_for_large_out_lists(monkeypatch):
+    """With the table capped at 256 slots, owners with d+ > 128 take the
+    binary-search path; the count must not change."""
+    g = fixture("dense400")
+    monkeypatch.setenv("MERCURY_TC_TABLE_LOG2_MAX", "8")
+    with DeviceGraph(g) as d:
+        assert d.tc_count() == GOLD["dense400"]["TC"]
+        assert d.tc_stats()["max_out_degree"] > 128
+
+
+def test_empty_and_edgeless_graphs():
+    with DeviceGraph(np.zeros(1, dtype=np.int64), np.zeros(0, dtype=np.int32)) as d:
+        assert d.tc_count() == 0
+    with DeviceGraph(np.zeros(7, dtype=np.int64), np.zeros(0, dtype=np.int32)) as d:
+        assert d.tc_count() == 0
+    rp, col = csr_from_edges(3, [(0, 1)])
+    with DeviceGraph(rp, col) as d:
+        assert d.tc_count() == 0
+
+
+@pytest.mark.parametrize("rowptr,col,sym", [
+    ([0, 2, 3, 4], [2, 1, 0, 0], False),    # unsorted row
+    ([0, 2, 3, 4], [1, 1, 0, 0], False),    # duplicate entry
+    ([0, 2, 3, 5], [1, 2, 0, 0, 2], False), # self-loop
+    ([0, 1, 2], [1, 9], False),             # id out of range
+    ([0, 1, 2], [1, -3], False),            # negative id
+    ([0, 2, 1, 2], [1, 2], False),          # offsets not monotone
+    ([0, 1, 1], [1], True),                 # asymmetric (checked on request)
+])
+def test_device_validation_rejects(rowptr, col, sym):
+    with pytest.raises(McError) as e:
+        DeviceGraph(np.array(rowptr), np.array(col), validate_symmetry=sym)
+    assert e.value.status == _ffi.MC_ERR_FORMAT
+
+
+def test_cli_tc_challenge_prints_reference_lines():
+    import subprocess
+    from conftest import ROOT
+    exe = os.path.join(ROOT, "mercury_b200", "bin", "tc_challenge")
+    prefix = os.path.join(GOLDEN, "graphs", "rmat10", "graph")
+    out = subprocess.run([exe, prefix], capture_output=True, text=True, check=True).stdout
+    assert "Triangle Counting" in out
+    assert any(line.startswith("Runtime  = ") and line.endswith(" sec") for line in out.splitlines())
+    assert f"total_num_triangles = {GOLD['rmat10']['TC']}" in out
