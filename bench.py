@@ -329,7 +329,7 @@ def run_ours(a, rank, world, local_rank):
 
     # ---- end to end through the public one-shot call, host buffers -------
     e2e = None
-    if rank == 0 or world == 1:
+    if (rank == 0 or world == 1) and a.e2e_steps > 0:
         rp_pin = torch.from_numpy(np.asarray(g.rowptr)).pin_memory()
         col_pin = torch.from_numpy(np.asarray(g.col)).pin_memory()
         rp_np, col_np = rp_pin.numpy(), col_pin.numpy()

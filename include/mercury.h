@@ -148,7 +148,8 @@ int mc_tc_count_shard(mc_dgraph_t *g, int shard, int num_shards,
 /* Preprocessing sizes of the last mc_tc_count on this handle. */
 int mc_tc_stats(const mc_dgraph_t *g, mc_tc_stats_t *stats);
 /* Copies the device-built DAG (after mc_tc_count) to host arrays of n+1
- * and dag_edges entries, for parity checks of the orientation. */
+ * and dag_edges entries, for parity checks of the orientation.  With
+ * col_out == NULL only the offsets are copied (rowptr_out[n] = dag_edges). */
 int mc_dgraph_export_dag(const mc_dgraph_t *g, int64_t *rowptr_out,
                          int32_t *col_out);
 

@@ -271,8 +271,7 @@ int mc_dgraph_export_dag(const mc_dgraph_t *g, int64_t *rowptr_out, int32_t *col
                               cudaMemcpyDeviceToHost, g->stream));
   MC_CUDA_TRY(cudaStreamSynchronize(g->stream));
   const int64_t m = rowptr_out[g->n];
-  if (m > 0) {
-    if (!col_out) return MC_ERR_ARG;
+  if (m > 0 && col_out) {
     MC_CUDA_TRY(cudaMemcpyAsync(col_out, g->dag_col, sizeof(int32_t) * (size_t)m,
                                 cudaMemcpyDeviceToHost, g->stream));
     MC_CUDA_TRY(cudaStreamSynchronize(g->stream));
