@@ -153,6 +153,15 @@ int mc_tc_stats(const mc_dgraph_t *g, mc_tc_stats_t *stats);
 int mc_dgraph_export_dag(const mc_dgraph_t *g, int64_t *rowptr_out,
                          int32_t *col_out);
 
+/* Pattern count P<pattern> (1..8) over the symmetric graph.  Replaces the
+ * single-rank path of SMSolverMultiGPU (subgraph_matching/sm_multigpu.cu:97,
+ * kernels in subgraph_matching/pattern_kernels.cuh, combine at
+ * sm_multigpu.cu:206-232): the same quantities over all 2m directed edges,
+ * bit-exact, without MPI.  Uses per-warp frontier scratch of max_degree
+ * entries per list, grown on first use and kept by the handle. */
+int mc_pattern_count(mc_dgraph_t *g, int pattern, uint64_t *count,
+                     mc_timing_t *timing);
+
 /* One-shot drop-in for TCSolver: host CSR in, count out.  Uploads, orients,
  * counts and copies the result back inside the call (timing->h2d_ms etc.).
  * Device buffers are cached in a per-thread context and reused while the

@@ -97,6 +97,7 @@ SIGNATURES = {
     "mc_tc_stats": (C.c_int, [_P, C.POINTER(TcStats)]),
     "mc_dgraph_export_dag": (C.c_int, [_P, _P, _P]),
     "mc_tc_count_host": (C.c_int, [_P, _P, _I64, _I64, _PU64, C.POINTER(Timing)]),
+    "mc_pattern_count": (C.c_int, [_P, C.c_int, _PU64, C.POINTER(Timing)]),
 }
 
 

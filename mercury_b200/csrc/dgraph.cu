@@ -13,16 +13,6 @@ namespace mc {
 namespace {
 thread_local cudaError_t t_last_cuda = cudaSuccess;
 
-__global__ void probe_work_kernel(const int32_t *prt_col, const int32_t *dplus, int64_t count,
-                                  unsigned long long *out) {
-  unsigned long long s = 0;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
-       i += (int64_t)gridDim.x * blockDim.x)
-    s += (unsigned long long)dplus[prt_col[i]];
-  s = warp_sum_u64(s);
-  if ((threadIdx.x & 31) == 0 && s) atomicAdd(out, s);
-}
-
 double elapsed(cudaEvent_t a, cudaEvent_t b) {
   float ms = 0.f;
   if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) return 0.0;
@@ -35,10 +25,10 @@ void release(mc_dgraph *g) {
   cudaGetDevice(&prev);
   cudaSetDevice(g->device);
   if (g->stream) cudaStreamSynchronize(g->stream);
-  void *bufs[] = {g->rowptr,     g->col,        g->deg,      g->dplus,     g->dag_rowptr,
-                  g->dag_col,    g->prt_rowptr, g->prt_col,  g->tile_counts, g->tile_offsets,
+  void *bufs[] = {g->rowptr,     g->col,        g->key,      g->dag_rowptr,
+                  g->dag_col,    g->keep,       g->tile_counts, g->tile_offsets,
                   g->hub_cnt,    g->leaf_cnt,   g->hub_off,  g->leaf_off,  g->hub_tasks,
-                  g->leaf_tasks, g->scan_temp,  g->counters, g->err};
+                  g->leaf_tasks, g->scan_temp,  g->counters, g->err, g->pat_scratch};
   for (void *p : bufs)
     if (p) cudaFree(p);
   if (g->h_counters) cudaFreeHost(g->h_counters);
@@ -106,27 +96,23 @@ int tc_stats(mc_dgraph *g, mc_tc_stats_t *st) {
   st->n = g->n;
   st->nnz = g->nnz;
   if (!g->tc_ready || g->n == 0) return MC_OK;
-  int64_t v[4] = {0, 0, 0, 0};
-  const int64_t *src[4] = {g->dag_rowptr + g->n, g->prt_rowptr + g->n, g->hub_off + g->n,
-                           g->leaf_off + g->n};
-  for (int i = 0; i < 4; ++i)
+  int64_t v[3] = {0, 0, 0};
+  const int64_t *src[3] = {g->dag_rowptr + g->n, g->hub_off + g->n, g->leaf_off + g->n};
+  for (int i = 0; i < 3; ++i)
     MC_CUDA_TRY(cudaMemcpyAsync(&v[i], src[i], sizeof(int64_t), cudaMemcpyDeviceToHost, g->stream));
-  MC_CUDA_TRY(cudaMemsetAsync(g->counters + 4, 0, sizeof(unsigned long long), g->stream));
+  unsigned long long maxd = 0;
+  MC_CUDA_TRY(cudaMemcpyAsync(&maxd, g->counters + 3, sizeof(maxd), cudaMemcpyDeviceToHost,
+                              g->stream));
   MC_CUDA_TRY(cudaStreamSynchronize(g->stream));
-  if (v[1] > 0) {
-    probe_work_kernel<<<g->num_sms * 4, 256, 0, g->stream>>>(g->prt_col, g->dplus, v[1],
-                                                            g->counters + 4);
-    MC_CUDA_TRY(cudaGetLastError());
-  }
-  unsigned long long c[8];
-  MC_CUDA_TRY(cudaMemcpyAsync(c, g->counters, sizeof(c), cudaMemcpyDeviceToHost, g->stream));
-  MC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  unsigned long long pe = 0, work = 0;
+  const int rc = tc_partner_stats(g, &pe, &work);
+  if (rc != MC_OK) return rc;
   st->dag_edges = v[0];
-  st->partner_edges = v[1];
-  st->hub_tasks = v[2];
-  st->leaf_tasks = v[3];
-  st->max_out_degree = (int64_t)c[3];
-  st->probe_work = (double)c[4];
+  st->hub_tasks = v[1];
+  st->leaf_tasks = v[2];
+  st->partner_edges = (int64_t)pe;
+  st->max_out_degree = (int64_t)maxd;
+  st->probe_work = (double)work;
   return MC_OK;
 }
 

@@ -6,13 +6,13 @@
 
 // Tunables of the triangle-count schedule (task classes and chunk sizes).
 namespace mc {
-constexpr int kTileThreads = 256;          // threads per compaction tile
+constexpr int kTileThreads = 256;          // threads per orientation tile
 constexpr int kEdgesPerThread = 16;        // consecutive CSR entries per thread
 constexpr int64_t kTileEdges = (int64_t)kTileThreads * kEdgesPerThread;
 constexpr int kLeafMaxOut = 64;            // d+(owner) <= this: warp task
 constexpr int kLeafSlots = 256;            // per-warp hash slots for leaf owners
-constexpr int kHubChunk = 256;             // partners per CTA (hub) task
-constexpr int kLeafChunk = 64;             // partners per warp (leaf) task
+constexpr int kHubChunk = 512;             // owner's neighbours per CTA (hub) task
+constexpr int kLeafChunk = 64;             // owner's neighbours per warp (leaf) task
 constexpr int kCountThreads = 256;         // threads per counting CTA
 constexpr int kHubTableLog2Max = 15;       // at most 32768 slots (128 KB smem)
 }  // namespace mc
@@ -23,17 +23,20 @@ struct mc_dgraph {
   bool own_stream = false;
   int num_sms = 0;
   int64_t n = 0, nnz = 0;
+  int64_t max_degree = 0;     // set by validation on upload
   int64_t *rowptr = nullptr;  // n + 1
   int32_t *col = nullptr;     // nnz
 
+  // ---- pattern-count scratch (frontier lists), grown on demand ----------
+  void *pat_scratch = nullptr;
+  size_t pat_scratch_bytes = 0;
+
   // ---- triangle-count scratch, allocated on the first mc_tc_count -------
   bool tc_ready = false;
-  int32_t *deg = nullptr;         // n      symmetric degree
-  int32_t *dplus = nullptr;       // n      DAG out-degree
+  int2 *key = nullptr;            // n      {symmetric degree, DAG out-degree}
   int64_t *dag_rowptr = nullptr;  // n + 1
   int32_t *dag_col = nullptr;     // nnz (capacity; m+ used)
-  int64_t *prt_rowptr = nullptr;  // n + 1  owner -> partner lists
-  int32_t *prt_col = nullptr;     // nnz (capacity)
+  uint16_t *keep = nullptr;       // one DAG keep mask per orientation thread
   int32_t *tile_counts = nullptr; // tiles
   int64_t *tile_offsets = nullptr;// tiles + 1
   int32_t *hub_cnt = nullptr, *leaf_cnt = nullptr;      // n
@@ -42,7 +45,8 @@ struct mc_dgraph {
   int64_t task_capacity = 0;
   void *scan_temp = nullptr;
   size_t scan_temp_size = 0;
-  // 0: result, 1: hub queue, 2: leaf queue, 3: max d+, 4: probe work
+  // 0: result, 1: hub queue, 2: leaf queue, 3: max d+, 4: probe work,
+  // 5: partner edges, 7: max degree (validation)
   unsigned long long *counters = nullptr;
   unsigned *err = nullptr;
   // pinned host mirror of counters + err
@@ -51,7 +55,6 @@ struct mc_dgraph {
   int hub_table_log2 = 10;
   cudaEvent_t ev[6] = {};
   int64_t launches = 0;  // kernels launched by the current call
-  mc_tc_stats_t stats = {};
 };
 
 namespace mc {
@@ -59,6 +62,9 @@ namespace mc {
 int validate_graph(mc_dgraph *g, unsigned flags);
 int tc_alloc(mc_dgraph *g);
 int tc_orient(mc_dgraph *g);
+int tc_partner_stats(mc_dgraph *g, unsigned long long *partner_edges, unsigned long long *work);
 // tc.cu
 int tc_count_launch(mc_dgraph *g, cudaEvent_t after_hub, int shard, int num_shards);
+// patterns.cu: result of P<pattern>; c12 (optional) receives counters 1 and 2.
+int pattern_count(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12, mc_timing_t *timing);
 }  // namespace mc

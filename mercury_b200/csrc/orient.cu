@@ -1,6 +1,6 @@
-// Device preprocessing of the triangle-count path: contract validation,
-// degree-ordered DAG build and the owner->partner lists, all as streaming
-// row-aware compactions of the symmetric CSR.
+// Device preprocessing of the triangle-count path: contract validation and
+// the degree-ordered DAG, built by two streaming row-aware passes over the
+// symmetric CSR, plus the counting task queues.
 //
 // Reference behaviour restated here: Graph::orientation_with_division
 // (graph.cc:196-321) runs on the host with OpenMP in five passes.  The DAG
@@ -9,11 +9,17 @@
 // (DAG direction, both out-degrees <= 128) and a "large" CSR (REVERSE_DAG:
 // from the endpoint with the larger DAG out-degree, ties to the larger id,
 // graph.cc:238-263), skipping edges with an endpoint of out-degree 0
-// (graph.cc:246).  Here every DAG edge with both out-degrees >= 1 goes to the
-// owner list of its larger-out-degree end (the reference's "large" rule for
-// all edges), because the counting kernels always hash the owner's list and
-// stream the partner's shorter list; the small/large routing is made per
-// owner instead (d+ <= kLeafMaxOut: warp task, else CTA task).
+// (graph.cc:246).  Here every DAG edge with both out-degrees >= 1 belongs to
+// its larger-out-degree end (the reference's "large" rule for all edges);
+// the counting kernels find an owner's partners by filtering the owner's own
+// symmetric row, so no partner CSR is written.  Routing is per owner
+// (d+ <= kLeafMaxOut: warp task, else CTA task).
+//
+// Passes (each CTA owns a tile of kTileEdges consecutive CSR entries and
+// stages the tile's row offsets in shared memory):
+//   A  DAG keep masks, per-tile DAG counts, d+ of every row by atomics
+//   B  DAG entries and row offsets written from the keep masks
+// Each vertex's (degree, d+) pair is one 8-byte word (key[]).
 #include <algorithm>
 #include <cstdio>
 
@@ -24,29 +30,7 @@
 namespace mc {
 namespace {
 
-// ---- predicates over one CSR entry (v -> u) ------------------------------
-
-// Degree-ordered orientation: keep u in N+(v).
-struct DagPred {
-  const int32_t *deg;
-  __device__ __forceinline__ int32_t row_value(int64_t v) const { return __ldg(deg + v); }
-  __device__ __forceinline__ bool operator()(int64_t v, int32_t dv, int32_t u) const {
-    int32_t du = __ldg(deg + u);
-    return du > dv || (du == dv && u > (int32_t)v);
-  }
-};
-
-// Owner rule: the end with the larger DAG out-degree owns the edge (ties to
-// the larger id); edges touching an out-degree-0 end are dropped.
-struct OwnerPred {
-  const int32_t *dplus;
-  __device__ __forceinline__ int32_t row_value(int64_t v) const { return __ldg(dplus + v); }
-  __device__ __forceinline__ bool operator()(int64_t v, int32_t pv, int32_t u) const {
-    if (pv < 1) return false;
-    int32_t pu = __ldg(dplus + u);
-    return pu >= 1 && (pv > pu || (pv == pu && (int32_t)v > u));
-  }
-};
+constexpr int kSegMax = 2048;  // row offsets of a tile kept in shared memory
 
 __device__ __forceinline__ void load_span(const int32_t *__restrict__ col, int64_t s, int64_t nnz,
                                           int32_t (&vals)[kEdgesPerThread]) {
@@ -66,15 +50,48 @@ __device__ __forceinline__ void load_span(const int32_t *__restrict__ col, int64
   }
 }
 
-// Row range [lo, hi] that covers the CSR entries of this tile.
-__device__ __forceinline__ void tile_rows(const int64_t *rowptr, int64_t n, int64_t t0, int64_t t1,
-                                          int64_t *lo, int64_t *hi) {
+// Row offsets of one tile: rows [lo, hi] hold the tile's entries; when the
+// segment rowptr[lo .. hi+1] fits it is read from shared memory.
+struct TileRows {
+  const int64_t *g;
+  const int64_t *s;
+  int64_t lo, hi;
+  __device__ __forceinline__ int64_t at(int64_t r) const { return s ? s[r - lo] : __ldg(g + r); }
+  // Largest r in [lo, hi] with rowptr[r] <= key.
+  __device__ __forceinline__ int64_t row_of(int64_t key) const {
+    int64_t a = lo, b = hi;
+    while (a < b) {
+      int64_t mid = a + ((b - a + 1) >> 1);
+      if (at(mid) <= key) a = mid;
+      else b = mid - 1;
+    }
+    return a;
+  }
+  // Smallest r in [a, b] with rowptr[r] >= key (rowptr[b] >= key).
+  __device__ __forceinline__ int64_t first_at(int64_t a, int64_t b, int64_t key) const {
+    while (a < b) {
+      int64_t mid = a + ((b - a) >> 1);
+      if (at(mid) >= key) b = mid;
+      else a = mid + 1;
+    }
+    return a;
+  }
+};
+
+__device__ __forceinline__ TileRows load_tile_rows(const int64_t *rowptr, int64_t n, int64_t t0,
+                                                   int64_t t1, int64_t *seg) {
   __shared__ int64_t sh[2];
   if (threadIdx.x == 0) sh[0] = upper_row(rowptr, 0, n - 1, t0);
   if (threadIdx.x == kTileThreads - 1) sh[1] = upper_row(rowptr, 0, n - 1, t1 - 1);
   __syncthreads();
-  *lo = sh[0];
-  *hi = sh[1];
+  TileRows tr{rowptr, nullptr, sh[0], sh[1]};
+  const int64_t len = tr.hi - tr.lo + 2;
+  if (len <= kSegMax) {
+    for (int64_t i = threadIdx.x; i < len; i += kTileThreads) seg[i] = __ldg(rowptr + tr.lo + i);
+    __syncthreads();
+    tr.s = seg;
+  }
+  return tr;
 }
 
 __device__ __forceinline__ int block_sum_int(int v) {
@@ -90,7 +107,8 @@ __device__ __forceinline__ int block_sum_int(int v) {
   return t;
 }
 
-__device__ __forceinline__ int block_exclusive_int(int v) {
+// Exclusive prefix of v over the block; *total receives the block sum.
+__device__ __forceinline__ int block_exclusive_int(int v, int *total) {
   __shared__ int ws[kTileThreads / kWarp];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   int x = warp_inclusive_scan(v, lane);
@@ -102,59 +120,25 @@ __device__ __forceinline__ int block_exclusive_int(int v) {
     if (lane < kTileThreads / kWarp) ws[lane] = w;
   }
   __syncthreads();
+  *total = ws[kTileThreads / kWarp - 1];
   return (wid ? ws[wid - 1] : 0) + x - v;
 }
 
-// Pass 1 (kWrite == false): tile_counts[tile] = kept entries in the tile.
-// Pass 2 (kWrite == true): stable compaction of the kept entries into
-// out_col and out_rowptr[r] = kept entries before rowptr[r], for every row.
-template <class Pred, bool kWrite>
-__global__ void __launch_bounds__(kTileThreads)
-    compact_kernel(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ col, int64_t n,
-                   int64_t nnz, Pred pred, int32_t *tile_counts, const int64_t *tile_offsets,
-                   int64_t *out_rowptr, int32_t *out_col) {
-  const int64_t t0 = (int64_t)blockIdx.x * kTileEdges;
-  const int64_t t1 = min(t0 + kTileEdges, nnz);
-  int64_t rlo, rhi;
-  tile_rows(rowptr, n, t0, t1, &rlo, &rhi);
-  const int64_t s = t0 + (int64_t)threadIdx.x * kEdgesPerThread;
-  const int64_t e_end = min(s + kEdgesPerThread, t1);
-  int32_t vals[kEdgesPerThread];
-  unsigned keep = 0;
-  int64_t r = 0;
-  if (s < t1) {
-    load_span(col, s, nnz, vals);
-    r = upper_row(rowptr, rlo, rhi, s);
-    int64_t next = __ldg(rowptr + r + 1);
-    int64_t v = r;
-    int32_t pv = pred.row_value(v);
-#pragma unroll
-    for (int k = 0; k < kEdgesPerThread; ++k) {
-      const int64_t e = s + k;
-      if (e < e_end) {
-        while (e == next) {
-          ++v;
-          next = __ldg(rowptr + v + 1);
-          pv = pred.row_value(v);
-        }
-        if (pred(v, pv, vals[k])) keep |= 1u << k;
-      }
-    }
-  }
-  const int cnt = __popc(keep);
-  if (!kWrite) {
-    int t = block_sum_int(cnt);
-    if (threadIdx.x == 0) tile_counts[blockIdx.x] = t;
-    return;
-  }
-  int64_t pos = tile_offsets[blockIdx.x] + block_exclusive_int(cnt);
-  if (s >= t1) return;
-  // Rows that start exactly at s (empty rows before r included) start here.
-  if (__ldg(rowptr + r) == s) {
-    int64_t rf = lower_row(rowptr, 0, r, s);
+// Writes the kept entries of this thread's span [s, e_end) (row r holds s)
+// from position pos on, and out_rowptr[q] = position for every row q that
+// starts inside the span.  Rows starting at nnz are written by the caller.
+__device__ __forceinline__ void write_span(const TileRows &tr, const int64_t *rowptr, int64_t t0,
+                                           int64_t s, int64_t e_end, int64_t r,
+                                           const int32_t (&vals)[kEdgesPerThread], unsigned keep,
+                                           int64_t pos, int64_t *out_rowptr, int32_t *out_col) {
+  if (tr.at(r) == s) {
+    // Rows starting exactly at s: row r and the empty rows just before it.
+    // For s > t0 they all lie in the staged range; the tile's first span may
+    // share its start with rows before the range.
+    const int64_t rf = s == t0 ? lower_row(rowptr, 0, r, s) : tr.first_at(tr.lo, r, s);
     for (int64_t q = rf; q <= r; ++q) out_rowptr[q] = pos;
   }
-  int64_t next = __ldg(rowptr + r + 1);
+  int64_t next = tr.at(r + 1);
 #pragma unroll
   for (int k = 0; k < kEdgesPerThread; ++k) {
     const int64_t e = s + k;
@@ -162,14 +146,78 @@ __global__ void __launch_bounds__(kTileThreads)
       while (e == next) {
         ++r;
         out_rowptr[r] = pos;
-        next = __ldg(rowptr + r + 1);
+        next = tr.at(r + 1);
       }
       if (keep & (1u << k)) out_col[pos++] = vals[k];
     }
   }
-  // Rows that start at nnz (trailing empty rows and r == n) get the total.
-  if (e_end == nnz)
-    for (int64_t q = r + 1; q <= n; ++q) out_rowptr[q] = pos;
+}
+
+// Pass A (kWrite == false): DAG entries of every thread's span as a 16-bit
+// mask in keep[], per-tile counts, and d+ of every row by atomics on
+// key[].y (which starts at 0).  Pass B (kWrite == true): the kept entries
+// compacted into out_col and out_rowptr[r] = kept entries before rowptr[r].
+template <bool kWrite>
+__global__ void __launch_bounds__(kTileThreads)
+    dag_pass_kernel(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ col,
+                    int64_t n, int64_t nnz, int2 *key, uint16_t *keep_masks, int32_t *counts_out,
+                    const int64_t *__restrict__ offs_in, int64_t *out_rowptr, int32_t *out_col) {
+  __shared__ int64_t seg[kSegMax];
+  const int64_t t0 = (int64_t)blockIdx.x * kTileEdges;
+  const int64_t t1 = min(t0 + kTileEdges, nnz);
+  const TileRows tr = load_tile_rows(rowptr, n, t0, t1, seg);
+  const int64_t s = t0 + (int64_t)threadIdx.x * kEdgesPerThread;
+  const int64_t e_end = min(s + kEdgesPerThread, t1);
+  const int64_t slot = (int64_t)blockIdx.x * kTileThreads + threadIdx.x;
+  int32_t vals[kEdgesPerThread];
+  unsigned keep = 0;
+  int64_t r = 0;
+  if (s < t1) {
+    load_span(col, s, nnz, vals);
+    r = tr.row_of(s);
+    if (!kWrite) {
+      int64_t v = r, next = tr.at(r + 1);
+      int dv = key[v].x;
+      int run = 0;  // DAG entries of row v seen in this span
+#pragma unroll
+      for (int k = 0; k < kEdgesPerThread; ++k) {
+        const int64_t e = s + k;
+        if (e < e_end) {
+          while (e == next) {
+            if (run) {
+              atomicAdd(&key[v].y, run);
+              run = 0;
+            }
+            ++v;
+            next = tr.at(v + 1);
+            dv = key[v].x;
+          }
+          const int u = vals[k];
+          const int du = key[u].x;
+          if (du > dv || (du == dv && u > (int)v)) {
+            keep |= 1u << k;
+            ++run;
+          }
+        }
+      }
+      if (run) atomicAdd(&key[v].y, run);
+      keep_masks[slot] = (uint16_t)keep;
+    } else {
+      keep = keep_masks[slot];
+    }
+  }
+  if (!kWrite) {
+    const int t = block_sum_int(__popc(keep));
+    if (threadIdx.x == 0) counts_out[blockIdx.x] = t;
+    return;
+  }
+  int total = 0;
+  const int64_t base = offs_in[blockIdx.x];
+  const int64_t pos = base + block_exclusive_int(__popc(keep), &total);
+  if (s < t1) write_span(tr, rowptr, t0, s, e_end, r, vals, keep, pos, out_rowptr, out_col);
+  // Rows after the last entry (trailing empty rows and q == n) start at nnz.
+  if (t1 == nnz)
+    for (int64_t q = tr.hi + 1 + threadIdx.x; q <= n; q += kTileThreads) out_rowptr[q] = base + total;
 }
 
 // Contract checks that need the row of each entry: ids in range, strictly
@@ -177,21 +225,21 @@ __global__ void __launch_bounds__(kTileThreads)
 __global__ void __launch_bounds__(kTileThreads)
     validate_entries_kernel(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ col,
                             int64_t n, int64_t nnz, int check_sym, unsigned *err) {
+  __shared__ int64_t seg[kSegMax];
   const int64_t t0 = (int64_t)blockIdx.x * kTileEdges;
   const int64_t t1 = min(t0 + kTileEdges, nnz);
-  int64_t rlo, rhi;
-  tile_rows(rowptr, n, t0, t1, &rlo, &rhi);
+  const TileRows tr = load_tile_rows(rowptr, n, t0, t1, seg);
   const int64_t s = t0 + (int64_t)threadIdx.x * kEdgesPerThread;
   const int64_t e_end = min(s + kEdgesPerThread, t1);
   if (s >= t1) return;
-  int64_t v = upper_row(rowptr, rlo, rhi, s);
-  int64_t start = __ldg(rowptr + v), next = __ldg(rowptr + v + 1);
+  int64_t v = tr.row_of(s);
+  int64_t start = tr.at(v), next = tr.at(v + 1);
   unsigned bad = 0;
   for (int64_t e = s; e < e_end; ++e) {
     while (e == next) {
       ++v;
       start = next;
-      next = __ldg(rowptr + v + 1);
+      next = tr.at(v + 1);
     }
     const int32_t u = __ldg(col + e);
     if (u < 0 || (int64_t)u >= n) {
@@ -207,8 +255,12 @@ __global__ void __launch_bounds__(kTileThreads)
       while (lo <= hi && lo >= 0 && hi < nnz) {
         int64_t mid = lo + ((hi - lo) >> 1);
         int32_t m = __ldg(col + mid);
-        if (m == (int32_t)v) { found = true; break; }
-        if (m < (int32_t)v) lo = mid + 1; else hi = mid - 1;
+        if (m == (int32_t)v) {
+          found = true;
+          break;
+        }
+        if (m < (int32_t)v) lo = mid + 1;
+        else hi = mid - 1;
       }
       if (!found) bad |= kErrAsymmetric;
     }
@@ -216,48 +268,53 @@ __global__ void __launch_bounds__(kTileThreads)
   if (bad) atomicOr(err, bad);
 }
 
-__global__ void validate_rowptr_kernel(const int64_t *rowptr, int64_t n, int64_t nnz, unsigned *err) {
+// Offsets monotone with the right ends; *max_deg receives the largest row.
+__global__ void validate_rowptr_kernel(const int64_t *rowptr, int64_t n, int64_t nnz,
+                                       unsigned *err, unsigned long long *max_deg) {
   const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (v > n) return;
-  const int64_t a = rowptr[v];
-  bool bad = (v == 0 && a != 0) || (v == n && a != nnz) || a < 0 || a > nnz;
-  if (v < n && rowptr[v + 1] < a) bad = true;
-  if (bad) atomicOr(err, (unsigned)kErrRowptr);
+  long long d = 0;
+  if (v <= n) {
+    const int64_t a = rowptr[v];
+    bool bad = (v == 0 && a != 0) || (v == n && a != nnz) || a < 0 || a > nnz;
+    if (v < n) {
+      d = rowptr[v + 1] - a;
+      if (d < 0) bad = true;
+    }
+    if (bad) atomicOr(err, (unsigned)kErrRowptr);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) d = max(d, __shfl_down_sync(kFull, d, o));
+  if ((threadIdx.x & 31) == 0 && d > 0) atomicMax(max_deg, (unsigned long long)d);
 }
 
-__global__ void degree_kernel(const int64_t *rowptr, int64_t n, int32_t *deg) {
+__global__ void init_key_kernel(const int64_t *rowptr, int64_t n, int2 *key) {
   const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (v < n) deg[v] = (int32_t)(rowptr[v + 1] - rowptr[v]);
+  if (v < n) key[v] = make_int2((int)(rowptr[v + 1] - rowptr[v]), 0);
 }
 
-__global__ void dplus_kernel(const int64_t *dag_rowptr, int64_t n, int32_t *dplus,
-                             unsigned long long *max_out) {
+// Tasks each owner contributes to the hub and leaf queues (chunks of its
+// symmetric row), and the largest DAG out-degree.
+__global__ void task_count_kernel(const int2 *key, int64_t n, int32_t *hub_cnt,
+                                  int32_t *leaf_cnt, unsigned long long *max_out) {
   const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   int32_t d = 0;
   if (v < n) {
-    d = (int32_t)(dag_rowptr[v + 1] - dag_rowptr[v]);
-    dplus[v] = d;
+    const int2 kv = key[v];
+    d = kv.y;
+    int32_t h = 0, l = 0;
+    // Owners need d+ >= 1 and a neighbour outside their own out-list
+    // (a partner has d+ <= d+(owner), so an owner with deg == d+ may still
+    // own out-edges: every neighbour counts).
+    if (d >= 1) {
+      if (d > kLeafMaxOut) h = (kv.x + kHubChunk - 1) / kHubChunk;
+      else l = (kv.x + kLeafChunk - 1) / kLeafChunk;
+    }
+    hub_cnt[v] = h;
+    leaf_cnt[v] = l;
   }
-  // Warp max, then one atomic per warp.
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) d = max(d, __shfl_down_sync(kFull, d, o));
   if ((threadIdx.x & 31) == 0 && d > 0) atomicMax(max_out, (unsigned long long)d);
-}
-
-// Number of tasks each owner contributes to the hub and leaf queues.
-__global__ void task_count_kernel(const int64_t *prt_rowptr, const int32_t *dplus, int64_t n,
-                                  int32_t *hub_cnt, int32_t *leaf_cnt) {
-  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= n) return;
-  const int64_t p = prt_rowptr[v + 1] - prt_rowptr[v];
-  const int32_t d = dplus[v];
-  int32_t h = 0, l = 0;
-  if (p > 0) {
-    if (d > kLeafMaxOut) h = (int32_t)((p + kHubChunk - 1) / kHubChunk);
-    else l = (int32_t)((p + kLeafChunk - 1) / kLeafChunk);
-  }
-  hub_cnt[v] = h;
-  leaf_cnt[v] = l;
 }
 
 // Task word: owner id in the high half, chunk index in the low half.
@@ -271,38 +328,49 @@ __global__ void task_fill_kernel(const int32_t *hub_cnt, const int64_t *hub_off,
   for (int32_t c = 0, l = leaf_cnt[v]; c < l; ++c) leaf_tasks[leaf_off[v] + c] = hi | (uint32_t)c;
 }
 
-unsigned grid_for(int64_t items, int threads) {
-  return (unsigned)std::max<int64_t>(1, (items + threads - 1) / threads);
+// Partner edges (owner rule) and their streamed-list work, for statistics.
+__global__ void partner_stats_kernel(const int64_t *rowptr, const int32_t *col, const int2 *key,
+                                     int64_t n, unsigned long long *out) {
+  unsigned long long pe = 0, work = 0;
+  for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n;
+       x += (int64_t)gridDim.x * blockDim.x) {
+    const int px = key[x].y;
+    if (px < 1) continue;
+    for (int64_t e = rowptr[x]; e < rowptr[x + 1]; ++e) {
+      const int y = col[e];
+      const int py = key[y].y;
+      if (py >= 1 && (px > py || (px == py && (int)x > y))) {
+        ++pe;
+        work += (unsigned long long)py;
+      }
+    }
+  }
+  pe = warp_sum_u64(pe);
+  work = warp_sum_u64(work);
+  if ((threadIdx.x & 31) == 0) {
+    if (pe) atomicAdd(out, pe);
+    if (work) atomicAdd(out + 1, work);
+  }
 }
 
-template <class Pred>
-int compact(mc_dgraph *g, Pred pred, int64_t *out_rowptr, int32_t *out_col) {
-  const int64_t tiles = (g->nnz + kTileEdges - 1) / kTileEdges;
-  if (tiles == 0) {
-    MC_CUDA_TRY(cudaMemsetAsync(out_rowptr, 0, sizeof(int64_t) * (g->n + 1), g->stream));
-    return MC_OK;
-  }
-  g->launches += 2 + scan_launches(tiles);
-  compact_kernel<Pred, false><<<(unsigned)tiles, kTileThreads, 0, g->stream>>>(
-      g->rowptr, g->col, g->n, g->nnz, pred, g->tile_counts, nullptr, nullptr, nullptr);
-  MC_CUDA_TRY(cudaGetLastError());
-  MC_CUDA_TRY(exclusive_scan(g->tile_counts, g->tile_offsets, tiles, g->scan_temp, g->stream));
-  compact_kernel<Pred, true><<<(unsigned)tiles, kTileThreads, 0, g->stream>>>(
-      g->rowptr, g->col, g->n, g->nnz, pred, nullptr, g->tile_offsets, out_rowptr, out_col);
-  MC_CUDA_TRY(cudaGetLastError());
-  return MC_OK;
+unsigned grid_for(int64_t items, int threads) {
+  return (unsigned)std::max<int64_t>(1, (items + threads - 1) / threads);
 }
 
 }  // namespace
 
 int validate_graph(mc_dgraph *g, unsigned flags) {
   MC_CUDA_TRY(cudaMemsetAsync(g->err, 0, sizeof(unsigned), g->stream));
-  validate_rowptr_kernel<<<grid_for(g->n + 1, 256), 256, 0, g->stream>>>(g->rowptr, g->n, g->nnz,
-                                                                        g->err);
+  MC_CUDA_TRY(cudaMemsetAsync(g->counters + 7, 0, sizeof(unsigned long long), g->stream));
+  validate_rowptr_kernel<<<grid_for(g->n + 1, 256), 256, 0, g->stream>>>(
+      g->rowptr, g->n, g->nnz, g->err, g->counters + 7);
   MC_CUDA_TRY(cudaGetLastError());
   MC_CUDA_TRY(cudaMemcpyAsync(g->h_err, g->err, sizeof(unsigned), cudaMemcpyDeviceToHost, g->stream));
+  MC_CUDA_TRY(cudaMemcpyAsync(g->h_counters + 7, g->counters + 7, sizeof(unsigned long long),
+                              cudaMemcpyDeviceToHost, g->stream));
   MC_CUDA_TRY(cudaStreamSynchronize(g->stream));
   if (*g->h_err) return MC_ERR_FORMAT;  // the entry walk needs monotone offsets
+  g->max_degree = (int64_t)g->h_counters[7];
   const int64_t tiles = (g->nnz + kTileEdges - 1) / kTileEdges;
   g->launches += 1 + (tiles > 0 ? 1 : 0);
   if (tiles > 0) {
@@ -319,16 +387,14 @@ int tc_alloc(mc_dgraph *g) {
   if (g->tc_ready) return MC_OK;
   const int64_t n = g->n, cap = std::max<int64_t>(g->nnz, 1);
   const int64_t tiles = std::max<int64_t>((g->nnz + kTileEdges - 1) / kTileEdges, 1);
-  // Each owner contributes at most ceil(p / chunk) <= 1 + p / chunk tasks.
+  // Each owner contributes ceil(deg / chunk) <= 1 + deg / chunk tasks.
   g->task_capacity = n + cap / std::min(kHubChunk, kLeafChunk) + 1;
   g->scan_temp_size = std::max(scan_temp_bytes(n + 1), scan_temp_bytes(tiles + 1));
 #define MC_ALLOC(ptr, count) MC_CUDA_TRY(cudaMalloc((void **)&(ptr), sizeof(*(ptr)) * (size_t)(count)))
-  MC_ALLOC(g->deg, n + 1);
-  MC_ALLOC(g->dplus, n + 1);
+  MC_ALLOC(g->key, n + 1);
   MC_ALLOC(g->dag_rowptr, n + 1);
   MC_ALLOC(g->dag_col, cap);
-  MC_ALLOC(g->prt_rowptr, n + 1);
-  MC_ALLOC(g->prt_col, cap);
+  MC_ALLOC(g->keep, tiles * kTileThreads);
   MC_ALLOC(g->tile_counts, tiles);
   MC_ALLOC(g->tile_offsets, tiles + 1);
   MC_ALLOC(g->hub_cnt, n + 1);
@@ -344,27 +410,53 @@ int tc_alloc(mc_dgraph *g) {
 }
 
 int tc_orient(mc_dgraph *g) {
-  const int64_t n = g->n;
+  const int64_t n = g->n, nnz = g->nnz;
   cudaStream_t s = g->stream;
-  MC_CUDA_TRY(cudaMemsetAsync(g->counters, 0, sizeof(unsigned long long) * 8, s));
+  MC_CUDA_TRY(cudaMemsetAsync(g->counters, 0, sizeof(unsigned long long) * 7, s));
   if (n == 0) return MC_OK;
-  g->launches += 4 + 2 * scan_launches(n);  // degree, d+, task count/fill, 2 scans
-  degree_kernel<<<grid_for(n, 256), 256, 0, s>>>(g->rowptr, n, g->deg);
+  const int64_t tiles = (nnz + kTileEdges - 1) / kTileEdges;
+  init_key_kernel<<<grid_for(n, 256), 256, 0, s>>>(g->rowptr, n, g->key);
   MC_CUDA_TRY(cudaGetLastError());
-  int rc = compact(g, DagPred{g->deg}, g->dag_rowptr, g->dag_col);
-  if (rc != MC_OK) return rc;
-  dplus_kernel<<<grid_for(n, 256), 256, 0, s>>>(g->dag_rowptr, n, g->dplus, g->counters + 3);
-  MC_CUDA_TRY(cudaGetLastError());
-  rc = compact(g, OwnerPred{g->dplus}, g->prt_rowptr, g->prt_col);
-  if (rc != MC_OK) return rc;
-  task_count_kernel<<<grid_for(n, 256), 256, 0, s>>>(g->prt_rowptr, g->dplus, n, g->hub_cnt,
-                                                     g->leaf_cnt);
+  g->launches += 1;
+  if (tiles == 0) {
+    MC_CUDA_TRY(cudaMemsetAsync(g->dag_rowptr, 0, sizeof(int64_t) * (n + 1), s));
+  } else {
+    const unsigned grid = (unsigned)tiles;
+    dag_pass_kernel<false><<<grid, kTileThreads, 0, s>>>(g->rowptr, g->col, n, nnz, g->key,
+                                                         g->keep, g->tile_counts, nullptr,
+                                                         nullptr, nullptr);
+    MC_CUDA_TRY(cudaGetLastError());
+    MC_CUDA_TRY(exclusive_scan(g->tile_counts, g->tile_offsets, tiles, g->scan_temp, s));
+    dag_pass_kernel<true><<<grid, kTileThreads, 0, s>>>(g->rowptr, g->col, n, nnz, g->key,
+                                                        g->keep, nullptr, g->tile_offsets,
+                                                        g->dag_rowptr, g->dag_col);
+    MC_CUDA_TRY(cudaGetLastError());
+    g->launches += 2 + scan_launches(tiles);
+  }
+  task_count_kernel<<<grid_for(n, 256), 256, 0, s>>>(g->key, n, g->hub_cnt, g->leaf_cnt,
+                                                     g->counters + 3);
   MC_CUDA_TRY(cudaGetLastError());
   MC_CUDA_TRY(exclusive_scan(g->hub_cnt, g->hub_off, n, g->scan_temp, s));
   MC_CUDA_TRY(exclusive_scan(g->leaf_cnt, g->leaf_off, n, g->scan_temp, s));
   task_fill_kernel<<<grid_for(n, 256), 256, 0, s>>>(g->hub_cnt, g->hub_off, g->leaf_cnt,
                                                     g->leaf_off, n, g->hub_tasks, g->leaf_tasks);
   MC_CUDA_TRY(cudaGetLastError());
+  g->launches += 2 + 2 * scan_launches(n);
+  return MC_OK;
+}
+
+int tc_partner_stats(mc_dgraph *g, unsigned long long *partner_edges, unsigned long long *work) {
+  *partner_edges = *work = 0;
+  if (!g->tc_ready || g->n == 0) return MC_OK;
+  MC_CUDA_TRY(cudaMemsetAsync(g->counters + 4, 0, sizeof(unsigned long long) * 2, g->stream));
+  partner_stats_kernel<<<g->num_sms * 8, 256, 0, g->stream>>>(g->rowptr, g->col, g->key, g->n,
+                                                              g->counters + 4);
+  MC_CUDA_TRY(cudaGetLastError());
+  unsigned long long c[2];
+  MC_CUDA_TRY(cudaMemcpyAsync(c, g->counters + 4, sizeof(c), cudaMemcpyDeviceToHost, g->stream));
+  MC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  *partner_edges = c[0];
+  *work = c[1];
   return MC_OK;
 }
 

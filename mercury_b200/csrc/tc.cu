@@ -1,9 +1,10 @@
 // Triangle-count kernels.  count = sum over DAG edges {x, y} of
 // |N+(x) & N+(y)|, where x is the edge's owner (larger d+, ties to the larger
-// id) and y its partner.  Both kernels put N+(owner) into a shared-memory
-// open-addressing table once per task and stream the partners' (shorter)
-// lists through it, 32 list entries per warp step with the lanes flattened
-// across partner boundaries.
+// id) and y its partner.  A task is (owner, chunk of the owner's symmetric
+// row): N+(owner) goes into a shared-memory open-addressing table, the
+// chunk's neighbours are filtered down to partners (owner rule on d+), and
+// each partner's list N+(y) -- never longer than N+(owner) -- is streamed
+// through the table.
 //
 // Reference counterparts: hashIndex_for_large_degree (CTA per large vertex,
 // 1019-bin hash staged through a 256 MiB global scratch,
@@ -11,7 +12,7 @@
 // (warp per small vertex, binary search in shared memory,
 // gpu_kernels/tc_challenge.cuh:195-303), each with an atomic work counter
 // (DYNAMIC_MODE, gpu_kernels/tuning_schedules.cuh:1-21).  Here the queues hold
-// bounded (owner, partner-chunk) tasks, the tables live in shared memory only,
+// bounded (owner, row-chunk) tasks, the tables live in shared memory only,
 // and the hash needs no global scratch.
 #include <algorithm>
 
@@ -21,11 +22,14 @@
 namespace mc {
 namespace {
 
+constexpr int kClaim = 16;  // owner-row entries a hub warp claims at a time
+
 struct CountArgs {
-  const int64_t *__restrict__ dag_rowptr;
+  const int64_t *__restrict__ rowptr;      // symmetric CSR
+  const int32_t *__restrict__ col;
+  const int2 *__restrict__ key;            // {deg, d+}
+  const int64_t *__restrict__ dag_rowptr;  // N+ lists
   const int32_t *__restrict__ dag_col;
-  const int64_t *__restrict__ prt_rowptr;
-  const int32_t *__restrict__ prt_col;
   const uint64_t *__restrict__ tasks;
   const int64_t *__restrict__ ntasks;  // device scalar (end of the offsets)
   unsigned long long *queue;
@@ -44,21 +48,24 @@ __device__ __forceinline__ uint64_t shard_task(const CountArgs &a, unsigned long
   return a.tasks[(int64_t)t * a.num_shards + a.shard];
 }
 
-// Probe of an open-addressing table (empty slot = -1, linear probing).
+// Probe of an open-addressing table (empty slot = -1, linear probing).  The
+// tables are filled to at most half, so a probe meets an empty slot; the
+// bound only guards against a corrupted table.
 struct TableProbe {
   const int *tab;
   unsigned mask;
   int shift;
-  __device__ __forceinline__ int operator()(int w) const {
+  __device__ __forceinline__ unsigned operator()(int w) const {
     unsigned h = hash_slot(w, shift);
+    int t = tab[h];
+    if (t == w) return 1u;
 #pragma unroll 1
-    for (unsigned it = 0; it <= mask; ++it) {
-      const int t = tab[h];
-      if (t == w) return 1;
-      if (t < 0) return 0;
+    for (unsigned it = 0; t >= 0 && it < mask; ++it) {
       h = (h + 1) & mask;
+      t = tab[h];
+      if (t == w) return 1u;
     }
-    return 0;
+    return 0u;
   }
 };
 
@@ -66,15 +73,15 @@ struct TableProbe {
 struct ListProbe {
   const int32_t *list;
   int len;
-  __device__ __forceinline__ int operator()(int w) const {
+  __device__ __forceinline__ unsigned operator()(int w) const {
     int lo = 0, hi = len - 1;
     while (lo <= hi) {
       int mid = (lo + hi) >> 1;
       int m = __ldg(list + mid);
-      if (m == w) return 1;
+      if (m == w) return 1u;
       if (m < w) lo = mid + 1; else hi = mid - 1;
     }
-    return 0;
+    return 0u;
   }
 };
 
@@ -92,38 +99,94 @@ __device__ __forceinline__ void table_insert(int *tab, unsigned mask, int shift,
   }
 }
 
-// Streams the partner lists of partners [q0, q1) (batches of 32 partners
-// starting at q0 + 32*first, stepping by 32*step) through `probe`.  Within a
-// batch the 32 lanes walk the concatenated lists 32 entries at a time: lane L
-// of window F handles flat entry F + L, and the partner that entry belongs to
-// comes from the bit mask of partner starts inside the window.
+// Partner test for neighbour y of owner x (px = d+(x), py = d+(y)).
+__device__ __forceinline__ bool owns(int x, int px, int y, int py) {
+  return py >= 1 && (px > py || (px == py && x > y));
+}
+
+// One warp streams one list col[st, st+len) through `probe`: 8-byte loads
+// (two probes per lane) with a scalar head/tail for odd ends.  Returns this
+// lane's hits.
 template <class Probe>
-__device__ __forceinline__ unsigned long long stream_partners(const CountArgs &a, int64_t q0,
-                                                              int64_t q1, int first, int step,
-                                                              int lane, const Probe &probe) {
+__device__ __forceinline__ unsigned stream_list(const int32_t *__restrict__ col, int64_t st,
+                                                int len, int lane, const Probe &probe) {
+  unsigned hits = 0;
+  const int head = (int)(st & 1) & (len > 0 ? 1 : 0);
+  if (lane == 0 && head) hits += probe(__ldg(col + st));
+  const int64_t a = st + head;
+  const int rest = len - head;
+  const int body = rest >> 1;
+  const int2 *v = reinterpret_cast<const int2 *>(col + a);
+  for (int k = lane; k < body; k += kWarp) {
+    const int2 q = __ldg(v + k);
+    hits += probe(q.x) + probe(q.y);
+  }
+  if (lane == 0 && (rest & 1)) hits += probe(__ldg(col + a + 2 * body));
+  return hits;
+}
+
+// Entries [e0, e0 + nc) of owner x's symmetric row, claimed by the CTA's warps
+// kClaim at a time from the shared counter *next; each claimed neighbour that
+// is a partner has its list streamed by the whole warp.
+template <class Probe>
+__device__ __forceinline__ unsigned long long claim_and_stream(const CountArgs &a, int x, int px,
+                                                               int64_t e0, int nc, int *next,
+                                                               int lane, const Probe &probe) {
   unsigned long long hits = 0;
-  for (int64_t qb = q0 + (int64_t)kWarp * first; qb < q1; qb += (int64_t)kWarp * step) {
-    const int64_t q = qb + lane;
-    const bool valid = q < q1;
-    const int y = valid ? __ldg(a.prt_col + q) : 0;
-    const int64_t st = valid ? __ldg(a.dag_rowptr + y) : 0;
-    const int len = valid ? (int)(__ldg(a.dag_rowptr + y + 1) - st) : 0;
-    const int incl = warp_inclusive_scan(len, lane);
-    const int excl = incl - len;
-    const int total = __shfl_sync(kFull, incl, kWarp - 1);
-    const unsigned upto = lane == kWarp - 1 ? kFull : ((2u << lane) - 1u);
-    int base = 0;
-    for (int F = 0; F < total; F += kWarp) {
-      const unsigned bit =
-          (len > 0 && excl >= F && excl < F + kWarp) ? (1u << (excl - F)) : 0u;
-      const unsigned starts = __reduce_or_sync(kFull, bit);
-      const int p = max(base + __popc(starts & upto) - 1, 0);
-      const int64_t pst = __shfl_sync(kFull, st, p);
-      const int pex = __shfl_sync(kFull, excl, p);
-      const int f = F + lane;
-      if (f < total) hits += probe(__ldg(a.dag_col + pst + (f - pex)));
-      base += __popc(starts);
+  for (;;) {
+    int g = 0;
+    if (lane == 0) g = atomicAdd(next, kClaim);
+    g = __shfl_sync(kFull, g, 0);
+    if (g >= nc) break;
+    bool part = false;
+    int64_t st = 0;
+    int len = 0;
+    if (lane < kClaim && g + lane < nc) {
+      const int y = __ldg(a.col + e0 + g + lane);
+      const int py = __ldg(&a.key[y].y);
+      if (owns(x, px, y, py)) {
+        part = true;
+        st = __ldg(a.dag_rowptr + y);
+        len = py;
+      }
     }
+    unsigned m = __ballot_sync(kFull, part);
+    unsigned h = 0;
+    while (m) {
+      const int p = __ffs(m) - 1;
+      m &= m - 1;
+      const int64_t s = __shfl_sync(kFull, st, p);
+      const int l = __shfl_sync(kFull, len, p);
+      h += stream_list(a.dag_col, s, l, lane, probe);
+    }
+    hits += h;
+  }
+  return hits;
+}
+
+// Short lists: lanes 0..k-1 hold one non-empty list each (st, len; the other
+// lanes len 0) and the warp walks the concatenated lists 32 entries at a
+// time; lane L of window F handles flat entry F + L, whose list is found by
+// counting the list starts inside the window.
+template <class Probe>
+__device__ __forceinline__ unsigned long long stream_flat(const int32_t *__restrict__ col,
+                                                          int64_t st, int len, int lane,
+                                                          const Probe &probe) {
+  unsigned long long hits = 0;
+  const int incl = warp_inclusive_scan(len, lane);
+  const int excl = incl - len;
+  const int total = __shfl_sync(kFull, incl, kWarp - 1);
+  const unsigned upto = lane == kWarp - 1 ? kFull : ((2u << lane) - 1u);
+  int base = 0;  // lists started before window F
+  for (int F = 0; F < total; F += kWarp) {
+    const unsigned bit = (len > 0 && excl >= F && excl < F + kWarp) ? (1u << (excl - F)) : 0u;
+    const unsigned starts = __reduce_or_sync(kFull, bit);
+    const int p = max(base + __popc(starts & upto) - 1, 0);
+    const int64_t pst = __shfl_sync(kFull, st, p);
+    const int pex = __shfl_sync(kFull, excl, p);
+    const int f = F + lane;
+    if (f < total) hits += probe(__ldg(col + pst + (f - pex)));
+    base += __popc(starts);
   }
   return hits;
 }
@@ -132,16 +195,20 @@ __device__ __forceinline__ int ceil_log2(int v) { return v <= 1 ? 0 : 32 - __clz
 
 // One CTA per hub task: N+(owner) into a table of 2^lg slots (load <= 1/4
 // when it fits, <= 1/2 at the size cap; owners beyond the cap use binary
-// search in global memory), then the 8 warps share the partner chunk.
+// search in global memory), then the 8 warps claim the row chunk kClaim
+// entries at a time and stream each partner's list through the table.
 __global__ void __launch_bounds__(kCountThreads) tc_hub_kernel(CountArgs a) {
   extern __shared__ int table[];
   __shared__ unsigned long long s_task;
-  const int lane = threadIdx.x & (kWarp - 1), warp = threadIdx.x / kWarp;
-  const int nwarps = blockDim.x / kWarp;
+  __shared__ int s_next;
+  const int lane = threadIdx.x & (kWarp - 1);
   const int64_t ntasks = shard_tasks(a);
   unsigned long long hits = 0;
   for (;;) {
-    if (threadIdx.x == 0) s_task = atomicAdd(a.queue, 1ull);
+    if (threadIdx.x == 0) {
+      s_task = atomicAdd(a.queue, 1ull);
+      s_next = 0;
+    }
     __syncthreads();
     const unsigned long long t = s_task;
     if ((int64_t)t >= ntasks) break;
@@ -149,10 +216,9 @@ __global__ void __launch_bounds__(kCountThreads) tc_hub_kernel(CountArgs a) {
     const int x = (int)(task >> 32);
     const int chunk = (int)(task & 0xffffffffu);
     const int64_t a0 = a.dag_rowptr[x];
-    const int d = (int)(a.dag_rowptr[x + 1] - a0);
-    const int64_t pend = a.prt_rowptr[x + 1];
-    const int64_t q0 = a.prt_rowptr[x] + (int64_t)chunk * kHubChunk;
-    const int64_t q1 = min(q0 + kHubChunk, pend);
+    const int d = a.key[x].y;
+    const int64_t e0 = a.rowptr[x] + (int64_t)chunk * kHubChunk;
+    const int nc = (int)min((int64_t)kHubChunk, a.rowptr[x + 1] - e0);
     int lg = max(8, ceil_log2(4 * d));
     if (lg > a.table_log2_max && 2 * d <= (1 << a.table_log2_max)) lg = a.table_log2_max;
     if (lg <= a.table_log2_max) {
@@ -165,23 +231,28 @@ __global__ void __launch_bounds__(kCountThreads) tc_hub_kernel(CountArgs a) {
       for (int i = threadIdx.x; i < d; i += blockDim.x)
         table_insert(table, mask, shift, __ldg(a.dag_col + a0 + i), a.err);
       __syncthreads();
-      hits += stream_partners(a, q0, q1, warp, nwarps, lane, TableProbe{table, mask, shift});
+      hits += claim_and_stream(a, x, d, e0, nc, &s_next, lane, TableProbe{table, mask, shift});
     } else {
-      hits += stream_partners(a, q0, q1, warp, nwarps, lane, ListProbe{a.dag_col + a0, d});
+      hits += claim_and_stream(a, x, d, e0, nc, &s_next, lane, ListProbe{a.dag_col + a0, d});
     }
-    __syncthreads();  // table and s_task are rewritten by the next task
+    __syncthreads();  // table, s_task and s_next are rewritten by the next task
   }
   hits = warp_sum_u64(hits);
   if (lane == 0 && hits) atomicAdd(a.result, hits);
 }
 
-// One warp per leaf task (owner d+ <= kLeafMaxOut): a private 256-slot table.
+// One warp per leaf task (owner d+ <= kLeafMaxOut): a private 256-slot table;
+// the chunk's neighbours, 32 at a time, are filtered to partners whose
+// (short) lists are walked flat.
 __global__ void __launch_bounds__(kCountThreads) tc_leaf_kernel(CountArgs a) {
   __shared__ int tables[kCountThreads / kWarp][kLeafSlots];
+  __shared__ int64_t c_st[kCountThreads / kWarp][kWarp];
+  __shared__ int c_len[kCountThreads / kWarp][kWarp];
   const int lane = threadIdx.x & (kWarp - 1), warp = threadIdx.x / kWarp;
   int *tab = tables[warp];
   constexpr int lg = 8;  // log2(kLeafSlots)
   static_assert((1 << lg) == kLeafSlots, "leaf table size");
+  const TableProbe probe{tab, kLeafSlots - 1, 32 - lg};
   const int64_t ntasks = shard_tasks(a);
   unsigned long long hits = 0;
   for (;;) {
@@ -193,16 +264,40 @@ __global__ void __launch_bounds__(kCountThreads) tc_leaf_kernel(CountArgs a) {
     const int x = (int)(task >> 32);
     const int chunk = (int)(task & 0xffffffffu);
     const int64_t a0 = a.dag_rowptr[x];
-    const int d = (int)(a.dag_rowptr[x + 1] - a0);
-    const int64_t q0 = a.prt_rowptr[x] + (int64_t)chunk * kLeafChunk;
-    const int64_t q1 = min(q0 + kLeafChunk, a.prt_rowptr[x + 1]);
+    const int d = a.key[x].y;
+    const int64_t e0 = a.rowptr[x] + (int64_t)chunk * kLeafChunk;
+    const int nc = (int)min((int64_t)kLeafChunk, a.rowptr[x + 1] - e0);
     int4 *t4 = reinterpret_cast<int4 *>(tab);
     for (int i = lane; i < kLeafSlots / 4; i += kWarp) t4[i] = make_int4(-1, -1, -1, -1);
     __syncwarp();
     for (int i = lane; i < d; i += kWarp)
       table_insert(tab, kLeafSlots - 1, 32 - lg, __ldg(a.dag_col + a0 + i), a.err);
     __syncwarp();
-    hits += stream_partners(a, q0, q1, 0, 1, lane, TableProbe{tab, kLeafSlots - 1, 32 - lg});
+    for (int b = 0; b < nc; b += kWarp) {
+      int64_t st = 0;
+      int len = 0;
+      if (b + lane < nc) {
+        const int y = __ldg(a.col + e0 + b + lane);
+        const int py = __ldg(&a.key[y].y);
+        if (owns(x, d, y, py)) {
+          st = __ldg(a.dag_rowptr + y);
+          len = py;
+        }
+      }
+      // Compact the partners into lanes 0..k-1.
+      const unsigned m = __ballot_sync(kFull, len > 0);
+      if (len > 0) {
+        const int r = __popc(m & ((1u << lane) - 1u));
+        c_st[warp][r] = st;
+        c_len[warp][r] = len;
+      }
+      __syncwarp();
+      const int k = __popc(m);
+      st = lane < k ? c_st[warp][lane] : 0;
+      len = lane < k ? c_len[warp][lane] : 0;
+      __syncwarp();
+      hits += stream_flat(a.dag_col, st, len, lane, probe);
+    }
     __syncwarp();
   }
   hits = warp_sum_u64(hits);
@@ -224,10 +319,11 @@ int tc_count_launch(mc_dgraph *g, cudaEvent_t after_hub, int shard, int num_shar
     return MC_OK;
   }
   CountArgs a{};
+  a.rowptr = g->rowptr;
+  a.col = g->col;
+  a.key = g->key;
   a.dag_rowptr = g->dag_rowptr;
   a.dag_col = g->dag_col;
-  a.prt_rowptr = g->prt_rowptr;
-  a.prt_col = g->prt_col;
   a.result = g->counters + 0;
   a.err = g->err;
   a.table_log2_max = g->hub_table_log2;

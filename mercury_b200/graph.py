@@ -171,6 +171,14 @@ class DeviceGraph:
                                       C.byref(self.last_timing)), "sharded triangle count")
         return out.value
 
+    def pattern_count(self, pattern) -> int:
+        """Count of pattern P1..P8 (int 1..8 or the string "P1".."P8")."""
+        k = int(str(pattern).upper().lstrip("P"))
+        out = C.c_uint64()
+        check(lib().mc_pattern_count(self._h, k, C.byref(out), C.byref(self.last_timing)),
+              f"pattern P{k}")
+        return out.value
+
     def tc_stats(self) -> dict:
         st = TcStats()
         check(lib().mc_tc_stats(self._h, C.byref(st)), "tc stats")
