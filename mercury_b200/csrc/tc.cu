@@ -125,9 +125,167 @@ __device__ __forceinline__ unsigned stream_list(const int32_t *__restrict__ col,
   return hits;
 }
 
+// ---- table probes with deferred collisions ---------------------------------
+// Every key gets one probe of its home slot.  A key that finds another key
+// there is appended to a per-warp queue in shared memory; the queue is worked
+// off 32 entries at a time, one slot per entry per step (entries that meet
+// yet another key are re-queued), so no lane waits on another lane's chain.
+constexpr int kQueueCap = 64;
+
+struct ProbeQueue {
+  int2 *q;  // this warp's kQueueCap entries {key, next slot}
+  int cnt;  // same value on every lane
+};
+
+__device__ __forceinline__ void queue_push(ProbeQueue &Q, bool need, int w, unsigned slot,
+                                           int lane) {
+  const unsigned m = __ballot_sync(kFull, need);
+  if (need) Q.q[Q.cnt + __popc(m & ((1u << lane) - 1u))] = make_int2(w, (int)slot);
+  Q.cnt += __popc(m);
+}
+
+// One step over the newest min(cnt, 32) queued keys.
+__device__ __forceinline__ unsigned queue_step(ProbeQueue &Q, const int *tab, unsigned mask,
+                                               int lane) {
+  __syncwarp();
+  const int take = min(Q.cnt, kWarp);
+  const int base = Q.cnt - take;
+  const bool act = lane < take;
+  const int2 e = act ? Q.q[base + lane] : make_int2(0, 0);
+  __syncwarp();
+  Q.cnt = base;
+  unsigned hit = 0;
+  bool more = false;
+  if (act) {
+    const int t = tab[e.y];
+    hit = t == e.x;
+    more = t >= 0 && t != e.x;
+  }
+  queue_push(Q, more, e.x, ((unsigned)e.y + 1u) & mask, lane);
+  return hit;
+}
+
+// Steps until at most keep_below keys wait.  Every queued key reaches an
+// empty slot or itself within mask + 1 steps (tables are at most half
+// full); the bound only guards against a corrupted table, which raises the
+// error flag and drops the queue.
+__device__ __forceinline__ unsigned queue_drain(ProbeQueue &Q, const int *tab, unsigned mask,
+                                                int lane, int keep_below, unsigned *err) {
+  unsigned hits = 0;
+  const int limit = 4 * (int)(mask + 1) + 8;
+  for (int it = 0; Q.cnt > keep_below; ++it) {
+    if (it >= limit) {
+      if (lane == 0) atomicOr(err, (unsigned)kErrHashFull);
+      Q.cnt = 0;
+      break;
+    }
+    hits += queue_step(Q, tab, mask, lane);
+  }
+  return hits;
+}
+
+// Home-slot probe of key w (valid lanes only); collisions are queued.
+__device__ __forceinline__ unsigned home_probe(ProbeQueue &Q, const int *tab, unsigned mask,
+                                               int shift, int w, bool valid, int lane) {
+  const unsigned h = hash_slot(w, shift);
+  const int t = valid ? tab[h] : -1;
+  queue_push(Q, t >= 0 && t != w, w, (h + 1u) & mask, lane);
+  return valid && t == w;
+}
+
+// One warp streams col[st, st+len) through the table: each lane keeps four
+// 8-byte loads in flight, then probes the eight keys.  The queue holds at
+// most 31 keys between push rounds, so one round (<= 32 keys) never
+// overflows its kQueueCap entries.
+__device__ __forceinline__ unsigned stream_list_q(const int32_t *__restrict__ col, int64_t st,
+                                                  int len, int lane, const int *tab,
+                                                  unsigned mask, int shift, ProbeQueue &Q,
+                                                  unsigned *err) {
+  constexpr int kU = 4;
+  unsigned hits = 0;
+  const int head = (int)(st & 1) & (len > 0 ? 1 : 0);
+  const int64_t a = st + head;
+  const int rest = len - head;
+  const int body = rest >> 1;
+  // the scalar ends: head (odd start) on lane 0, odd tail on lane 1
+  {
+    const bool h = lane == 0 && head;
+    const bool t = lane == 1 && (rest & 1);
+    const int w = h ? __ldg(col + st) : (t ? __ldg(col + a + 2 * body) : 0);
+    hits += home_probe(Q, tab, mask, shift, w, h || t, lane);
+    hits += queue_drain(Q, tab, mask, lane, kWarp - 1, err);
+  }
+  const int2 *v = reinterpret_cast<const int2 *>(col + a);
+  for (int k0 = 0; k0 < body; k0 += kWarp * kU) {
+    int2 q[kU];
+    bool ok[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const int k = k0 + u * kWarp + lane;
+      ok[u] = k < body;
+      q[u] = ok[u] ? __ldg(v + k) : make_int2(0, 0);
+    }
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      hits += home_probe(Q, tab, mask, shift, q[u].x, ok[u], lane);
+      hits += queue_drain(Q, tab, mask, lane, kWarp - 1, err);
+      hits += home_probe(Q, tab, mask, shift, q[u].y, ok[u], lane);
+      hits += queue_drain(Q, tab, mask, lane, kWarp - 1, err);
+    }
+  }
+  return hits;
+}
+
+// Hub task over entries [e0, e0 + nc) of owner x's symmetric row: the CTA's
+// warps claim entries from the shared counter *next (smaller claims as the
+// chunk runs out); each claimed neighbour that is a partner has its list
+// streamed through the owner's table by the whole warp.
+__device__ __forceinline__ unsigned long long claim_and_stream_table(
+    const CountArgs &a, int x, int px, int64_t e0, int nc, int *next, int lane, const int *tab,
+    unsigned mask, int shift, ProbeQueue &Q) {
+  unsigned long long hits = 0;
+  for (;;) {
+    int g = 0;
+    if (lane == 0) {
+      const int seen = *(volatile int *)next;
+      const int size = max(1, min(kClaim, (nc - seen) / 16));
+      g = atomicAdd(next, size) | (size << 20);
+    }
+    g = __shfl_sync(kFull, g, 0);
+    const int size = g >> 20;
+    g &= (1 << 20) - 1;
+    if (g >= nc) break;
+    bool part = false;
+    int64_t st = 0;
+    int len = 0;
+    if (lane < size && g + lane < nc) {
+      const int y = __ldg(a.col + e0 + g + lane);
+      const int py = __ldg(&a.key[y].y);
+      if (owns(x, px, y, py)) {
+        part = true;
+        st = __ldg(a.dag_rowptr + y);
+        len = py;
+      }
+    }
+    unsigned m = __ballot_sync(kFull, part);
+    unsigned h = 0;
+    while (m) {
+      const int p = __ffs(m) - 1;
+      m &= m - 1;
+      const int64_t s = __shfl_sync(kFull, st, p);
+      const int l = __shfl_sync(kFull, len, p);
+      h += stream_list_q(a.dag_col, s, l, lane, tab, mask, shift, Q, a.err);
+    }
+    h += queue_drain(Q, tab, mask, lane, 0, a.err);
+    hits += h;
+  }
+  return hits;
+}
+
 // Entries [e0, e0 + nc) of owner x's symmetric row, claimed by the CTA's warps
 // kClaim at a time from the shared counter *next; each claimed neighbour that
-// is a partner has its list streamed by the whole warp.
+// is a partner has its list streamed by the whole warp (binary-search probe
+// for owners too large for the shared-memory table).
 template <class Probe>
 __device__ __forceinline__ unsigned long long claim_and_stream(const CountArgs &a, int x, int px,
                                                                int64_t e0, int nc, int *next,
@@ -197,11 +355,13 @@ __device__ __forceinline__ int ceil_log2(int v) { return v <= 1 ? 0 : 32 - __clz
 // when it fits, <= 1/2 at the size cap; owners beyond the cap use binary
 // search in global memory), then the 8 warps claim the row chunk kClaim
 // entries at a time and stream each partner's list through the table.
-__global__ void __launch_bounds__(kCountThreads) tc_hub_kernel(CountArgs a) {
+__global__ void __launch_bounds__(kCountThreads, 5) tc_hub_kernel(CountArgs a) {
   extern __shared__ int table[];
   __shared__ unsigned long long s_task;
   __shared__ int s_next;
+  __shared__ int2 s_queue[kCountThreads / kWarp][kQueueCap];
   const int lane = threadIdx.x & (kWarp - 1);
+  ProbeQueue Q{s_queue[threadIdx.x / kWarp], 0};
   const int64_t ntasks = shard_tasks(a);
   unsigned long long hits = 0;
   for (;;) {
@@ -231,7 +391,7 @@ __global__ void __launch_bounds__(kCountThreads) tc_hub_kernel(CountArgs a) {
       for (int i = threadIdx.x; i < d; i += blockDim.x)
         table_insert(table, mask, shift, __ldg(a.dag_col + a0 + i), a.err);
       __syncthreads();
-      hits += claim_and_stream(a, x, d, e0, nc, &s_next, lane, TableProbe{table, mask, shift});
+      hits += claim_and_stream_table(a, x, d, e0, nc, &s_next, lane, table, mask, shift, Q);
     } else {
       hits += claim_and_stream(a, x, d, e0, nc, &s_next, lane, ListProbe{a.dag_col + a0, d});
     }
@@ -267,23 +427,34 @@ __global__ void __launch_bounds__(kCountThreads) tc_leaf_kernel(CountArgs a) {
     const int d = a.key[x].y;
     const int64_t e0 = a.rowptr[x] + (int64_t)chunk * kLeafChunk;
     const int nc = (int)min((int64_t)kLeafChunk, a.rowptr[x + 1] - e0);
+    // Partners of the chunk first (kLeafChunk / 32 per lane); no table is
+    // built for a chunk without partners.
+    static_assert(kLeafChunk == 2 * kWarp, "two neighbours per lane");
+    int64_t pst[2] = {0, 0};
+    int plen[2] = {0, 0};
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int i = r * kWarp + lane;
+      if (i < nc) {
+        const int y = __ldg(a.col + e0 + i);
+        const int py = __ldg(&a.key[y].y);
+        if (owns(x, d, y, py)) {
+          pst[r] = __ldg(a.dag_rowptr + y);
+          plen[r] = py;
+        }
+      }
+    }
+    if (!__any_sync(kFull, plen[0] > 0 || plen[1] > 0)) continue;
     int4 *t4 = reinterpret_cast<int4 *>(tab);
     for (int i = lane; i < kLeafSlots / 4; i += kWarp) t4[i] = make_int4(-1, -1, -1, -1);
     __syncwarp();
     for (int i = lane; i < d; i += kWarp)
       table_insert(tab, kLeafSlots - 1, 32 - lg, __ldg(a.dag_col + a0 + i), a.err);
     __syncwarp();
-    for (int b = 0; b < nc; b += kWarp) {
-      int64_t st = 0;
-      int len = 0;
-      if (b + lane < nc) {
-        const int y = __ldg(a.col + e0 + b + lane);
-        const int py = __ldg(&a.key[y].y);
-        if (owns(x, d, y, py)) {
-          st = __ldg(a.dag_rowptr + y);
-          len = py;
-        }
-      }
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      int64_t st = pst[r];
+      int len = plen[r];
       // Compact the partners into lanes 0..k-1.
       const unsigned m = __ballot_sync(kFull, len > 0);
       if (len > 0) {
