@@ -1,20 +1,21 @@
 // Triangle-count kernels.  count = sum over DAG edges {x, y} of
 // |N+(x) & N+(y)|, where x is the edge's owner (larger d+, ties to the larger
 // id) and y its partner.  A task is (owner, chunk of the owner's symmetric
-// row): N+(owner) goes into a shared-memory open-addressing table, the
-// chunk's neighbours are filtered down to partners (owner rule on d+), and
-// each partner's list N+(y) -- never longer than N+(owner) -- is streamed
-// through the table.
+// row): N+(owner) goes into a shared-memory cuckoo table, the chunk's
+// neighbours are filtered down to partners (owner rule on d+), and each
+// partner's list N+(y) -- never longer than N+(owner) -- is streamed through
+// the table.
 //
 // Reference counterparts: hashIndex_for_large_degree (CTA per large vertex,
-// 1019-bin hash staged through a 256 MiB global scratch,
-// gpu_kernels/tc_challenge.cuh:4-192) and binarySearch_for_small_degree
-// (warp per small vertex, binary search in shared memory,
-// gpu_kernels/tc_challenge.cuh:195-303), each with an atomic work counter
-// (DYNAMIC_MODE, gpu_kernels/tuning_schedules.cuh:1-21).  Here the queues hold
-// bounded (owner, row-chunk) tasks, the tables live in shared memory only,
-// and the hash needs no global scratch.
+// 1019-bin hash staged through a 256 MiB global scratch, bin scanned
+// linearly per probe, gpu_kernels/tc_challenge.cuh:4-192) and
+// binarySearch_for_small_degree (warp per small vertex, binary search in
+// shared memory, gpu_kernels/tc_challenge.cuh:195-303), each with an atomic
+// work counter (DYNAMIC_MODE, gpu_kernels/tuning_schedules.cuh:1-21).  Here
+// the queues hold bounded (owner, row-chunk) tasks, the tables live in shared
+// memory only, and a probe is two fixed table reads with no branch.
 #include <algorithm>
+#include <climits>
 
 #include "dgraph.cuh"
 #include "device_common.cuh"
@@ -22,7 +23,9 @@
 namespace mc {
 namespace {
 
-constexpr int kClaim = 16;  // owner-row entries a hub warp claims at a time
+constexpr int kClaim = 16;     // owner-row entries a hub warp claims at a time
+constexpr int kMaxKicks = 64;  // cuckoo displacements allowed per inserted key
+constexpr int kNoKey = INT_MIN;  // probe value that matches no slot
 
 struct CountArgs {
   const int64_t *__restrict__ rowptr;      // symmetric CSR
@@ -48,28 +51,47 @@ __device__ __forceinline__ uint64_t shard_task(const CountArgs &a, unsigned long
   return a.tasks[(int64_t)t * a.num_shards + a.shard];
 }
 
-// Probe of an open-addressing table (empty slot = -1, linear probing).  The
-// tables are filled to at most half, so a probe meets an empty slot; the
-// bound only guards against a corrupted table.
-struct TableProbe {
+// ---- cuckoo tables ---------------------------------------------------------
+// A table of 2^lg int slots (empty = -1).  Key k lives in one of two slots:
+// s1 (multiplicative hash) or s2 = s1 ^ (odd second hash), so s2 != s1 and
+// each slot names the other.  Lookup reads both slots.
+__device__ __forceinline__ void cuckoo_slots(int key, int shift, unsigned &s1, unsigned &s2) {
+  s1 = ((unsigned)key * 2654435769u) >> shift;
+  s2 = s1 ^ ((((unsigned)key * 0x85EBCA77u) >> shift) | 1u);
+}
+
+struct CuckooProbe {
   const int *tab;
-  unsigned mask;
   int shift;
   __device__ __forceinline__ unsigned operator()(int w) const {
-    unsigned h = hash_slot(w, shift);
-    int t = tab[h];
-    if (t == w) return 1u;
-#pragma unroll 1
-    for (unsigned it = 0; t >= 0 && it < mask; ++it) {
-      h = (h + 1) & mask;
-      t = tab[h];
-      if (t == w) return 1u;
-    }
-    return 0u;
+    unsigned s1, s2;
+    cuckoo_slots(w, shift, s1, s2);
+    return (unsigned)(tab[s1] == w) | (unsigned)(tab[s2] == w);
   }
 };
 
-// Binary search in a sorted global list (owners too large for the table).
+// Concurrent insertion: exchange the key into a slot and carry the evicted
+// key to its other slot.  Every key stays in exactly one carrier (a slot or
+// a thread), so with all threads done each inserted key sits in s1 or s2 --
+// unless a thread ran out of displacements, in which case the key it carries
+// is not stored and the function returns false.
+__device__ __forceinline__ bool cuckoo_insert(int *tab, int shift, int key) {
+  unsigned s1, s2;
+  cuckoo_slots(key, shift, s1, s2);
+  unsigned pos = s1;
+  int k = key;
+  for (int kick = 0; kick < kMaxKicks; ++kick) {
+    const int old = atomicExch(tab + pos, k);
+    if (old < 0) return true;
+    k = old;
+    cuckoo_slots(k, shift, s1, s2);
+    pos = pos == s1 ? s2 : s1;
+  }
+  return false;
+}
+
+// Binary search in a sorted global list: owners too large for the table, or
+// whose table could not be built.
 struct ListProbe {
   const int32_t *list;
   int len;
@@ -85,164 +107,50 @@ struct ListProbe {
   }
 };
 
-__device__ __forceinline__ void table_insert(int *tab, unsigned mask, int shift, int key,
-                                             unsigned *err) {
-  unsigned h = hash_slot(key, shift);
-  for (unsigned it = 0;; ++it) {
-    const int prev = atomicCAS(tab + h, -1, key);
-    if (prev == -1 || prev == key) return;
-    h = (h + 1) & mask;
-    if (it >= mask) {
-      atomicOr(err, (unsigned)kErrHashFull);
-      return;
-    }
-  }
-}
-
 // Partner test for neighbour y of owner x (px = d+(x), py = d+(y)).
 __device__ __forceinline__ bool owns(int x, int px, int y, int py) {
   return py >= 1 && (px > py || (px == py && x > y));
 }
 
-// One warp streams one list col[st, st+len) through `probe`: 8-byte loads
-// (two probes per lane) with a scalar head/tail for odd ends.  Returns this
-// lane's hits.
+// One warp streams one list col[st, st+len) through `probe`: each lane keeps
+// four 8-byte loads in flight, then probes the eight keys; an odd head and
+// tail are probed by lanes 0 and 1.  Returns this lane's hits.
 template <class Probe>
 __device__ __forceinline__ unsigned stream_list(const int32_t *__restrict__ col, int64_t st,
                                                 int len, int lane, const Probe &probe) {
-  unsigned hits = 0;
-  const int head = (int)(st & 1) & (len > 0 ? 1 : 0);
-  if (lane == 0 && head) hits += probe(__ldg(col + st));
-  const int64_t a = st + head;
-  const int rest = len - head;
-  const int body = rest >> 1;
-  const int2 *v = reinterpret_cast<const int2 *>(col + a);
-  for (int k = lane; k < body; k += kWarp) {
-    const int2 q = __ldg(v + k);
-    hits += probe(q.x) + probe(q.y);
-  }
-  if (lane == 0 && (rest & 1)) hits += probe(__ldg(col + a + 2 * body));
-  return hits;
-}
-
-// ---- table probes with deferred collisions ---------------------------------
-// Every key gets one probe of its home slot.  A key that finds another key
-// there is appended to a per-warp queue in shared memory; the queue is worked
-// off 32 entries at a time, one slot per entry per step (entries that meet
-// yet another key are re-queued), so no lane waits on another lane's chain.
-constexpr int kQueueCap = 64;
-
-struct ProbeQueue {
-  int2 *q;  // this warp's kQueueCap entries {key, next slot}
-  int cnt;  // same value on every lane
-};
-
-__device__ __forceinline__ void queue_push(ProbeQueue &Q, bool need, int w, unsigned slot,
-                                           int lane) {
-  const unsigned m = __ballot_sync(kFull, need);
-  if (need) Q.q[Q.cnt + __popc(m & ((1u << lane) - 1u))] = make_int2(w, (int)slot);
-  Q.cnt += __popc(m);
-}
-
-// One step over the newest min(cnt, 32) queued keys.
-__device__ __forceinline__ unsigned queue_step(ProbeQueue &Q, const int *tab, unsigned mask,
-                                               int lane) {
-  __syncwarp();
-  const int take = min(Q.cnt, kWarp);
-  const int base = Q.cnt - take;
-  const bool act = lane < take;
-  const int2 e = act ? Q.q[base + lane] : make_int2(0, 0);
-  __syncwarp();
-  Q.cnt = base;
-  unsigned hit = 0;
-  bool more = false;
-  if (act) {
-    const int t = tab[e.y];
-    hit = t == e.x;
-    more = t >= 0 && t != e.x;
-  }
-  queue_push(Q, more, e.x, ((unsigned)e.y + 1u) & mask, lane);
-  return hit;
-}
-
-// Steps until at most keep_below keys wait.  Every queued key reaches an
-// empty slot or itself within mask + 1 steps (tables are at most half
-// full); the bound only guards against a corrupted table, which raises the
-// error flag and drops the queue.
-__device__ __forceinline__ unsigned queue_drain(ProbeQueue &Q, const int *tab, unsigned mask,
-                                                int lane, int keep_below, unsigned *err) {
-  unsigned hits = 0;
-  const int limit = 4 * (int)(mask + 1) + 8;
-  for (int it = 0; Q.cnt > keep_below; ++it) {
-    if (it >= limit) {
-      if (lane == 0) atomicOr(err, (unsigned)kErrHashFull);
-      Q.cnt = 0;
-      break;
-    }
-    hits += queue_step(Q, tab, mask, lane);
-  }
-  return hits;
-}
-
-// Home-slot probe of key w (valid lanes only); collisions are queued.
-__device__ __forceinline__ unsigned home_probe(ProbeQueue &Q, const int *tab, unsigned mask,
-                                               int shift, int w, bool valid, int lane) {
-  const unsigned h = hash_slot(w, shift);
-  const int t = valid ? tab[h] : -1;
-  queue_push(Q, t >= 0 && t != w, w, (h + 1u) & mask, lane);
-  return valid && t == w;
-}
-
-// One warp streams col[st, st+len) through the table: each lane keeps four
-// 8-byte loads in flight, then probes the eight keys.  The queue holds at
-// most 31 keys between push rounds, so one round (<= 32 keys) never
-// overflows its kQueueCap entries.
-__device__ __forceinline__ unsigned stream_list_q(const int32_t *__restrict__ col, int64_t st,
-                                                  int len, int lane, const int *tab,
-                                                  unsigned mask, int shift, ProbeQueue &Q,
-                                                  unsigned *err) {
   constexpr int kU = 4;
   unsigned hits = 0;
   const int head = (int)(st & 1) & (len > 0 ? 1 : 0);
   const int64_t a = st + head;
   const int rest = len - head;
   const int body = rest >> 1;
-  // the scalar ends: head (odd start) on lane 0, odd tail on lane 1
-  {
-    const bool h = lane == 0 && head;
-    const bool t = lane == 1 && (rest & 1);
-    const int w = h ? __ldg(col + st) : (t ? __ldg(col + a + 2 * body) : 0);
-    hits += home_probe(Q, tab, mask, shift, w, h || t, lane);
-    hits += queue_drain(Q, tab, mask, lane, kWarp - 1, err);
+  if (head | (rest & 1)) {
+    const bool h = lane == 0 && head, t = lane == 1 && (rest & 1);
+    const int w = h ? __ldg(col + st) : (t ? __ldg(col + a + 2 * body) : kNoKey);
+    hits += probe(w);
   }
   const int2 *v = reinterpret_cast<const int2 *>(col + a);
   for (int k0 = 0; k0 < body; k0 += kWarp * kU) {
     int2 q[kU];
-    bool ok[kU];
 #pragma unroll
     for (int u = 0; u < kU; ++u) {
       const int k = k0 + u * kWarp + lane;
-      ok[u] = k < body;
-      q[u] = ok[u] ? __ldg(v + k) : make_int2(0, 0);
+      q[u] = k < body ? __ldg(v + k) : make_int2(kNoKey, kNoKey);
     }
 #pragma unroll
-    for (int u = 0; u < kU; ++u) {
-      hits += home_probe(Q, tab, mask, shift, q[u].x, ok[u], lane);
-      hits += queue_drain(Q, tab, mask, lane, kWarp - 1, err);
-      hits += home_probe(Q, tab, mask, shift, q[u].y, ok[u], lane);
-      hits += queue_drain(Q, tab, mask, lane, kWarp - 1, err);
-    }
+    for (int u = 0; u < kU; ++u) hits += probe(q[u].x) + probe(q[u].y);
   }
   return hits;
 }
 
-// Hub task over entries [e0, e0 + nc) of owner x's symmetric row: the CTA's
-// warps claim entries from the shared counter *next (smaller claims as the
+// Entries [e0, e0 + nc) of owner x's symmetric row, claimed by the CTA's warps
+// from the shared counter *next (kClaim at a time, smaller claims as the
 // chunk runs out); each claimed neighbour that is a partner has its list
-// streamed through the owner's table by the whole warp.
-__device__ __forceinline__ unsigned long long claim_and_stream_table(
-    const CountArgs &a, int x, int px, int64_t e0, int nc, int *next, int lane, const int *tab,
-    unsigned mask, int shift, ProbeQueue &Q) {
+// streamed by the whole warp.
+template <class Probe>
+__device__ __forceinline__ unsigned long long claim_and_stream(const CountArgs &a, int x, int px,
+                                                               int64_t e0, int nc, int *next,
+                                                               int lane, const Probe &probe) {
   unsigned long long hits = 0;
   for (;;) {
     int g = 0;
@@ -259,47 +167,6 @@ __device__ __forceinline__ unsigned long long claim_and_stream_table(
     int64_t st = 0;
     int len = 0;
     if (lane < size && g + lane < nc) {
-      const int y = __ldg(a.col + e0 + g + lane);
-      const int py = __ldg(&a.key[y].y);
-      if (owns(x, px, y, py)) {
-        part = true;
-        st = __ldg(a.dag_rowptr + y);
-        len = py;
-      }
-    }
-    unsigned m = __ballot_sync(kFull, part);
-    unsigned h = 0;
-    while (m) {
-      const int p = __ffs(m) - 1;
-      m &= m - 1;
-      const int64_t s = __shfl_sync(kFull, st, p);
-      const int l = __shfl_sync(kFull, len, p);
-      h += stream_list_q(a.dag_col, s, l, lane, tab, mask, shift, Q, a.err);
-    }
-    h += queue_drain(Q, tab, mask, lane, 0, a.err);
-    hits += h;
-  }
-  return hits;
-}
-
-// Entries [e0, e0 + nc) of owner x's symmetric row, claimed by the CTA's warps
-// kClaim at a time from the shared counter *next; each claimed neighbour that
-// is a partner has its list streamed by the whole warp (binary-search probe
-// for owners too large for the shared-memory table).
-template <class Probe>
-__device__ __forceinline__ unsigned long long claim_and_stream(const CountArgs &a, int x, int px,
-                                                               int64_t e0, int nc, int *next,
-                                                               int lane, const Probe &probe) {
-  unsigned long long hits = 0;
-  for (;;) {
-    int g = 0;
-    if (lane == 0) g = atomicAdd(next, kClaim);
-    g = __shfl_sync(kFull, g, 0);
-    if (g >= nc) break;
-    bool part = false;
-    int64_t st = 0;
-    int len = 0;
-    if (lane < kClaim && g + lane < nc) {
       const int y = __ldg(a.col + e0 + g + lane);
       const int py = __ldg(&a.key[y].y);
       if (owns(x, px, y, py)) {
@@ -343,7 +210,7 @@ __device__ __forceinline__ unsigned long long stream_flat(const int32_t *__restr
     const int64_t pst = __shfl_sync(kFull, st, p);
     const int pex = __shfl_sync(kFull, excl, p);
     const int f = F + lane;
-    if (f < total) hits += probe(__ldg(col + pst + (f - pex)));
+    hits += probe(f < total ? __ldg(col + pst + (f - pex)) : kNoKey);
     base += __popc(starts);
   }
   return hits;
@@ -351,23 +218,23 @@ __device__ __forceinline__ unsigned long long stream_flat(const int32_t *__restr
 
 __device__ __forceinline__ int ceil_log2(int v) { return v <= 1 ? 0 : 32 - __clz(v - 1); }
 
-// One CTA per hub task: N+(owner) into a table of 2^lg slots (load <= 1/4
-// when it fits, <= 1/2 at the size cap; owners beyond the cap use binary
-// search in global memory), then the 8 warps claim the row chunk kClaim
-// entries at a time and stream each partner's list through the table.
+// One CTA per hub task: N+(owner) into a cuckoo table of 2^lg slots (load
+// <= 1/4 when it fits, <= 1/2 at the size cap), then the 8 warps claim the
+// row chunk and stream each partner's list through the table.  Owners beyond
+// the cap, or whose table could not be built, are probed by binary search in
+// global memory instead.
 __global__ void __launch_bounds__(kCountThreads, 5) tc_hub_kernel(CountArgs a) {
   extern __shared__ int table[];
   __shared__ unsigned long long s_task;
-  __shared__ int s_next;
-  __shared__ int2 s_queue[kCountThreads / kWarp][kQueueCap];
+  __shared__ int s_next, s_fail;
   const int lane = threadIdx.x & (kWarp - 1);
-  ProbeQueue Q{s_queue[threadIdx.x / kWarp], 0};
   const int64_t ntasks = shard_tasks(a);
   unsigned long long hits = 0;
   for (;;) {
     if (threadIdx.x == 0) {
       s_task = atomicAdd(a.queue, 1ull);
       s_next = 0;
+      s_fail = 0;
     }
     __syncthreads();
     const unsigned long long t = s_task;
@@ -381,28 +248,32 @@ __global__ void __launch_bounds__(kCountThreads, 5) tc_hub_kernel(CountArgs a) {
     const int nc = (int)min((int64_t)kHubChunk, a.rowptr[x + 1] - e0);
     int lg = max(8, ceil_log2(4 * d));
     if (lg > a.table_log2_max && 2 * d <= (1 << a.table_log2_max)) lg = a.table_log2_max;
-    if (lg <= a.table_log2_max) {
+    bool use_table = lg <= a.table_log2_max;
+    if (use_table) {
       const int size = 1 << lg;
-      const unsigned mask = (unsigned)size - 1u;
       const int shift = 32 - lg;
       int4 *t4 = reinterpret_cast<int4 *>(table);
       for (int i = threadIdx.x; i < size / 4; i += blockDim.x) t4[i] = make_int4(-1, -1, -1, -1);
       __syncthreads();
+      bool ok = true;
       for (int i = threadIdx.x; i < d; i += blockDim.x)
-        table_insert(table, mask, shift, __ldg(a.dag_col + a0 + i), a.err);
+        ok &= cuckoo_insert(table, shift, __ldg(a.dag_col + a0 + i));
+      if (!ok) s_fail = 1;
       __syncthreads();
-      hits += claim_and_stream_table(a, x, d, e0, nc, &s_next, lane, table, mask, shift, Q);
-    } else {
-      hits += claim_and_stream(a, x, d, e0, nc, &s_next, lane, ListProbe{a.dag_col + a0, d});
+      use_table = s_fail == 0;
+      if (use_table)
+        hits += claim_and_stream(a, x, d, e0, nc, &s_next, lane, CuckooProbe{table, shift});
     }
-    __syncthreads();  // table, s_task and s_next are rewritten by the next task
+    if (!use_table)
+      hits += claim_and_stream(a, x, d, e0, nc, &s_next, lane, ListProbe{a.dag_col + a0, d});
+    __syncthreads();  // table and the shared words are rewritten by the next task
   }
   hits = warp_sum_u64(hits);
   if (lane == 0 && hits) atomicAdd(a.result, hits);
 }
 
-// One warp per leaf task (owner d+ <= kLeafMaxOut): a private 256-slot table;
-// the chunk's neighbours, 32 at a time, are filtered to partners whose
+// One warp per leaf task (owner d+ <= kLeafMaxOut): a private 256-slot cuckoo
+// table (load <= 1/4); the chunk's neighbours are filtered to partners whose
 // (short) lists are walked flat.
 __global__ void __launch_bounds__(kCountThreads) tc_leaf_kernel(CountArgs a) {
   __shared__ int tables[kCountThreads / kWarp][kLeafSlots];
@@ -412,7 +283,8 @@ __global__ void __launch_bounds__(kCountThreads) tc_leaf_kernel(CountArgs a) {
   int *tab = tables[warp];
   constexpr int lg = 8;  // log2(kLeafSlots)
   static_assert((1 << lg) == kLeafSlots, "leaf table size");
-  const TableProbe probe{tab, kLeafSlots - 1, 32 - lg};
+  static_assert(4 * kLeafMaxOut <= kLeafSlots, "leaf table load <= 1/4");
+  const CuckooProbe probe{tab, 32 - lg};
   const int64_t ntasks = shard_tasks(a);
   unsigned long long hits = 0;
   for (;;) {
@@ -448,8 +320,9 @@ __global__ void __launch_bounds__(kCountThreads) tc_leaf_kernel(CountArgs a) {
     int4 *t4 = reinterpret_cast<int4 *>(tab);
     for (int i = lane; i < kLeafSlots / 4; i += kWarp) t4[i] = make_int4(-1, -1, -1, -1);
     __syncwarp();
-    for (int i = lane; i < d; i += kWarp)
-      table_insert(tab, kLeafSlots - 1, 32 - lg, __ldg(a.dag_col + a0 + i), a.err);
+    bool ok = true;
+    for (int i = lane; i < d; i += kWarp) ok &= cuckoo_insert(tab, 32 - lg, __ldg(a.dag_col + a0 + i));
+    const bool use_table = __all_sync(kFull, ok);
     __syncwarp();
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
@@ -458,16 +331,17 @@ __global__ void __launch_bounds__(kCountThreads) tc_leaf_kernel(CountArgs a) {
       // Compact the partners into lanes 0..k-1.
       const unsigned m = __ballot_sync(kFull, len > 0);
       if (len > 0) {
-        const int r = __popc(m & ((1u << lane) - 1u));
-        c_st[warp][r] = st;
-        c_len[warp][r] = len;
+        const int rank = __popc(m & ((1u << lane) - 1u));
+        c_st[warp][rank] = st;
+        c_len[warp][rank] = len;
       }
       __syncwarp();
       const int k = __popc(m);
       st = lane < k ? c_st[warp][lane] : 0;
       len = lane < k ? c_len[warp][lane] : 0;
       __syncwarp();
-      hits += stream_flat(a.dag_col, st, len, lane, probe);
+      if (use_table) hits += stream_flat(a.dag_col, st, len, lane, probe);
+      else hits += stream_flat(a.dag_col, st, len, lane, ListProbe{a.dag_col + a0, d});
     }
     __syncwarp();
   }
