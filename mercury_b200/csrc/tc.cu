@@ -23,7 +23,7 @@
 namespace mc {
 namespace {
 
-constexpr int kClaim = 16;     // owner-row entries a hub warp claims at a time
+constexpr int kClaim = 32;     // owner-row entries a hub warp claims at a time
 constexpr int kMaxKicks = 64;  // cuckoo displacements allowed per inserted key
 constexpr int kNoKey = INT_MIN;  // probe value that matches no slot
 
@@ -132,13 +132,16 @@ __device__ __forceinline__ unsigned stream_list(const int32_t *__restrict__ col,
   const int2 *v = reinterpret_cast<const int2 *>(col + a);
   for (int k0 = 0; k0 < body; k0 += kWarp * kU) {
     int2 q[kU];
+    // Blocks of 32 pairs past the end are skipped (a warp-uniform test).
 #pragma unroll
     for (int u = 0; u < kU; ++u) {
       const int k = k0 + u * kWarp + lane;
-      q[u] = k < body ? __ldg(v + k) : make_int2(kNoKey, kNoKey);
+      q[u] = make_int2(kNoKey, kNoKey);
+      if (k0 + u * kWarp < body && k < body) q[u] = __ldg(v + k);
     }
 #pragma unroll
-    for (int u = 0; u < kU; ++u) hits += probe(q[u].x) + probe(q[u].y);
+    for (int u = 0; u < kU; ++u)
+      if (k0 + u * kWarp < body) hits += probe(q[u].x) + probe(q[u].y);
   }
   return hits;
 }
