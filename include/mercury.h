@@ -162,6 +162,32 @@ int mc_dgraph_export_dag(const mc_dgraph_t *g, int64_t *rowptr_out,
 int mc_pattern_count(mc_dgraph_t *g, int pattern, uint64_t *count,
                      mc_timing_t *timing);
 
+/* Pattern count P<pattern> (1..8) of a symmetric CSR the caller already
+ * holds in device memory (d_rowptr: int64[n+1], d_col: int32[nnz]), for
+ * callers that cannot allocate device memory: a host application that owns
+ * all of the GPU's memory through its own pool and forbids allocations
+ * outside it, or a latency-bound caller that cannot afford cudaMalloc /
+ * cudaFree (cudaFree waits for the whole device).  This entry point calls no
+ * cudaMalloc, cudaFree or allocating library routine: its scratch (the
+ * per-warp frontier lists and a few counter words) is a file-scope device
+ * array of 32 MiB that every GPU loading this library holds until the
+ * process exits.  Frontier lists need 6 x max_degree ints per warp, so
+ * graphs whose maximum degree leaves room for fewer than 8 warps
+ * (max_degree > 174762) are refused with MC_ERR_UNSUPPORTED; larger
+ * degrees run fewer warps.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) with that device current; make that
+ * first call before any stream capture.  All calls share the array and its
+ * last contents (the counters are cleared at the start of every call):
+ * calls whose work overlaps on the GPU -- from two host threads, or on two
+ * streams -- race and must be serialised by the caller.  `stream` is a
+ * cudaStream_t (NULL: the default stream); the call returns after the count
+ * is on the host.  The graph is checked like mc_dgraph_create (MC_ERR_FORMAT).
+ * No counterpart in the reference, which allocates its frontier with
+ * cudaMalloc (subgraph_matching/sm_multigpu.cu:117-122). */
+int mc_pattern_count_static(const int64_t *d_rowptr, const int32_t *d_col,
+                            int64_t n, int64_t nnz, int pattern,
+                            uint64_t *count, void *stream);
+
 /* One-shot drop-in for TCSolver: host CSR in, count out.  Uploads, orients,
  * counts and copies the result back inside the call (timing->h2d_ms etc.).
  * Device buffers are cached in a per-thread context and reused while the

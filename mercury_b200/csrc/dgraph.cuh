@@ -63,6 +63,11 @@ int validate_graph(mc_dgraph *g, unsigned flags);
 int tc_alloc(mc_dgraph *g);
 int tc_orient(mc_dgraph *g);
 int tc_partner_stats(mc_dgraph *g, unsigned long long *partner_edges, unsigned long long *work);
+// Contract checks of a caller-owned device CSR with caller-provided device
+// words for the error flag and the maximum degree (nothing is allocated).
+int validate_csr_words(const int64_t *rowptr, const int32_t *col, int64_t n, int64_t nnz,
+                       unsigned *d_err, unsigned long long *d_max_deg, cudaStream_t s,
+                       int64_t *max_degree);
 // tc.cu
 int tc_count_launch(mc_dgraph *g, cudaEvent_t after_hub, int shard, int num_shards);
 // patterns.cu: result of P<pattern>; c12 (optional) receives counters 1 and 2.

@@ -383,6 +383,30 @@ int validate_graph(mc_dgraph *g, unsigned flags) {
   return *g->h_err ? MC_ERR_FORMAT : MC_OK;
 }
 
+int validate_csr_words(const int64_t *rowptr, const int32_t *col, int64_t n, int64_t nnz,
+                       unsigned *d_err, unsigned long long *d_max_deg, cudaStream_t s,
+                       int64_t *max_degree) {
+  unsigned h_err = 0;
+  unsigned long long h_max = 0;
+  MC_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(unsigned), s));
+  MC_CUDA_TRY(cudaMemsetAsync(d_max_deg, 0, sizeof(unsigned long long), s));
+  validate_rowptr_kernel<<<grid_for(n + 1, 256), 256, 0, s>>>(rowptr, n, nnz, d_err, d_max_deg);
+  MC_CUDA_TRY(cudaGetLastError());
+  MC_CUDA_TRY(cudaMemcpyAsync(&h_err, d_err, sizeof(h_err), cudaMemcpyDeviceToHost, s));
+  MC_CUDA_TRY(cudaMemcpyAsync(&h_max, d_max_deg, sizeof(h_max), cudaMemcpyDeviceToHost, s));
+  MC_CUDA_TRY(cudaStreamSynchronize(s));
+  if (h_err) return MC_ERR_FORMAT;  // the entry walk needs monotone offsets
+  const int64_t tiles = (nnz + kTileEdges - 1) / kTileEdges;
+  if (tiles > 0) {
+    validate_entries_kernel<<<(unsigned)tiles, kTileThreads, 0, s>>>(rowptr, col, n, nnz, 0, d_err);
+    MC_CUDA_TRY(cudaGetLastError());
+    MC_CUDA_TRY(cudaMemcpyAsync(&h_err, d_err, sizeof(h_err), cudaMemcpyDeviceToHost, s));
+    MC_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  *max_degree = (int64_t)h_max;
+  return h_err ? MC_ERR_FORMAT : MC_OK;
+}
+
 int tc_alloc(mc_dgraph *g) {
   if (g->tc_ready) return MC_OK;
   const int64_t n = g->n, cap = std::max<int64_t>(g->nnz, 1);

@@ -18,7 +18,9 @@
 // P3, P5, P7, P8), the product is formed the same way (wrapped to 32 bits,
 // sign-extended).
 #include <algorithm>
+#include <climits>
 #include <cstring>
+#include <mutex>
 
 #include "dgraph.cuh"
 #include "device_common.cuh"
@@ -431,4 +433,112 @@ extern "C" int mc_pattern_count(mc_dgraph_t *g, int pattern, uint64_t *count, mc
   if (!g || !count || pattern < 1 || pattern > 8) return MC_ERR_ARG;
   MC_CUDA_TRY(cudaSetDevice(g->device));
   return mc::pattern_count(g, pattern, count, nullptr, timing);
+}
+
+// ---- pattern count without allocation --------------------------------------
+// mc_pattern_count_static: the same kernels as mc_pattern_count over a CSR the
+// caller already holds in device memory, with every byte of scratch taken from
+// file-scope device arrays instead of cudaMalloc.  The arrays exist once per
+// GPU that loads this library and stay until the process exits.
+namespace mc {
+namespace {
+
+// Frontier lists of all warps: kLists lists of max_degree entries per warp.
+constexpr int64_t kStaticFrontierInts = int64_t(8) << 20;  // 32 MiB
+static __device__ __align__(256) int32_t g_static_frontier[kStaticFrontierInts];
+// [0] c1, [1] c2, [2] star queue, [3] edge queue, [4] max degree, [5] error
+static __device__ __align__(256) unsigned long long g_static_words[8];
+
+constexpr int kMaxStaticDevices = 64;
+struct StaticScratch {
+  int32_t *frontier = nullptr;
+  unsigned long long *words = nullptr;
+  bool ready = false;
+};
+StaticScratch g_static_scratch[kMaxStaticDevices];
+std::mutex g_static_mu;
+
+// Device addresses of the file-scope arrays on device `dev` (the current
+// device).  The host-side names are stand-ins, not device addresses; the
+// addresses come from cudaGetSymbolAddress, once per device.
+int static_scratch(int dev, StaticScratch *out) {
+  if (dev < 0 || dev >= kMaxStaticDevices) return MC_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  StaticScratch &s = g_static_scratch[dev];
+  if (!s.ready) {
+    MC_CUDA_TRY(cudaGetSymbolAddress((void **)&s.frontier, g_static_frontier));
+    MC_CUDA_TRY(cudaGetSymbolAddress((void **)&s.words, g_static_words));
+    s.ready = true;
+  }
+  *out = s;
+  return MC_OK;
+}
+
+template <int P, bool kStar>
+int launch_static(cudaStream_t s, const PatArgs &a, int grid) {
+  pattern_kernel<P, kStar><<<grid, kPatThreads, 0, s>>>(a);
+  MC_CUDA_TRY(cudaGetLastError());
+  return MC_OK;
+}
+
+}  // namespace
+}  // namespace mc
+
+extern "C" int mc_pattern_count_static(const int64_t *d_rowptr, const int32_t *d_col, int64_t n,
+                                       int64_t nnz, int pattern, uint64_t *count, void *stream) {
+  using namespace mc;
+  if (!d_rowptr || (nnz > 0 && !d_col) || !count || n < 0 || nnz < 0) return MC_ERR_ARG;
+  if (pattern < 1 || pattern > 8) return MC_ERR_ARG;
+  if (n > INT32_MAX - 1) return MC_ERR_UNSUPPORTED;
+  int dev = 0;
+  MC_CUDA_TRY(cudaGetDevice(&dev));
+  StaticScratch sc;
+  int rc = static_scratch(dev, &sc);
+  if (rc != MC_OK) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // Contract checks (ids in range, sorted rows, no self-loops) and the largest
+  // degree, which sizes the frontier lists; both use the static words.
+  int64_t max_degree = 0;
+  rc = validate_csr_words(d_rowptr, d_col, n, nnz, reinterpret_cast<unsigned *>(sc.words + 5),
+                          sc.words + 4, s, &max_degree);
+  if (rc != MC_OK) return rc;
+  const int64_t cap = std::max<int64_t>(max_degree, 1);
+  // Whole blocks of warps that fit in the static frontier array.
+  const int64_t per_block = (int64_t)(kPatThreads / kWarp) * kLists * cap;
+  const int64_t fit_blocks = kStaticFrontierInts / per_block;
+  if (fit_blocks < 1) return MC_ERR_UNSUPPORTED;  // max degree beyond the static capacity
+  int dev_sms = 0, per_sm = 0;
+  MC_CUDA_TRY(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, dev));
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pattern_kernel<3, false>, kPatThreads,
+                                                    0) != cudaSuccess)
+    per_sm = 4;
+  const int grid = (int)std::min<int64_t>(fit_blocks, (int64_t)dev_sms * std::max(per_sm, 1));
+  // The words keep the previous call's values: the counters and queues must
+  // start at zero.
+  MC_CUDA_TRY(cudaMemsetAsync(sc.words, 0, sizeof(unsigned long long) * 4, s));
+  PatArgs a{d_rowptr, d_col, n, nnz, sc.frontier, cap, sc.words + 0, sc.words + 2};
+  if (n > 0 && nnz > 0) {
+    switch (pattern) {
+      case 1:
+        rc = launch_static<1, true>(s, a, grid);
+        if (rc == MC_OK) {
+          a.queue = sc.words + 3;
+          rc = launch_static<1, false>(s, a, grid);
+        }
+        break;
+      case 2: rc = launch_static<2, false>(s, a, grid); break;
+      case 3: rc = launch_static<3, false>(s, a, grid); break;
+      case 4: rc = launch_static<4, false>(s, a, grid); break;
+      case 5: rc = launch_static<5, false>(s, a, grid); break;
+      case 6: rc = launch_static<6, false>(s, a, grid); break;
+      case 7: rc = launch_static<7, false>(s, a, grid); break;
+      default: rc = launch_static<8, false>(s, a, grid); break;
+    }
+    if (rc != MC_OK) return rc;
+  }
+  unsigned long long c[2] = {0, 0};
+  MC_CUDA_TRY(cudaMemcpyAsync(c, sc.words, sizeof(c), cudaMemcpyDeviceToHost, s));
+  MC_CUDA_TRY(cudaStreamSynchronize(s));
+  *count = (pattern == 4 || pattern == 6) ? c[0] : c[0] - c[1];
+  return MC_OK;
 }
