@@ -188,6 +188,29 @@ int mc_pattern_count_static(const int64_t *d_rowptr, const int32_t *d_col,
                             int64_t n, int64_t nnz, int pattern,
                             uint64_t *count, void *stream);
 
+/* ---- batches ---------------------------------------------------------------
+ * Many graphs counted in one captured CUDA-graph launch (no reference
+ * counterpart: the reference runs TCSolver / SMSolverMultiGPU once per
+ * graph).  The batch is one symmetric CSR, the disjoint union of the graphs:
+ * graph g owns vertices [graph_vptr[g], graph_vptr[g+1]) (ids are global)
+ * and no edge may join two graphs (MC_ERR_FORMAT).  jobs[g] is 0 for a
+ * triangle count or 1..8 for pattern P1..P8.  Every count equals the
+ * single-graph result (mc_tc_count / mc_pattern_count) of that graph. */
+typedef struct mc_batch mc_batch_t;
+int mc_batch_create(const int64_t *rowptr, const int32_t *col, int64_t n,
+                    int64_t nnz, const int64_t *graph_vptr, int num_graphs,
+                    const int32_t *jobs, void *stream, mc_batch_t **out);
+/* Tunes the triangle schedule per degree bucket of the triangle graphs
+ * (largest degree < 64, < 256, < 1024, >= 1024): the owner out-degree up to
+ * which a task is one warp (else one CTA) and the table slots per key, each
+ * from a small grid, by timing the bucket's graphs; re-captures the launch.
+ * `choice` (optional, 8 ints) receives {threshold, log2 slots per key} per
+ * bucket, -1 for empty buckets. */
+int mc_batch_autotune(mc_batch_t *b, int32_t *choice);
+/* counts[g] for every graph, from one replay of the captured launch. */
+int mc_batch_count(mc_batch_t *b, uint64_t *counts, mc_timing_t *timing);
+void mc_batch_free(mc_batch_t *b);
+
 /* One-shot drop-in for TCSolver: host CSR in, count out.  Uploads, orients,
  * counts and copies the result back inside the call (timing->h2d_ms etc.).
  * Device buffers are cached in a per-thread context and reused while the

@@ -17,6 +17,18 @@ constexpr int kCountThreads = 256;         // threads per counting CTA
 constexpr int kHubTableLog2Max = 15;       // at most 32768 slots (128 KB smem)
 }  // namespace mc
 
+namespace mc {
+// Per-graph data when one device CSR holds many graphs (a batch: the
+// disjoint union, graph g owning vertices [gptr[g], gptr[g+1])).  All null
+// for a single graph, which then uses the compile-time schedule.
+struct BatchView {
+  const int32_t *gid = nullptr;       // vertex -> graph
+  const int32_t *job = nullptr;       // graph -> 0 (triangles) or 1..8 (pattern)
+  const int2 *param = nullptr;        // graph -> {leaf d+ threshold, log2 table factor}
+  unsigned long long *res = nullptr;  // graph -> triangle count
+};
+}  // namespace mc
+
 struct mc_dgraph {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -55,6 +67,7 @@ struct mc_dgraph {
   int hub_table_log2 = 10;
   cudaEvent_t ev[6] = {};
   int64_t launches = 0;  // kernels launched by the current call
+  mc::BatchView batch;   // set by a batch that owns this handle
 };
 
 namespace mc {
@@ -72,4 +85,25 @@ int validate_csr_words(const int64_t *rowptr, const int32_t *col, int64_t n, int
 int tc_count_launch(mc_dgraph *g, cudaEvent_t after_hub, int shard, int num_shards);
 // patterns.cu: result of P<pattern>; c12 (optional) receives counters 1 and 2.
 int pattern_count(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12, mc_timing_t *timing);
+
+// Pattern tasks of a batch (see batch.cu): pattern graphs 0..num_graphs-1.
+struct BatchPatternArgs {
+  const int64_t *rp;          // union CSR
+  const int32_t *ci;
+  int num_graphs;
+  const int32_t *graph;       // pattern graph -> batch graph id
+  const int32_t *job;         // pattern graph -> 1..8
+  const int64_t *v0, *v1;     // pattern graph -> vertex range
+  const int64_t *star_off;    // cumulative P1 star tasks, num_graphs + 1
+  const int64_t *edge_off;    // cumulative directed-edge tasks, num_graphs + 1
+  int32_t *scratch;           // frontier lists
+  int64_t cap;                // list capacity (max degree over pattern graphs)
+  unsigned long long *c1, *c2;  // per batch graph
+  unsigned long long *queue;
+};
+int batch_pattern_launch(const BatchPatternArgs &b, int grid, cudaStream_t s);
+// Blocks of the batch pattern kernel whose frontier lists fit the scratch
+// budget; *warps receives the resident warp count.
+int batch_pattern_grid(int num_sms, int64_t cap, int64_t *warps);
+int pattern_lists();
 }  // namespace mc

@@ -295,18 +295,23 @@ __global__ void init_key_kernel(const int64_t *rowptr, int64_t n, int2 *key) {
 // Tasks each owner contributes to the hub and leaf queues (chunks of its
 // symmetric row), and the largest DAG out-degree.
 __global__ void task_count_kernel(const int2 *key, int64_t n, int32_t *hub_cnt,
-                                  int32_t *leaf_cnt, unsigned long long *max_out) {
+                                  int32_t *leaf_cnt, unsigned long long *max_out, BatchView bv) {
   const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   int32_t d = 0;
   if (v < n) {
     const int2 kv = key[v];
     d = kv.y;
     int32_t h = 0, l = 0;
-    // Owners need d+ >= 1 and a neighbour outside their own out-list
-    // (a partner has d+ <= d+(owner), so an owner with deg == d+ may still
-    // own out-edges: every neighbour counts).
-    if (d >= 1) {
-      if (d > kLeafMaxOut) h = (kv.x + kHubChunk - 1) / kHubChunk;
+    int leaf_max = kLeafMaxOut;
+    bool counted = true;
+    if (bv.gid) {  // batch: only triangle jobs get tasks, with their graph's threshold
+      const int g = bv.gid[v];
+      counted = bv.job[g] == 0;
+      if (bv.param) leaf_max = bv.param[g].x;
+    }
+    // Owners need d+ >= 1; every neighbour of the row may be a partner.
+    if (counted && d >= 1) {
+      if (d > leaf_max) h = (kv.x + kHubChunk - 1) / kHubChunk;
       else l = (kv.x + kLeafChunk - 1) / kLeafChunk;
     }
     hub_cnt[v] = h;
@@ -458,7 +463,7 @@ int tc_orient(mc_dgraph *g) {
     g->launches += 2 + scan_launches(tiles);
   }
   task_count_kernel<<<grid_for(n, 256), 256, 0, s>>>(g->key, n, g->hub_cnt, g->leaf_cnt,
-                                                     g->counters + 3);
+                                                     g->counters + 3, g->batch);
   MC_CUDA_TRY(cudaGetLastError());
   MC_CUDA_TRY(exclusive_scan(g->hub_cnt, g->hub_off, n, g->scan_temp, s));
   MC_CUDA_TRY(exclusive_scan(g->leaf_cnt, g->leaf_off, n, g->scan_temp, s));

@@ -364,7 +364,92 @@ int grid_blocks(mc_dgraph *g, int64_t cap) {
   return (int)std::min(resident, fit);
 }
 
+// ---- batches: many graphs, each with its own pattern ----------------------
+// Largest i in [0, count) with off[i] <= t (off ascending, off[0] == 0).
+__device__ __forceinline__ int find_graph(const int64_t *off, int count, int64_t t) {
+  int lo = 0, hi = count - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(off + mid) <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int P>
+__device__ __forceinline__ void batch_edge(const Warp &w, int v0, int v1, int32_t *L, int64_t cap,
+                                           Acc &acc) {
+  edge_pattern<P>(w, v0, v1, L, cap, acc);
+}
+
+// Persistent warps over the pattern tasks of a batch: first the P1 star
+// tasks (one per vertex of every P1 graph), then one task per directed edge
+// of every pattern graph; each task's counters go to its own graph.
+__global__ void __launch_bounds__(kPatThreads) batch_pattern_kernel(BatchPatternArgs b) {
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
+  int32_t *L = b.scratch + gw * kLists * b.cap;
+  const Warp w{b.rp, b.ci, lane};
+  const int64_t n_star = b.star_off[b.num_graphs], n_edge = b.edge_off[b.num_graphs];
+  for (;;) {
+    unsigned long long t = 0;
+    if (lane == 0) t = atomicAdd(b.queue, 1ull);
+    t = __shfl_sync(kFull, t, 0);
+    if ((int64_t)t >= n_star + n_edge) break;
+    Acc acc;
+    int pg;
+    if ((int64_t)t < n_star) {
+      pg = find_graph(b.star_off, b.num_graphs, (int64_t)t);
+      vertex_star(w, (int)(b.v0[pg] + ((int64_t)t - b.star_off[pg])), L, acc);
+    } else {
+      const int64_t te = (int64_t)t - n_star;
+      pg = find_graph(b.edge_off, b.num_graphs, te);
+      const int64_t vb = b.v0[pg], ve = b.v1[pg];
+      const int64_t e = __ldg(b.rp + vb) + (te - b.edge_off[pg]);
+      const int v0 = (int)upper_row(b.rp, vb, ve - 1, e);
+      const int v1 = __ldg(b.ci + e);
+      switch (b.job[pg]) {
+        case 1: batch_edge<1>(w, v0, v1, L, b.cap, acc); break;
+        case 2: batch_edge<2>(w, v0, v1, L, b.cap, acc); break;
+        case 3: batch_edge<3>(w, v0, v1, L, b.cap, acc); break;
+        case 4: batch_edge<4>(w, v0, v1, L, b.cap, acc); break;
+        case 5: batch_edge<5>(w, v0, v1, L, b.cap, acc); break;
+        case 6: batch_edge<6>(w, v0, v1, L, b.cap, acc); break;
+        case 7: batch_edge<7>(w, v0, v1, L, b.cap, acc); break;
+        default: batch_edge<8>(w, v0, v1, L, b.cap, acc); break;
+      }
+    }
+    const unsigned long long c1 = warp_sum_u64(acc.c1), c2 = warp_sum_u64(acc.c2);
+    if (lane == 0) {
+      const int g = b.graph[pg];
+      if (c1) atomicAdd(b.c1 + g, c1);
+      if (c2) atomicAdd(b.c2 + g, c2);
+    }
+  }
+}
+
 }  // namespace
+
+int batch_pattern_launch(const BatchPatternArgs &b, int grid, cudaStream_t s) {
+  batch_pattern_kernel<<<grid, kPatThreads, 0, s>>>(b);
+  MC_CUDA_TRY(cudaGetLastError());
+  return MC_OK;
+}
+
+int batch_pattern_grid(int num_sms, int64_t cap, int64_t *warps) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_pattern_kernel, kPatThreads,
+                                                    0) != cudaSuccess)
+    per_sm = 4;
+  const int64_t resident = (int64_t)num_sms * std::max(per_sm, 1);
+  const int64_t block_bytes = (int64_t)(kPatThreads / kWarp) * kLists * cap * 4;
+  const int64_t fit = std::max<int64_t>(1, (int64_t)kScratchBudget / block_bytes);
+  const int grid = (int)std::min(resident, fit);
+  *warps = (int64_t)grid * (kPatThreads / kWarp);
+  return grid;
+}
+
+int pattern_lists() { return kLists; }
 
 int pattern_count(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12, mc_timing_t *timing) {
   cudaStream_t s = g->stream;

@@ -40,7 +40,22 @@ struct CountArgs {
   unsigned *err;
   int table_log2_max;
   int shard, num_shards;  // this call counts tasks shard, shard + num_shards, ...
+  BatchView bv;           // per-graph table factor and counts of a batch
 };
+
+// log2 of the table slots per key of owner x's graph (4 slots per key by
+// default: load <= 1/4).
+__device__ __forceinline__ int table_factor_log2(const CountArgs &a, int x) {
+  return a.bv.param ? a.bv.param[a.bv.gid[x]].y : 2;
+}
+
+// A batch adds each task's hits to its graph's count (one atomic per warp).
+__device__ __forceinline__ void flush_task(const CountArgs &a, int x, unsigned long long task_hits,
+                                           int lane) {
+  if (!a.bv.res) return;
+  task_hits = warp_sum_u64(task_hits);
+  if (lane == 0 && task_hits) atomicAdd(a.bv.res + a.bv.gid[x], task_hits);
+}
 
 // Tasks of this shard: queue position t maps to task t * num_shards + shard.
 __device__ __forceinline__ int64_t shard_tasks(const CountArgs &a) {
@@ -60,13 +75,19 @@ __device__ __forceinline__ void cuckoo_slots(int key, int shift, unsigned &s1, u
   s2 = s1 ^ ((((unsigned)key * 0x85EBCA77u) >> shift) | 1u);
 }
 
+// A key always enters at s1 and moves to s2 only when another key takes s1,
+// and a filled slot never empties: so an empty s1 means the key is absent,
+// and s2 is read only when s1 holds a different key.
 struct CuckooProbe {
   const int *tab;
   int shift;
   __device__ __forceinline__ unsigned operator()(int w) const {
     unsigned s1, s2;
     cuckoo_slots(w, shift, s1, s2);
-    return (unsigned)(tab[s1] == w) | (unsigned)(tab[s2] == w);
+    const int t1 = tab[s1];
+    unsigned hit = t1 == w;
+    if (t1 >= 0 && t1 != w) hit = tab[s2] == w;
+    return hit;
   }
 };
 
@@ -249,9 +270,10 @@ __global__ void __launch_bounds__(kCountThreads, 5) tc_hub_kernel(CountArgs a) {
     const int d = a.key[x].y;
     const int64_t e0 = a.rowptr[x] + (int64_t)chunk * kHubChunk;
     const int nc = (int)min((int64_t)kHubChunk, a.rowptr[x + 1] - e0);
-    int lg = max(8, ceil_log2(4 * d));
+    int lg = max(8, ceil_log2(d << table_factor_log2(a, x)));
     if (lg > a.table_log2_max && 2 * d <= (1 << a.table_log2_max)) lg = a.table_log2_max;
     bool use_table = lg <= a.table_log2_max;
+    unsigned long long th = 0;
     if (use_table) {
       const int size = 1 << lg;
       const int shift = 32 - lg;
@@ -265,10 +287,12 @@ __global__ void __launch_bounds__(kCountThreads, 5) tc_hub_kernel(CountArgs a) {
       __syncthreads();
       use_table = s_fail == 0;
       if (use_table)
-        hits += claim_and_stream(a, x, d, e0, nc, &s_next, lane, CuckooProbe{table, shift});
+        th = claim_and_stream(a, x, d, e0, nc, &s_next, lane, CuckooProbe{table, shift});
     }
     if (!use_table)
-      hits += claim_and_stream(a, x, d, e0, nc, &s_next, lane, ListProbe{a.dag_col + a0, d});
+      th = claim_and_stream(a, x, d, e0, nc, &s_next, lane, ListProbe{a.dag_col + a0, d});
+    hits += th;
+    flush_task(a, x, th, lane);
     __syncthreads();  // table and the shared words are rewritten by the next task
   }
   hits = warp_sum_u64(hits);
@@ -327,6 +351,7 @@ __global__ void __launch_bounds__(kCountThreads) tc_leaf_kernel(CountArgs a) {
     for (int i = lane; i < d; i += kWarp) ok &= cuckoo_insert(tab, 32 - lg, __ldg(a.dag_col + a0 + i));
     const bool use_table = __all_sync(kFull, ok);
     __syncwarp();
+    unsigned long long th = 0;
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
       int64_t st = pst[r];
@@ -343,9 +368,11 @@ __global__ void __launch_bounds__(kCountThreads) tc_leaf_kernel(CountArgs a) {
       st = lane < k ? c_st[warp][lane] : 0;
       len = lane < k ? c_len[warp][lane] : 0;
       __syncwarp();
-      if (use_table) hits += stream_flat(a.dag_col, st, len, lane, probe);
-      else hits += stream_flat(a.dag_col, st, len, lane, ListProbe{a.dag_col + a0, d});
+      if (use_table) th += stream_flat(a.dag_col, st, len, lane, probe);
+      else th += stream_flat(a.dag_col, st, len, lane, ListProbe{a.dag_col + a0, d});
     }
+    hits += th;
+    flush_task(a, x, th, lane);
     __syncwarp();
   }
   hits = warp_sum_u64(hits);
@@ -377,6 +404,7 @@ int tc_count_launch(mc_dgraph *g, cudaEvent_t after_hub, int shard, int num_shar
   a.table_log2_max = g->hub_table_log2;
   a.shard = shard;
   a.num_shards = num_shards;
+  a.bv = g->batch;
 
   const size_t hub_smem = sizeof(int) << g->hub_table_log2;
   MC_CUDA_TRY(cudaFuncSetAttribute(tc_hub_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
