@@ -211,6 +211,39 @@ int mc_batch_autotune(mc_batch_t *b, int32_t *choice);
 int mc_batch_count(mc_batch_t *b, uint64_t *counts, mc_timing_t *timing);
 void mc_batch_free(mc_batch_t *b);
 
+/* ---- serving ---------------------------------------------------------------
+ * A request loop with continuous batching (no reference counterpart).
+ * Worker threads (each with its own stream) take every queued request that
+ * fits the HBM budget -- up to max_batch per batch, in arrival order --
+ * assemble the batch on the device, count it with the batch kernels and
+ * deliver each graph's count; requests that arrive while batches run are
+ * admitted as memory is returned, and batches of different workers overlap
+ * on the device.  A request with a non-zero key leaves its CSR resident on
+ * the device (within the budget, least recently used evicted first); later
+ * requests with that key may pass NULL arrays.  A request that cannot fit
+ * the budget even alone fails with MC_ERR_BUDGET.  Counts equal the
+ * single-graph results. */
+typedef struct mc_server mc_server_t;
+typedef struct mc_server_stats {
+  int64_t submitted, completed, failed, batches, cache_hits;
+  int64_t cache_bytes, cached_graphs, queued, max_batch_seen;
+} mc_server_stats_t;
+int mc_server_create(int64_t hbm_budget_bytes, int max_batch, int workers,
+                     mc_server_t **out);
+/* Copies the graph (unless `key` is resident) and queues it; *ticket names
+ * the request for mc_server_wait.  job: 0 triangles, 1..8 pattern P1..P8. */
+int mc_server_submit(mc_server_t *s, const int64_t *rowptr, const int32_t *col,
+                     int64_t n, int64_t nnz, int job, uint64_t key,
+                     uint64_t *ticket);
+/* Waits up to timeout_ms (MC_ERR_TIMEOUT after that; the ticket stays
+ * valid); on completion returns the request's status, its count and its
+ * latency from submission to result. */
+int mc_server_wait(mc_server_t *s, uint64_t ticket, int timeout_ms,
+                   uint64_t *count, double *latency_ms);
+int mc_server_stats(mc_server_t *s, mc_server_stats_t *stats);
+/* Finishes the queued requests, stops the workers, frees the cache. */
+void mc_server_free(mc_server_t *s);
+
 /* One-shot drop-in for TCSolver: host CSR in, count out.  Uploads, orients,
  * counts and copies the result back inside the call (timing->h2d_ms etc.).
  * Device buffers are cached in a per-thread context and reused while the

@@ -103,6 +103,11 @@ SIGNATURES = {
     "mc_batch_autotune": (C.c_int, [_P, _P]),
     "mc_batch_count": (C.c_int, [_P, _PU64, C.POINTER(Timing)]),
     "mc_batch_free": (None, [_P]),
+    "mc_server_create": (C.c_int, [_I64, C.c_int, C.c_int, _PP]),
+    "mc_server_submit": (C.c_int, [_P, _P, _P, _I64, _I64, C.c_int, C.c_uint64, _PU64]),
+    "mc_server_wait": (C.c_int, [_P, C.c_uint64, C.c_int, _PU64, C.POINTER(C.c_double)]),
+    "mc_server_stats": (C.c_int, [_P, _P]),
+    "mc_server_free": (None, [_P]),
 }
 
 

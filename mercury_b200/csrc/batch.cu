@@ -120,9 +120,10 @@ void batch_release(mc_batch *b) {
   void *bufs[] = {b->d_gptr, b->d_gid, b->d_job, b->d_job_active, b->d_param, b->d_res, b->d_out,
                   (void *)b->pa.graph, (void *)b->pa.job, (void *)b->pa.v0, (void *)b->pa.v1,
                   (void *)b->pa.star_off, (void *)b->pa.edge_off, b->pa.scratch, b->pa.queue};
-  for (void *p : bufs)
-    if (p) cudaFree(p);
-  if (b->h_out) cudaFreeHost(b->h_out);
+  if (b->g)
+    for (void *p : bufs)
+      if (p) dev_free(p, b->g->stream);
+  delete[] b->h_out;
   if (b->e0) cudaEventDestroy(b->e0);
   if (b->e1) cudaEventDestroy(b->e1);
   if (b->g) mc_dgraph_free(b->g);
@@ -167,9 +168,17 @@ int enqueue(mc_batch *b) {
   combine_kernel<<<blocks(G, 256), 256, 0, s>>>(b->d_job, b->d_res, G, b->d_out);
   MC_CUDA_TRY(cudaGetLastError());
   g->launches += 1;
-  MC_CUDA_TRY(cudaMemcpyAsync(b->h_out, b->d_out, sizeof(unsigned long long) * G,
-                              cudaMemcpyDeviceToHost, s));
-  MC_CUDA_TRY(cudaMemcpyAsync(g->h_err, g->err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  return MC_OK;
+}
+
+// Counts and the error word to the host, after the stream reached them.
+int read_back(mc_batch *b) {
+  mc_dgraph *g = b->g;
+  MC_CUDA_TRY(cudaMemcpyAsync(b->h_out, b->d_out, sizeof(unsigned long long) * b->num_graphs,
+                              cudaMemcpyDeviceToHost, g->stream));
+  MC_CUDA_TRY(cudaMemcpyAsync(g->h_err, g->err, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                              g->stream));
+  MC_CUDA_TRY(cudaStreamSynchronize(g->stream));
   return MC_OK;
 }
 
@@ -210,12 +219,16 @@ int upload_params(mc_batch *b) {
 
 using mc::batch_release;
 
-extern "C" {
+namespace mc {
 
-int mc_batch_create(const int64_t *rowptr, const int32_t *col, int64_t n, int64_t nnz,
-                    const int64_t *graph_vptr, int num_graphs, const int32_t *jobs, void *stream,
-                    mc_batch_t **out) {
-  using namespace mc;
+// Builds a batch from a union CSR held in host memory (device_csr false) or
+// device memory (true), with each graph's largest degree and entry count
+// given by the caller (gmaxdeg, gnnz); with do_capture the count sequence is
+// captured as a CUDA graph, otherwise every count launches it directly.
+int batch_create(const int64_t *rowptr, const int32_t *col, bool device_csr, int64_t n,
+                 int64_t nnz, const int64_t *graph_vptr, int num_graphs, const int32_t *jobs,
+                 const int64_t *gmaxdeg, const int64_t *gnnz_of, void *stream, bool do_capture,
+                 mc_batch_t **out) {
   if (!out || !rowptr || !graph_vptr || !jobs || num_graphs < 1 || n < 0 || nnz < 0)
     return MC_ERR_ARG;
   *out = nullptr;
@@ -236,21 +249,20 @@ int mc_batch_create(const int64_t *rowptr, const int32_t *col, int64_t n, int64_
     batch_release(b);
     return rc;
   };
-  int rc = mc_dgraph_create(rowptr, col, n, nnz, stream, 0, &b->g);
+  int rc = device_csr ? mc_dgraph_create_device(rowptr, col, n, nnz, stream, 0, &b->g)
+                      : mc_dgraph_create(rowptr, col, n, nnz, stream, 0, &b->g);
   if (rc != MC_OK) return fail(rc);
   mc_dgraph *g = b->g;
   cudaStream_t s = g->stream;
   const int G = num_graphs;
-  // Per-graph sizes from the host arrays: largest degree and a bound on d+
-  // (d+(v)^2 <= the graph's nnz, as every out-neighbour has degree >= d+(v)).
+  // Per-graph sizes: largest degree and a bound on d+ (d+(v)^2 <= the
+  // graph's nnz, as every out-neighbour has degree >= d+(v)).
   int64_t pat_cap = 1;
   std::vector<int32_t> pg_graph, pg_job;
   std::vector<int64_t> pg_v0, pg_v1, star_off(1, 0), edge_off(1, 0);
   for (int i = 0; i < G; ++i) {
-    int64_t md = 0;
-    for (int64_t v = graph_vptr[i]; v < graph_vptr[i + 1]; ++v)
-      md = std::max<int64_t>(md, rowptr[v + 1] - rowptr[v]);
-    const int64_t gnnz = rowptr[graph_vptr[i + 1]] - rowptr[graph_vptr[i]];
+    const int64_t md = gmaxdeg[i];
+    const int64_t gnnz = gnnz_of[i];
     if (jobs[i] == 0) {
       b->has_tc = true;
       b->bucket[i] = degree_bucket(md);
@@ -266,7 +278,7 @@ int mc_batch_create(const int64_t *rowptr, const int32_t *col, int64_t n, int64_
       edge_off.push_back(edge_off.back() + gnnz);
     }
   }
-  auto alloc = [](void **p, size_t bytes) { return cudaMalloc(p, std::max<size_t>(bytes, 8)); };
+  auto alloc = [s](void **p, size_t bytes) { return dev_alloc(p, bytes, s); };
 #define MC_BALLOC(ptr, bytes) MC_CUDA_TRY(alloc((void **)&(ptr), (bytes)))
   try {
     MC_BALLOC(b->d_gptr, sizeof(int64_t) * (G + 1));
@@ -276,7 +288,7 @@ int mc_batch_create(const int64_t *rowptr, const int32_t *col, int64_t n, int64_
     MC_BALLOC(b->d_param, sizeof(int2) * G);
     MC_BALLOC(b->d_res, sizeof(unsigned long long) * 3 * G);
     MC_BALLOC(b->d_out, sizeof(unsigned long long) * G);
-    MC_CUDA_TRY(cudaMallocHost((void **)&b->h_out, sizeof(unsigned long long) * G));
+    b->h_out = new unsigned long long[G]();
     MC_CUDA_TRY(cudaEventCreate(&b->e0));
     MC_CUDA_TRY(cudaEventCreate(&b->e1));
     MC_CUDA_TRY(cudaMemcpyAsync(b->d_gptr, graph_vptr, sizeof(int64_t) * (G + 1),
@@ -339,10 +351,34 @@ int mc_batch_create(const int64_t *rowptr, const int32_t *col, int64_t n, int64_
 #undef MC_BALLOC
   MC_CUDA_TRY(cudaStreamSynchronize(s));
   size_tables(b);
-  rc = capture(b);
-  if (rc != MC_OK) return fail(rc);
+  if (do_capture) {
+    rc = capture(b);
+    if (rc != MC_OK) return fail(rc);
+  }
   *out = b;
   return MC_OK;
+}
+
+}  // namespace mc
+
+extern "C" {
+
+int mc_batch_create(const int64_t *rowptr, const int32_t *col, int64_t n, int64_t nnz,
+                    const int64_t *graph_vptr, int num_graphs, const int32_t *jobs, void *stream,
+                    mc_batch_t **out) {
+  if (!rowptr || !graph_vptr || num_graphs < 1 || n < 0) return MC_ERR_ARG;
+  if (graph_vptr[0] != 0 || graph_vptr[num_graphs] != n) return MC_ERR_ARG;
+  for (int i = 0; i < num_graphs; ++i)
+    if (graph_vptr[i + 1] < graph_vptr[i]) return MC_ERR_ARG;
+  // Per-graph largest degree and entry count from the host arrays.
+  std::vector<int64_t> md(num_graphs, 0), gnnz(num_graphs, 0);
+  for (int i = 0; i < num_graphs; ++i) {
+    for (int64_t v = graph_vptr[i]; v < graph_vptr[i + 1]; ++v)
+      md[i] = std::max<int64_t>(md[i], rowptr[v + 1] - rowptr[v]);
+    gnnz[i] = rowptr[graph_vptr[i + 1]] - rowptr[graph_vptr[i]];
+  }
+  return mc::batch_create(rowptr, col, false, n, nnz, graph_vptr, num_graphs, jobs, md.data(),
+                          gnnz.data(), stream, true, out);
 }
 
 int mc_batch_count(mc_batch_t *b, uint64_t *counts, mc_timing_t *timing) {
@@ -350,9 +386,15 @@ int mc_batch_count(mc_batch_t *b, uint64_t *counts, mc_timing_t *timing) {
   MC_CUDA_TRY(cudaSetDevice(b->g->device));
   cudaStream_t s = b->g->stream;
   MC_CUDA_TRY(cudaEventRecord(b->e0, s));
-  MC_CUDA_TRY(cudaGraphLaunch(b->exec, s));
+  if (b->exec) {
+    MC_CUDA_TRY(cudaGraphLaunch(b->exec, s));
+  } else {
+    const int erc = mc::enqueue(b);
+    if (erc != MC_OK) return erc;
+  }
   MC_CUDA_TRY(cudaEventRecord(b->e1, s));
-  MC_CUDA_TRY(cudaStreamSynchronize(s));
+  const int rc = mc::read_back(b);
+  if (rc != MC_OK) return rc;
   if (*b->g->h_err) return MC_ERR_DEVICE;
   std::memcpy(counts, b->h_out, sizeof(uint64_t) * b->num_graphs);
   if (timing) {
@@ -397,7 +439,7 @@ int mc_batch_autotune(mc_batch_t *b, int32_t *choice) {
             MC_CUDA_TRY(cudaEventRecord(b->e0, s));
             rc = enqueue(b);
             MC_CUDA_TRY(cudaEventRecord(b->e1, s));
-            MC_CUDA_TRY(cudaStreamSynchronize(s));
+            if (rc == MC_OK) rc = read_back(b);
             cudaEventElapsedTime(&ms, b->e0, b->e1);
           }
           if (rc == MC_OK && *b->g->h_err) rc = MC_ERR_DEVICE;

@@ -32,6 +32,13 @@ enum DeviceError : unsigned {
 
 void set_last_cuda_error(cudaError_t e);
 
+// Device buffers come from the stream-ordered allocator on the owning
+// handle's stream: freeing one never waits for the whole device.
+inline cudaError_t dev_alloc(void **p, size_t bytes, cudaStream_t s) {
+  return cudaMallocAsync(p, bytes < 8 ? 8 : bytes, s);
+}
+inline void dev_free(void *p, cudaStream_t s) { cudaFreeAsync(p, s); }
+
 __device__ __forceinline__ int warp_inclusive_scan(int v, int lane) {
 #pragma unroll
   for (int o = 1; o < kWarp; o <<= 1) {

@@ -24,14 +24,16 @@ void release(mc_dgraph *g) {
   int prev = -1;
   cudaGetDevice(&prev);
   cudaSetDevice(g->device);
-  if (g->stream) cudaStreamSynchronize(g->stream);
   void *bufs[] = {g->rowptr,     g->col,        g->key,      g->dag_rowptr,
                   g->dag_col,    g->keep,       g->tile_counts, g->tile_offsets,
                   g->hub_cnt,    g->leaf_cnt,   g->hub_off,  g->leaf_off,  g->hub_tasks,
                   g->leaf_tasks, g->scan_temp,  g->counters, g->err, g->pat_scratch};
+  // Stream-ordered frees: no device-wide synchronisation, so other handles'
+  // work keeps running while this one is released.
   for (void *p : bufs)
-    if (p) cudaFree(p);
-  if (g->h_counters) cudaFreeHost(g->h_counters);
+    if (p) dev_free(p, g->stream);
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  delete[] g->h_counters;
   for (cudaEvent_t e : g->ev)
     if (e) cudaEventDestroy(e);
   if (g->own_stream && g->stream) cudaStreamDestroy(g->stream);
@@ -58,11 +60,14 @@ int create_common(int64_t n, int64_t nnz, void *stream, mc_dgraph **out, mc_dgra
   }
   g->n = n;
   g->nnz = nnz;
-  MC_CUDA_TRY(cudaMalloc((void **)&g->rowptr, sizeof(int64_t) * (size_t)(n + 1)));
-  MC_CUDA_TRY(cudaMalloc((void **)&g->col, sizeof(int32_t) * (size_t)std::max<int64_t>(nnz, 1)));
-  MC_CUDA_TRY(cudaMalloc((void **)&g->counters, sizeof(unsigned long long) * 8));
-  MC_CUDA_TRY(cudaMalloc((void **)&g->err, sizeof(unsigned)));
-  MC_CUDA_TRY(cudaMallocHost((void **)&g->h_counters, sizeof(unsigned long long) * 8 + 64));
+  MC_CUDA_TRY(dev_alloc((void **)&g->rowptr, sizeof(int64_t) * (size_t)(n + 1), g->stream));
+  MC_CUDA_TRY(dev_alloc((void **)&g->col, sizeof(int32_t) * (size_t)std::max<int64_t>(nnz, 1),
+                        g->stream));
+  MC_CUDA_TRY(dev_alloc((void **)&g->counters, sizeof(unsigned long long) * 8, g->stream));
+  MC_CUDA_TRY(dev_alloc((void **)&g->err, sizeof(unsigned), g->stream));
+  // Host mirror of the counters (read after a stream synchronisation).
+  g->h_counters = new (std::nothrow) unsigned long long[16]();
+  if (!g->h_counters) return MC_ERR_OOM;
   g->h_err = reinterpret_cast<unsigned *>(g->h_counters + 8);
   for (cudaEvent_t &e : g->ev) MC_CUDA_TRY(cudaEventCreate(&e));
   return MC_OK;

@@ -102,6 +102,11 @@ struct BatchPatternArgs {
   unsigned long long *queue;
 };
 int batch_pattern_launch(const BatchPatternArgs &b, int grid, cudaStream_t s);
+// batch.cu: a batch over a host (device_csr false) or device union CSR.
+int batch_create(const int64_t *rowptr, const int32_t *col, bool device_csr, int64_t n,
+                 int64_t nnz, const int64_t *graph_vptr, int num_graphs, const int32_t *jobs,
+                 const int64_t *gmaxdeg, const int64_t *gnnz_of, void *stream, bool do_capture,
+                 mc_batch_t **out);
 // Blocks of the batch pattern kernel whose frontier lists fit the scratch
 // budget; *warps receives the resident warp count.
 int batch_pattern_grid(int num_sms, int64_t cap, int64_t *warps);

@@ -419,7 +419,8 @@ int tc_alloc(mc_dgraph *g) {
   // Each owner contributes ceil(deg / chunk) <= 1 + deg / chunk tasks.
   g->task_capacity = n + cap / std::min(kHubChunk, kLeafChunk) + 1;
   g->scan_temp_size = std::max(scan_temp_bytes(n + 1), scan_temp_bytes(tiles + 1));
-#define MC_ALLOC(ptr, count) MC_CUDA_TRY(cudaMalloc((void **)&(ptr), sizeof(*(ptr)) * (size_t)(count)))
+#define MC_ALLOC(ptr, count) \
+  MC_CUDA_TRY(dev_alloc((void **)&(ptr), sizeof(*(ptr)) * (size_t)(count), g->stream))
   MC_ALLOC(g->key, n + 1);
   MC_ALLOC(g->dag_rowptr, n + 1);
   MC_ALLOC(g->dag_col, cap);
@@ -432,7 +433,7 @@ int tc_alloc(mc_dgraph *g) {
   MC_ALLOC(g->leaf_off, n + 1);
   MC_ALLOC(g->hub_tasks, g->task_capacity);
   MC_ALLOC(g->leaf_tasks, g->task_capacity);
-  MC_CUDA_TRY(cudaMalloc(&g->scan_temp, g->scan_temp_size));
+  MC_CUDA_TRY(dev_alloc(&g->scan_temp, g->scan_temp_size, g->stream));
 #undef MC_ALLOC
   g->tc_ready = true;
   return MC_OK;

@@ -461,10 +461,10 @@ int pattern_count(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12, mc_ti
   const int64_t warps = (int64_t)grid * (kPatThreads / kWarp);
   const size_t need = sizeof(int32_t) * (size_t)(warps * kLists * cap);
   if (need > g->pat_scratch_bytes) {
-    if (g->pat_scratch) cudaFree(g->pat_scratch);
+    if (g->pat_scratch) dev_free(g->pat_scratch, s);
     g->pat_scratch = nullptr;
     g->pat_scratch_bytes = 0;
-    MC_CUDA_TRY(cudaMalloc(&g->pat_scratch, need));
+    MC_CUDA_TRY(dev_alloc(&g->pat_scratch, need, s));
     g->pat_scratch_bytes = need;
   }
   PatArgs a{g->rowptr, g->col, g->n, g->nnz, static_cast<int32_t *>(g->pat_scratch), cap,
