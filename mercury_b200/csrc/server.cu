@@ -48,6 +48,7 @@ struct Request {
   std::vector<int32_t> col;
   int64_t n = 0, nnz = 0, max_degree = 0;
   Clock::time_point submitted;
+  bool prepinned = false;  // resident graph pinned at submission (no arrays copied)
   bool done = false;
   int status = MC_OK;
   uint64_t count = 0;
@@ -194,7 +195,7 @@ void run_batch(mc_server *s, std::vector<std::shared_ptr<Request>> &batch, int64
         r.n = it->second.n;
         r.nnz = it->second.nnz;
         r.max_degree = it->second.max_degree;
-        ++it->second.pins;
+        if (!r.prepinned) ++it->second.pins;  // a prepinned request holds its pin already
         pinned.push_back(r.key);
         cached = true;
         ++s->stats.cache_hits;
@@ -319,6 +320,10 @@ void worker_main(mc_server *s) {
           const int64_t cap = r->job != 0 ? std::max(pattern_cap, r->max_degree) : pattern_cap;
           if (cap > pattern_cap) f += pattern_scratch(cap) - (pattern_cap ? pattern_scratch(pattern_cap) : 0);
           if (f > s->budget) {  // can never fit: refuse it
+            if (r->prepinned) {
+              auto c = s->cache.find(r->key);
+              if (c != s->cache.end() && c->second.pins > 0) --c->second.pins;
+            }
             r->status = MC_ERR_BUDGET;
             r->done = true;
             r->latency_ms = ms_since(r->submitted);
@@ -379,10 +384,14 @@ int mc_server_submit(mc_server_t *s, const int64_t *rowptr, const int32_t *col, 
     std::lock_guard<std::mutex> lock(s->mu);
     auto it = key ? s->cache.find(key) : s->cache.end();
     if (it != s->cache.end()) {
+      // Resident: pin it now so it cannot be evicted before a worker runs
+      // this request (the batch that runs it drops the pin).
       cached = true;
       r->n = it->second.n;
       r->nnz = it->second.nnz;
       r->max_degree = it->second.max_degree;
+      ++it->second.pins;
+      r->prepinned = true;
     }
   }
   if (!cached) {
@@ -401,7 +410,13 @@ int mc_server_submit(mc_server_t *s, const int64_t *rowptr, const int32_t *col, 
   r->submitted = mc::Clock::now();
   {
     std::lock_guard<std::mutex> lock(s->mu);
-    if (s->stop) return MC_ERR_ARG;
+    if (s->stop) {
+      if (r->prepinned) {
+        auto c = s->cache.find(key);
+        if (c != s->cache.end() && c->second.pins > 0) --c->second.pins;
+      }
+      return MC_ERR_ARG;
+    }
     r->ticket = s->next_ticket++;
     s->tickets[r->ticket] = r;
     s->pending.push_back(r);
