@@ -276,6 +276,27 @@ def run_reference(a, rank, world):
     return 0
 
 
+# ---------------------------------------------------------------- ranks
+def combine_ranks(partial_count: int, elapsed_ms: float, device):
+    """Sum of the ranks' partial counts and the max of their times (the
+    reference's MPI_Reduce SUM and MAX, tc_multigpu/tc_challenge_multigpu.cu
+    :198-206), over the default process group."""
+    import torch
+    import torch.distributed as dist
+    c = torch.tensor([partial_count], dtype=torch.int64, device=device)
+    t = torch.tensor([elapsed_ms], dtype=torch.float64, device=device)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return int(c.item()), float(t.item())
+
+
+def shard_of(rank: int, world: int):
+    """(shard, num_shards) this rank counts: tasks are dealt round-robin."""
+    if not 0 <= rank < world:
+        raise ValueError("rank outside the world")
+    return rank, world
+
+
 # ---------------------------------------------------------------- GPU side
 def run_ours(a, rank, world, local_rank):
     import torch
@@ -296,11 +317,10 @@ def run_ours(a, rank, world, local_rank):
     def step():
         if world == 1:
             return dg.tc_count(), dg.last_timing
-        part = dg.tc_count_shard(rank, world)
+        part = dg.tc_count_shard(*shard_of(rank, world))
         t = dg.last_timing
-        buf = torch.tensor([part], dtype=torch.int64, device="cuda")
-        dist.all_reduce(buf)
-        return int(buf.item()), t
+        total, _ = combine_ranks(part, t.total_ms, "cuda")
+        return total, t
 
     first = None
     for _ in range(a.warmup):
@@ -329,9 +349,7 @@ def run_ours(a, rank, world, local_rank):
     torch.cuda.synchronize()
     total_ms = ev0.elapsed_time(ev1)
     if world > 1:
-        tt = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
+        _, total_ms = combine_ranks(0, total_ms, "cuda")
         dist.barrier()
     ms_per_step = total_ms / a.steps
     value = m / (ms_per_step / 1e3)
