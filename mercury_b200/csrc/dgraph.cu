@@ -27,7 +27,8 @@ void release(mc_dgraph *g) {
   void *bufs[] = {g->rowptr,     g->col,        g->key,      g->dag_rowptr,
                   g->dag_col,    g->keep,       g->tile_counts, g->tile_offsets,
                   g->hub_cnt,    g->leaf_cnt,   g->hub_off,  g->leaf_off,  g->hub_tasks,
-                  g->leaf_tasks, g->scan_temp,  g->counters, g->err, g->pat_scratch};
+                  g->leaf_tasks, g->scan_temp,  g->counters, g->err, g->pat_scratch,
+                  g->mega_cnt,   g->mega_off,   g->mega_tasks};
   // Stream-ordered frees: no device-wide synchronisation, so other handles'
   // work keeps running while this one is released.
   for (void *p : bufs)
@@ -101,9 +102,10 @@ int tc_stats(mc_dgraph *g, mc_tc_stats_t *st) {
   st->n = g->n;
   st->nnz = g->nnz;
   if (!g->tc_ready || g->n == 0) return MC_OK;
-  int64_t v[3] = {0, 0, 0};
-  const int64_t *src[3] = {g->dag_rowptr + g->n, g->hub_off + g->n, g->leaf_off + g->n};
-  for (int i = 0; i < 3; ++i)
+  int64_t v[4] = {0, 0, 0, 0};
+  const int64_t *src[4] = {g->dag_rowptr + g->n, g->hub_off + g->n, g->leaf_off + g->n,
+                           g->mega_off + g->n};
+  for (int i = 0; i < 4; ++i)
     MC_CUDA_TRY(cudaMemcpyAsync(&v[i], src[i], sizeof(int64_t), cudaMemcpyDeviceToHost, g->stream));
   unsigned long long maxd = 0;
   MC_CUDA_TRY(cudaMemcpyAsync(&maxd, g->counters + 3, sizeof(maxd), cudaMemcpyDeviceToHost,
@@ -113,7 +115,7 @@ int tc_stats(mc_dgraph *g, mc_tc_stats_t *st) {
   const int rc = tc_partner_stats(g, &pe, &work);
   if (rc != MC_OK) return rc;
   st->dag_edges = v[0];
-  st->hub_tasks = v[1];
+  st->hub_tasks = v[1] + v[3];  // both table-size classes
   st->leaf_tasks = v[2];
   st->partner_edges = (int64_t)pe;
   st->max_out_degree = (int64_t)maxd;

@@ -15,6 +15,10 @@ constexpr int kHubChunk = 512;             // owner's neighbours per CTA (hub) t
 constexpr int kLeafChunk = 64;             // owner's neighbours per warp (leaf) task
 constexpr int kCountThreads = 256;         // threads per counting CTA
 constexpr int kHubTableLog2Max = 15;       // at most 32768 slots (128 KB smem)
+// Hub owners up to this d+ run in a launch with small tables (16 KB, high
+// occupancy); larger ones in a launch sized for the largest table.
+constexpr int kHubSmallMaxOut = 1024;
+constexpr int kHubSmallTableLog2 = 12;
 }  // namespace mc
 
 namespace mc {
@@ -51,14 +55,14 @@ struct mc_dgraph {
   uint16_t *keep = nullptr;       // one DAG keep mask per orientation thread
   int32_t *tile_counts = nullptr; // tiles
   int64_t *tile_offsets = nullptr;// tiles + 1
-  int32_t *hub_cnt = nullptr, *leaf_cnt = nullptr;      // n
-  int64_t *hub_off = nullptr, *leaf_off = nullptr;      // n + 1
-  uint64_t *hub_tasks = nullptr, *leaf_tasks = nullptr; // capacity
+  int32_t *hub_cnt = nullptr, *leaf_cnt = nullptr, *mega_cnt = nullptr;    // n
+  int64_t *hub_off = nullptr, *leaf_off = nullptr, *mega_off = nullptr;    // n + 1
+  uint64_t *hub_tasks = nullptr, *leaf_tasks = nullptr, *mega_tasks = nullptr;  // capacity
   int64_t task_capacity = 0;
   void *scan_temp = nullptr;
   size_t scan_temp_size = 0;
-  // 0: result, 1: hub queue, 2: leaf queue, 3: max d+, 4: probe work,
-  // 5: partner edges, 7: max degree (validation)
+  // 0: result, 1: hub queue, 2: leaf queue, 3: max d+, 4-5: partner
+  // statistics, 6: large-table hub queue, 7: max degree (validation)
   unsigned long long *counters = nullptr;
   unsigned *err = nullptr;
   // pinned host mirror of counters + err

@@ -292,16 +292,17 @@ __global__ void init_key_kernel(const int64_t *rowptr, int64_t n, int2 *key) {
   if (v < n) key[v] = make_int2((int)(rowptr[v + 1] - rowptr[v]), 0);
 }
 
-// Tasks each owner contributes to the hub and leaf queues (chunks of its
-// symmetric row), and the largest DAG out-degree.
+// Tasks each owner contributes to the hub, large-table hub and leaf queues
+// (chunks of its symmetric row), and the largest DAG out-degree.
 __global__ void task_count_kernel(const int2 *key, int64_t n, int32_t *hub_cnt,
-                                  int32_t *leaf_cnt, unsigned long long *max_out, BatchView bv) {
+                                  int32_t *leaf_cnt, int32_t *mega_cnt,
+                                  unsigned long long *max_out, BatchView bv) {
   const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   int32_t d = 0;
   if (v < n) {
     const int2 kv = key[v];
     d = kv.y;
-    int32_t h = 0, l = 0;
+    int32_t h = 0, l = 0, m = 0;
     int leaf_max = kLeafMaxOut;
     bool counted = true;
     if (bv.gid) {  // batch: only triangle jobs get tasks, with their graph's threshold
@@ -311,11 +312,13 @@ __global__ void task_count_kernel(const int2 *key, int64_t n, int32_t *hub_cnt,
     }
     // Owners need d+ >= 1; every neighbour of the row may be a partner.
     if (counted && d >= 1) {
-      if (d > leaf_max) h = (kv.x + kHubChunk - 1) / kHubChunk;
-      else l = (kv.x + kLeafChunk - 1) / kLeafChunk;
+      if (d <= leaf_max) l = (kv.x + kLeafChunk - 1) / kLeafChunk;
+      else if (d <= kHubSmallMaxOut) h = (kv.x + kHubChunk - 1) / kHubChunk;
+      else m = (kv.x + kHubChunk - 1) / kHubChunk;
     }
     hub_cnt[v] = h;
     leaf_cnt[v] = l;
+    mega_cnt[v] = m;
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) d = max(d, __shfl_down_sync(kFull, d, o));
@@ -324,13 +327,15 @@ __global__ void task_count_kernel(const int2 *key, int64_t n, int32_t *hub_cnt,
 
 // Task word: owner id in the high half, chunk index in the low half.
 __global__ void task_fill_kernel(const int32_t *hub_cnt, const int64_t *hub_off,
-                                 const int32_t *leaf_cnt, const int64_t *leaf_off, int64_t n,
-                                 uint64_t *hub_tasks, uint64_t *leaf_tasks) {
+                                 const int32_t *leaf_cnt, const int64_t *leaf_off,
+                                 const int32_t *mega_cnt, const int64_t *mega_off, int64_t n,
+                                 uint64_t *hub_tasks, uint64_t *leaf_tasks, uint64_t *mega_tasks) {
   const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= n) return;
   const uint64_t hi = (uint64_t)v << 32;
   for (int32_t c = 0, h = hub_cnt[v]; c < h; ++c) hub_tasks[hub_off[v] + c] = hi | (uint32_t)c;
   for (int32_t c = 0, l = leaf_cnt[v]; c < l; ++c) leaf_tasks[leaf_off[v] + c] = hi | (uint32_t)c;
+  for (int32_t c = 0, m = mega_cnt[v]; c < m; ++c) mega_tasks[mega_off[v] + c] = hi | (uint32_t)c;
 }
 
 // Partner edges (owner rule) and their streamed-list work, for statistics.
@@ -433,6 +438,9 @@ int tc_alloc(mc_dgraph *g) {
   MC_ALLOC(g->leaf_off, n + 1);
   MC_ALLOC(g->hub_tasks, g->task_capacity);
   MC_ALLOC(g->leaf_tasks, g->task_capacity);
+  MC_ALLOC(g->mega_cnt, n + 1);
+  MC_ALLOC(g->mega_off, n + 1);
+  MC_ALLOC(g->mega_tasks, g->task_capacity);
   MC_CUDA_TRY(dev_alloc(&g->scan_temp, g->scan_temp_size, g->stream));
 #undef MC_ALLOC
   g->tc_ready = true;
@@ -464,14 +472,16 @@ int tc_orient(mc_dgraph *g) {
     g->launches += 2 + scan_launches(tiles);
   }
   task_count_kernel<<<grid_for(n, 256), 256, 0, s>>>(g->key, n, g->hub_cnt, g->leaf_cnt,
-                                                     g->counters + 3, g->batch);
+                                                     g->mega_cnt, g->counters + 3, g->batch);
   MC_CUDA_TRY(cudaGetLastError());
   MC_CUDA_TRY(exclusive_scan(g->hub_cnt, g->hub_off, n, g->scan_temp, s));
   MC_CUDA_TRY(exclusive_scan(g->leaf_cnt, g->leaf_off, n, g->scan_temp, s));
+  MC_CUDA_TRY(exclusive_scan(g->mega_cnt, g->mega_off, n, g->scan_temp, s));
   task_fill_kernel<<<grid_for(n, 256), 256, 0, s>>>(g->hub_cnt, g->hub_off, g->leaf_cnt,
-                                                    g->leaf_off, n, g->hub_tasks, g->leaf_tasks);
+                                                    g->leaf_off, g->mega_cnt, g->mega_off, n,
+                                                    g->hub_tasks, g->leaf_tasks, g->mega_tasks);
   MC_CUDA_TRY(cudaGetLastError());
-  g->launches += 2 + 2 * scan_launches(n);
+  g->launches += 2 + 3 * scan_launches(n);
   return MC_OK;
 }
 

@@ -406,16 +406,31 @@ int tc_count_launch(mc_dgraph *g, cudaEvent_t after_hub, int shard, int num_shar
   a.num_shards = num_shards;
   a.bv = g->batch;
 
-  const size_t hub_smem = sizeof(int) << g->hub_table_log2;
+  // Owners with d+ <= kHubSmallMaxOut: tables of at most 2^12 slots (16 KB),
+  // so many CTAs share an SM; the few larger owners run in a second launch
+  // whose shared memory fits the largest table.
+  const int small_lg = std::min(kHubSmallTableLog2, g->hub_table_log2);
+  const int big_lg = std::max(kHubSmallTableLog2, g->hub_table_log2);
+  const size_t small_smem = sizeof(int) << small_lg, big_smem = sizeof(int) << big_lg;
   MC_CUDA_TRY(cudaFuncSetAttribute(tc_hub_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)hub_smem));
-  const int hub_grid = g->num_sms * resident_blocks((const void *)tc_hub_kernel, kCountThreads, hub_smem);
+                                   (int)big_smem));
+  a.table_log2_max = small_lg;
   a.tasks = g->hub_tasks;
   a.ntasks = g->hub_off + g->n;
   a.queue = g->counters + 1;
-  g->launches += 2;
-  tc_hub_kernel<<<hub_grid, kCountThreads, hub_smem, g->stream>>>(a);
+  const int small_grid =
+      g->num_sms * resident_blocks((const void *)tc_hub_kernel, kCountThreads, small_smem);
+  tc_hub_kernel<<<small_grid, kCountThreads, small_smem, g->stream>>>(a);
   MC_CUDA_TRY(cudaGetLastError());
+  a.table_log2_max = big_lg;
+  a.tasks = g->mega_tasks;
+  a.ntasks = g->mega_off + g->n;
+  a.queue = g->counters + 6;
+  const int big_grid =
+      g->num_sms * resident_blocks((const void *)tc_hub_kernel, kCountThreads, big_smem);
+  tc_hub_kernel<<<big_grid, kCountThreads, big_smem, g->stream>>>(a);
+  MC_CUDA_TRY(cudaGetLastError());
+  g->launches += 3;
   if (after_hub) MC_CUDA_TRY(cudaEventRecord(after_hub, g->stream));
 
   const int leaf_grid = g->num_sms * resident_blocks((const void *)tc_leaf_kernel, kCountThreads, 0);
