@@ -52,9 +52,13 @@ def parse_args():
     p.add_argument("--cpu-seconds", type=float, default=12.0,
                    help="target CPU time of the bounded CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--mode", choices=["tc", "batch", "serve"], default="tc",
+    p.add_argument("--mode", choices=["tc", "batch", "serve", "patterns"], default="tc",
                    help="tc: plain triangle count (the headline); batch: batched graphs/s; "
-                        "serve: Poisson request stream, p50/p99 latency")
+                        "serve: Poisson request stream, p50/p99 latency; patterns: P1..P8 "
+                        "matches/s on a Chung-Lu graph")
+    p.add_argument("--pat-n", type=int, default=100000)
+    p.add_argument("--pat-mean", type=float, default=10.0)
+    p.add_argument("--pat-cap", type=float, default=200.0)
     p.add_argument("--serve-rates", default="100,1000,5000,20000")
     p.add_argument("--serve-seconds", type=float, default=2.0)
     p.add_argument("--serve-pool", type=int, default=512)
@@ -573,8 +577,40 @@ def run_serve(a, local_rank):
     return 0
 
 
+def run_patterns(a, local_rank):
+    """P1..P8 on one seeded Chung-Lu graph: count and device time per
+    pattern (matches/s = count / kernel time; directed-edge tasks/s beside)."""
+    import torch
+    from mercury_b200 import DeviceGraph, Graph
+    torch.cuda.set_device(local_rank)
+    g = Graph.chung_lu(a.pat_n, 2.1, a.pat_mean, a.pat_cap, seed=1)
+    per = []
+    with DeviceGraph(g) as d:
+        for k in range(1, 9):
+            first = d.pattern_count(k)
+            ts = []
+            for _ in range(max(a.steps, 1)):
+                assert d.pattern_count(k) == first
+                ts.append(d.last_timing.count_ms)
+            ms = statistics.mean(ts)
+            per.append({"pattern": f"P{k}", "count": first, "ms": ms,
+                        "matches_per_s": first / (ms / 1e3) if ms > 0 else None,
+                        "edge_tasks_per_s": g.nnz / (ms / 1e3) if ms > 0 else None})
+    line = {"metric": "P1-P8 matches/s", "value": statistics.mean(p["matches_per_s"] for p in per),
+            "unit": "matches/s", "n_gpus": 1, "higher_is_better": True, "vs_baseline": None,
+            "dtype": "int32", "data": "synthetic",
+            "config": {"workload": f"Chung-Lu n={a.pat_n} gamma 2.1 mean {a.pat_mean} cap "
+                                   f"{a.pat_cap} seed 1", "n": g.n, "m": g.nnz // 2,
+                       "max_degree": g.max_degree},
+            "patterns": per}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     a = parse_args()
+    if a.mode == "patterns":
+        return run_patterns(a, int(os.environ.get("LOCAL_RANK", "0")))
     if a.mode == "batch":
         return run_batch(a, 0, 1, int(os.environ.get("LOCAL_RANK", "0")))
     if a.mode == "serve":

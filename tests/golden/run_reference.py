@@ -127,8 +127,70 @@ def timing(scales, repeats, timeout):
     return res
 
 
+OUR_SM = os.path.join(ROOT, "mercury_b200", "bin", "sm")
+SM_RUNTIME_ANY = re.compile(r"Total runtime  = ([0-9.eE+-]+) sec")
+
+
+def pattern_timing(n, mean, cap, repeats, timeout):
+    """The reference's pattern kernels and this build's `sm` on one seeded
+    Chung-Lu graph (the generator bench.py --mode patterns uses)."""
+    from mercury_b200 import Graph
+    g = Graph.chung_lu(n, 2.1, mean, cap, seed=1)
+    res = {"n": g.n, "m": g.nnz // 2, "max_degree": g.max_degree}
+    with tempfile.TemporaryDirectory() as tmp:
+        prefix = os.path.join(tmp, "cl", "graph")
+        os.makedirs(os.path.dirname(prefix))
+        g.write(prefix)
+        for k in range(1, 9):
+            rec = {}
+            for label, exe in (("reference", REF_SM), ("ours", OUR_SM)):
+                best = None
+                for _ in range(repeats):
+                    s, err = run([exe, prefix, f"P{k}"], timeout)
+                    if s is None:
+                        best = err
+                        break
+                    t = float(SM_RUNTIME_ANY.search(s).group(1))
+                    c = int(COUNT.search(s).group(1))
+                    if best is None or t < best["runtime_s"]:
+                        best = {"runtime_s": t, "count": c}
+                rec[label] = best
+            res[f"P{k}"] = rec
+            print(f"P{k}", rec, flush=True)
+    return res
+
+
+def tc_chung_lu_timing(n, repeats, timeout):
+    from mercury_b200 import Graph
+    g = Graph.chung_lu(n, 2.1, 20.0, 50000.0, seed=1)
+    rec = {"n": g.n, "m": g.nnz // 2, "max_degree": g.max_degree}
+    ok, why = reference_tc_limits_ok(np.asarray(g.rowptr), np.asarray(g.col))
+    rec["ref_limits"] = why
+    with tempfile.TemporaryDirectory() as tmp:
+        prefix = os.path.join(tmp, "cl", "graph")
+        os.makedirs(os.path.dirname(prefix))
+        g.write(prefix)
+        for label, exe, allowed in (("reference", REF_TC, ok), ("ours", OUR_TC, True)):
+            if not allowed:
+                rec[label] = "skipped: " + why
+                continue
+            runs = []
+            for _ in range(repeats):
+                s, err = run([exe, prefix], timeout)
+                if s is None:
+                    runs.append(err)
+                    break
+                runs.append({"runtime_s": float(RUNTIME.search(s).group(1)),
+                             "count": int(COUNT.search(s).group(1))})
+            rec[label] = runs
+    print("chung-lu", rec, flush=True)
+    return rec
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--patterns", default="", help="n,mean,cap of a Chung-Lu graph to time P1..P8")
+    ap.add_argument("--tc-chung-lu", type=int, default=0, help="vertices of a Chung-Lu TC timing")
     ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "reference_run.json"))
     ap.add_argument("--scales", default="16,20,22")
     ap.add_argument("--repeats", type=int, default=3)
@@ -141,6 +203,11 @@ def main():
     scales = [int(s) for s in a.scales.split(",") if s]
     if scales:
         result["timing"] = timing(scales, a.repeats, a.timeout)
+    if a.patterns:
+        pn, pm, pc = a.patterns.split(",")
+        result["patterns"] = pattern_timing(int(pn), float(pm), float(pc), a.repeats, a.timeout)
+    if a.tc_chung_lu:
+        result["tc_chung_lu"] = tc_chung_lu_timing(a.tc_chung_lu, a.repeats, a.timeout)
     os.makedirs(os.path.dirname(a.out), exist_ok=True)
     with open(a.out, "w") as f:
         json.dump(result, f, indent=1)
