@@ -111,6 +111,75 @@ int mc_gen_rmat(int scale, int edge_factor, double a, double b, double c,
 int mc_gen_chung_lu(int64_t n, double gamma, double mean_degree,
                     double max_weight, uint64_t seed, mc_graph_t **out);
 
+/* ---- edge lists and the device CSR build --------------------------------
+ * These replace the reference's dataset preparation. That is the closed
+ * binary `converter mtx <file> <prefix> ...` (datasets/converter.sh:5), which
+ * writes the CSR triple from a Matrix Market file, and datasets/tsv2mtx.py
+ * (GraphChallenge TSV -> Matrix Market through a networkx Graph, i.e.
+ * undirected with duplicates merged).
+ * Parsing text is host work. Symmetrising, dropping self-loops, merging
+ * duplicates, sorting rows and building the row offsets run on the device. */
+typedef struct mc_edges mc_edges_t;   /* host edge list (pairs of int32 ids) */
+
+#define MC_EDGES_MTX 1  /* Matrix Market "coordinate" file: '%' comment lines,
+                           "rows cols entries", then one "i j [value]" per
+                           entry; ids 1-based                              */
+#define MC_EDGES_TSV 2  /* GraphChallenge TSV: "u<TAB>v[<TAB>w]" per line;
+                           ids 1-based                                     */
+#define MC_EDGES_SNAP 3 /* whitespace-separated "u v" per line, '#' comment
+                           lines; ids 0-based                              */
+
+/* Reads an edge list. id_base is the id of the first vertex in the file (0 or
+ * 1); a negative id_base takes the format's default (1 for MTX and TSV, 0 for
+ * SNAP). The reference's converter_vidfrom0 corresponds to MTX with
+ * id_base 0.
+ * The vertex count is max(rows, cols) from an MTX size line, or the
+ * largest id seen + 1 - id_base when that is larger. Any id below id_base,
+ * a value that is not an integer, a line with one field, or an MTX body
+ * whose entry count differs from its size line is refused with
+ * MC_ERR_FORMAT. "array" Matrix Market files are MC_ERR_UNSUPPORTED. */
+int mc_edges_load(const char *path, int format, int id_base, mc_edges_t **out);
+/* Copies caller arrays (ids already 0-based) into an edge list. */
+int mc_edges_from_arrays(const int32_t *src, const int32_t *dst,
+                         int64_t num_edges, int64_t n, mc_edges_t **out);
+int mc_edges_info(const mc_edges_t *e, int64_t *num_edges, int64_t *n);
+/* Borrowed pointers, valid until mc_edges_free. */
+const int32_t *mc_edges_src(const mc_edges_t *e);
+const int32_t *mc_edges_dst(const mc_edges_t *e);
+void mc_edges_free(mc_edges_t *e);
+/* The raw endpoint draws behind mc_gen_rmat / mc_gen_chung_lu, before any
+ * symmetrising or merging (the same seed gives the same graph after a
+ * CSR build). */
+int mc_gen_rmat_edges(int scale, int edge_factor, double a, double b,
+                      double c, uint64_t seed, mc_edges_t **out);
+int mc_gen_chung_lu_edges(int64_t n, double gamma, double mean_degree,
+                          double max_weight, uint64_t seed, mc_edges_t **out);
+
+/* Flag of the CSR builds: src/dst are device pointers on the current device.
+ * Otherwise they are host pointers and are copied in. */
+#define MC_BUILD_DEVICE_INPUT 0x100u
+
+/* Builds the symmetric CSR of the simple undirected graph on [0, n) given by
+ * the pairs (src[i], dst[i]) on the current device, and returns it as a
+ * host graph. Every pair u != v puts v in N(u) and u in N(v). Self-loops
+ * are dropped, duplicates merged and rows sorted ascending, so the result
+ * meets the graph contract above. An id outside [0, n) is refused with
+ * MC_ERR_FORMAT. Replaces the converter's CSR construction. `stream` is a
+ * cudaStream_t (NULL: a stream of the call's own). `timing` (may be NULL)
+ * gets h2d_ms (input copy), count_ms (device build), d2h_ms (result copy),
+ * total_ms and launches; its other fields are zero. */
+int mc_csr_build(const int32_t *src, const int32_t *dst, int64_t num_edges,
+                 int64_t n, unsigned flags, void *stream, mc_graph_t **out,
+                 mc_timing_t *timing);
+/* Same build, but the CSR stays on the device as a graph handle ready for
+ * mc_tc_count / mc_pattern_count, with no host round trip. flags may also
+ * hold MC_VALIDATE_SYMMETRY (the handle's contract check runs as in
+ * mc_dgraph_create). timing->total_ms includes the handle's check. */
+int mc_dgraph_from_edges(const int32_t *src, const int32_t *dst,
+                         int64_t num_edges, int64_t n, unsigned flags,
+                         void *stream, mc_dgraph_t **out,
+                         mc_timing_t *timing);
+
 /* ---- device graphs -------------------------------------------------------
  * mc_dgraph_create replaces GraphGPU::init / init_with_division
  * (include/graph_gpu.h:87-188): copies the symmetric CSR to the current
@@ -128,6 +197,13 @@ int mc_dgraph_create_device(const int64_t *d_rowptr, const int32_t *d_col,
                             unsigned flags, mc_dgraph_t **out);
 /* The cudaStream_t every call on this handle is issued on. */
 int mc_dgraph_stream(const mc_dgraph_t *g, void **stream);
+/* Sizes of the handle's symmetric CSR (max_degree from its contract check). */
+int mc_dgraph_info(const mc_dgraph_t *g, int64_t *n, int64_t *nnz,
+                   int64_t *max_degree);
+/* Copies the handle's symmetric CSR to host arrays of n+1 and nnz entries
+ * (col_out may be NULL for the offsets only). */
+int mc_dgraph_export_csr(const mc_dgraph_t *g, int64_t *rowptr_out,
+                         int32_t *col_out);
 void mc_dgraph_free(mc_dgraph_t *g);
 
 /* Triangle count.  Replaces TCSolver(Graph&, uint64_t&) (tc_challenge.cu:11,

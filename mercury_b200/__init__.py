@@ -9,5 +9,6 @@ from ._ffi import McError, Timing, lib  # noqa: F401
 from .graph import DeviceGraph, Graph, TCSolver, tc_count_host  # noqa: F401
 from .batch import Batch, union_csr  # noqa: F401
 from .server import Server  # noqa: F401
+from .edges import EdgeList, csr_build, dgraph_from_edges  # noqa: F401
 
 __version__ = "0.1.0"

@@ -25,6 +25,11 @@ MC_ERR_BUDGET = -9
 MC_ERR_TIMEOUT = -10
 
 MC_VALIDATE_SYMMETRY = 0x1
+MC_BUILD_DEVICE_INPUT = 0x100
+
+MC_EDGES_MTX = 1
+MC_EDGES_TSV = 2
+MC_EDGES_SNAP = 3
 
 
 class McError(RuntimeError):
@@ -88,9 +93,21 @@ SIGNATURES = {
     "mc_graph_free": (None, [_P]),
     "mc_gen_rmat": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_uint64, _PP]),
     "mc_gen_chung_lu": (C.c_int, [_I64, C.c_double, C.c_double, C.c_double, C.c_uint64, _PP]),
+    "mc_edges_load": (C.c_int, [C.c_char_p, C.c_int, C.c_int, _PP]),
+    "mc_edges_from_arrays": (C.c_int, [_P, _P, _I64, _I64, _PP]),
+    "mc_edges_info": (C.c_int, [_P, _PI64, _PI64]),
+    "mc_edges_src": (_P, [_P]),
+    "mc_edges_dst": (_P, [_P]),
+    "mc_edges_free": (None, [_P]),
+    "mc_gen_rmat_edges": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_uint64, _PP]),
+    "mc_gen_chung_lu_edges": (C.c_int, [_I64, C.c_double, C.c_double, C.c_double, C.c_uint64, _PP]),
+    "mc_csr_build": (C.c_int, [_P, _P, _I64, _I64, C.c_uint, _P, _PP, C.POINTER(Timing)]),
+    "mc_dgraph_from_edges": (C.c_int, [_P, _P, _I64, _I64, C.c_uint, _P, _PP, C.POINTER(Timing)]),
     "mc_dgraph_create": (C.c_int, [_P, _P, _I64, _I64, _P, C.c_uint, _PP]),
     "mc_dgraph_create_device": (C.c_int, [_P, _P, _I64, _I64, _P, C.c_uint, _PP]),
     "mc_dgraph_stream": (C.c_int, [_P, _PP]),
+    "mc_dgraph_info": (C.c_int, [_P, _PI64, _PI64, _PI64]),
+    "mc_dgraph_export_csr": (C.c_int, [_P, _P, _P]),
     "mc_dgraph_free": (None, [_P]),
     "mc_tc_count": (C.c_int, [_P, _PU64, C.POINTER(Timing)]),
     "mc_tc_count_shard": (C.c_int, [_P, C.c_int, C.c_int, _PU64, C.POINTER(Timing)]),

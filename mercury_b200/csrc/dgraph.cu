@@ -188,6 +188,78 @@ int mc_dgraph_create_device(const int64_t *d_rowptr, const int32_t *d_col, int64
   return mc::finish_create(g, flags, out, up());
 }
 
+int mc_dgraph_from_edges(const int32_t *src, const int32_t *dst, int64_t num_edges, int64_t n,
+                         unsigned flags, void *stream, mc_dgraph_t **out, mc_timing_t *timing) {
+  if (!out || num_edges < 0 || (num_edges > 0 && (!src || !dst))) return MC_ERR_ARG;
+  if (timing) std::memset(timing, 0, sizeof(*timing));
+  mc_dgraph *g = nullptr;
+  // The handle starts with an empty column array; it is sized once the
+  // build has counted the distinct entries.
+  int rc = mc::create_common(n, 0, stream, out, &g);
+  if (rc != MC_OK) {
+    release(g);
+    return rc;
+  }
+  mc::CsrBuild *b = nullptr;
+  auto run = [&]() -> int {
+    MC_CUDA_TRY(cudaEventRecord(g->ev[0], g->stream));
+    int r = mc::csr_build_create(num_edges, n, g->stream, &b);
+    if (r != MC_OK) return r;
+    r = mc::csr_build_input(b, src, dst, (flags & MC_BUILD_DEVICE_INPUT) != 0);
+    if (r != MC_OK) return r;
+    MC_CUDA_TRY(cudaEventRecord(g->ev[1], g->stream));
+    int64_t nnz = 0, max_degree = 0;
+    r = mc::csr_build_sort(b, &nnz);
+    if (r != MC_OK) return r;
+    mc::dev_free(g->col, g->stream);
+    g->col = nullptr;
+    MC_CUDA_TRY(mc::dev_alloc((void **)&g->col, sizeof(int32_t) * (size_t)std::max<int64_t>(nnz, 1),
+                              g->stream));
+    g->nnz = nnz;
+    r = mc::csr_build_emit(b, g->rowptr, g->col, &max_degree);
+    if (r != MC_OK) return r;
+    MC_CUDA_TRY(cudaEventRecord(g->ev[2], g->stream));
+    return MC_OK;
+  };
+  rc = run();
+  const int64_t launches = mc::csr_build_launches(b);
+  mc::csr_build_free(b);
+  // The contract check of every handle (and its max degree) runs on the
+  // built CSR too.
+  g->launches = 0;
+  rc = mc::finish_create(g, flags & MC_VALIDATE_SYMMETRY, out, rc);
+  if (rc != MC_OK) return rc;
+  if (timing) {
+    MC_CUDA_TRY(cudaEventRecord(g->ev[3], g->stream));
+    MC_CUDA_TRY(cudaEventSynchronize(g->ev[3]));
+    timing->h2d_ms = mc::elapsed(g->ev[0], g->ev[1]);
+    timing->count_ms = mc::elapsed(g->ev[1], g->ev[2]);
+    timing->total_ms = mc::elapsed(g->ev[0], g->ev[3]);
+    timing->launches = launches + g->launches;
+  }
+  return MC_OK;
+}
+
+int mc_dgraph_info(const mc_dgraph_t *g, int64_t *n, int64_t *nnz, int64_t *max_degree) {
+  if (!g) return MC_ERR_ARG;
+  if (n) *n = g->n;
+  if (nnz) *nnz = g->nnz;
+  if (max_degree) *max_degree = g->max_degree;
+  return MC_OK;
+}
+
+int mc_dgraph_export_csr(const mc_dgraph_t *g, int64_t *rowptr_out, int32_t *col_out) {
+  if (!g || !rowptr_out) return MC_ERR_ARG;
+  MC_CUDA_TRY(cudaSetDevice(g->device));
+  MC_CUDA_TRY(cudaMemcpyAsync(rowptr_out, g->rowptr, sizeof(int64_t) * (size_t)(g->n + 1),
+                              cudaMemcpyDeviceToHost, g->stream));
+  if (col_out && g->nnz > 0)
+    MC_CUDA_TRY(cudaMemcpyAsync(col_out, g->col, sizeof(int32_t) * (size_t)g->nnz,
+                                cudaMemcpyDeviceToHost, g->stream));
+  MC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  return MC_OK;
+}
+
 int mc_dgraph_stream(const mc_dgraph_t *g, void **stream) {
   if (!g || !stream) return MC_ERR_ARG;
   *stream = (void *)g->stream;
@@ -228,6 +300,7 @@ int mc_tc_count_shard(mc_dgraph_t *g, int shard, int num_shards, uint64_t *count
   int lg = 8;
   while (lg < cap && (1ll << lg) < 4 * maxd) ++lg;
   g->hub_table_log2 = lg;
+
   MC_CUDA_TRY(cudaEventRecord(g->ev[4], s));
   rc = mc::tc_count_launch(g, g->ev[2], shard, num_shards);
   if (rc != MC_OK) return rc;

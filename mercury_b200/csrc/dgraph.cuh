@@ -115,4 +115,19 @@ int batch_create(const int64_t *rowptr, const int32_t *col, bool device_csr, int
 // budget; *warps receives the resident warp count.
 int batch_pattern_grid(int num_sms, int64_t cap, int64_t *warps);
 int pattern_lists();
+
+// build.cu: the device CSR build from an edge list, in steps so that callers
+// can time them and place the output where they need it.
+struct CsrBuild;
+// Scratch for m pairs over n vertices, on stream s.
+int csr_build_create(int64_t m, int64_t n, cudaStream_t s, CsrBuild **out);
+// Pairs in: copied from the host, or read in place from device memory.
+int csr_build_input(CsrBuild *b, const int32_t *src, const int32_t *dst, bool device_input);
+// Sorts the packed keys and counts the distinct entries; waits for the
+// stream. MC_ERR_FORMAT when an id is outside [0, n).
+int csr_build_sort(CsrBuild *b, int64_t *nnz);
+// Writes col[nnz] and rowptr[n + 1]; *max_degree gets the largest row.
+int csr_build_emit(CsrBuild *b, int64_t *rowptr, int32_t *col, int64_t *max_degree);
+int64_t csr_build_launches(const CsrBuild *b);
+void csr_build_free(CsrBuild *b);
 }  // namespace mc

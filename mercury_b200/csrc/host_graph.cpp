@@ -99,7 +99,103 @@ int build_symmetric_csr(int64_t n, const std::vector<int32_t> &src,
   return MC_OK;
 }
 
+
+int rmat_draws(int scale, int edge_factor, double a, double b, double c, uint64_t seed,
+               int64_t *n_out, std::vector<int32_t> &src, std::vector<int32_t> &dst) {
+  if (scale < 1 || scale > 30 || edge_factor < 1) return MC_ERR_ARG;
+  if (a < 0 || b < 0 || c < 0 || a + b + c > 1.0) return MC_ERR_ARG;
+  const int64_t n = int64_t(1) << scale;
+  const int64_t draws = n * edge_factor;
+  // Quadrant thresholds on a 32-bit uniform: [0,a) -> (0,0), [a,a+b) -> (0,1),
+  // [a+b,a+b+c) -> (1,0), rest -> (1,1) for (src bit, dst bit), top bit first.
+  const double s32 = 4294967296.0;
+  const uint64_t ta = (uint64_t)(a * s32), tb = (uint64_t)((a + b) * s32),
+                 tc = (uint64_t)((a + b + c) * s32);
+  try {
+    src.resize(draws);
+    dst.resize(draws);
+  } catch (const std::bad_alloc &) {
+    return MC_ERR_OOM;
+  }
+  const uint64_t key = mix64(seed ^ 0x52D4A7ull);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < draws; ++i) {
+    uint32_t s = 0, d = 0;
+    uint64_t bits = 0;
+    for (int l = 0; l < scale; ++l) {
+      if ((l & 1) == 0) bits = mix64(key + (uint64_t)i * 0x1000193ull + (uint64_t)(l >> 1));
+      uint64_t r = (l & 1) ? (bits >> 32) : (bits & 0xFFFFFFFFull);
+      uint32_t sb = 0, db = 0;
+      if (r < ta) { sb = 0; db = 0; }
+      else if (r < tb) { sb = 0; db = 1; }
+      else if (r < tc) { sb = 1; db = 0; }
+      else { sb = 1; db = 1; }
+      s = (s << 1) | sb;
+      d = (d << 1) | db;
+    }
+    src[i] = (int32_t)s;
+    dst[i] = (int32_t)d;
+  }
+  *n_out = n;
+  return MC_OK;
+}
+
+int chung_lu_draws(int64_t n, double gamma, double mean_degree, double max_weight,
+                   uint64_t seed, std::vector<int32_t> &src, std::vector<int32_t> &dst) {
+  if (n < 2 || n > INT32_MAX || gamma <= 1.0 || mean_degree <= 0 || max_weight <= 0)
+    return MC_ERR_ARG;
+  std::vector<double> cdf;
+  const int64_t pairs = (int64_t)std::llround((double)n * mean_degree / 2.0);
+  try {
+    cdf.resize(n);
+    src.resize(pairs);
+    dst.resize(pairs);
+  } catch (const std::bad_alloc &) {
+    return MC_ERR_OOM;
+  }
+  // Expected-degree weights w_i = (i+1)^(-1/(gamma-1)), scaled to the mean,
+  // then capped.
+  const double expo = -1.0 / (gamma - 1.0);
+  double sum = 0;
+  for (int64_t i = 0; i < n; ++i) sum += std::pow((double)(i + 1), expo);
+  const double scale = mean_degree * (double)n / sum;
+  double acc = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    double w = std::min(scale * std::pow((double)(i + 1), expo), max_weight);
+    acc += w;
+    cdf[i] = acc;
+  }
+  const double total = acc;
+  const uint64_t key = mix64(seed ^ 0xC1u);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < pairs; ++i) {
+    uint64_t r = mix64(key + (uint64_t)i);
+    double u0 = (double)(r >> 32) * (1.0 / 4294967296.0) * total;
+    double u1 = (double)(r & 0xFFFFFFFFull) * (1.0 / 4294967296.0) * total;
+    src[i] = (int32_t)(std::upper_bound(cdf.begin(), cdf.end(), u0) - cdf.begin());
+    dst[i] = (int32_t)(std::upper_bound(cdf.begin(), cdf.end(), u1) - cdf.begin());
+    if (src[i] >= n) src[i] = (int32_t)(n - 1);
+    if (dst[i] >= n) dst[i] = (int32_t)(n - 1);
+  }
+  return MC_OK;
+}
+
 }  // namespace mc
+
+namespace {
+int finish_generated(int64_t n, const std::vector<int32_t> &src, const std::vector<int32_t> &dst,
+                     mc_graph_t **out) {
+  mc_graph *g = new (std::nothrow) mc_graph();
+  if (!g) return MC_ERR_OOM;
+  int rc = mc::build_symmetric_csr(n, src, dst, g);
+  if (rc != MC_OK) {
+    delete g;
+    return rc;
+  }
+  *out = g;
+  return MC_OK;
+}
+}  // namespace
 
 extern "C" {
 
@@ -215,101 +311,23 @@ void mc_graph_free(mc_graph_t *g) { delete g; }
 
 int mc_gen_rmat(int scale, int edge_factor, double a, double b, double c,
                 uint64_t seed, mc_graph_t **out) {
-  if (!out || scale < 1 || scale > 30 || edge_factor < 1) return MC_ERR_ARG;
-  if (a < 0 || b < 0 || c < 0 || a + b + c > 1.0) return MC_ERR_ARG;
+  if (!out) return MC_ERR_ARG;
   *out = nullptr;
-  const int64_t n = int64_t(1) << scale;
-  const int64_t draws = n * edge_factor;
-  // Quadrant thresholds on a 32-bit uniform: [0,a) -> (0,0), [a,a+b) -> (0,1),
-  // [a+b,a+b+c) -> (1,0), rest -> (1,1) for (src bit, dst bit), top bit first.
-  const double s32 = 4294967296.0;
-  const uint64_t ta = (uint64_t)(a * s32), tb = (uint64_t)((a + b) * s32),
-                 tc = (uint64_t)((a + b + c) * s32);
   std::vector<int32_t> src, dst;
-  try {
-    src.resize(draws);
-    dst.resize(draws);
-  } catch (const std::bad_alloc &) {
-    return MC_ERR_OOM;
-  }
-  const uint64_t key = mc::mix64(seed ^ 0x52D4A7ull);
-#pragma omp parallel for schedule(static)
-  for (int64_t i = 0; i < draws; ++i) {
-    uint32_t s = 0, d = 0;
-    uint64_t bits = 0;
-    for (int l = 0; l < scale; ++l) {
-      if ((l & 1) == 0) bits = mc::mix64(key + (uint64_t)i * 0x1000193ull + (uint64_t)(l >> 1));
-      uint64_t r = (l & 1) ? (bits >> 32) : (bits & 0xFFFFFFFFull);
-      uint32_t sb = 0, db = 0;
-      if (r < ta) { sb = 0; db = 0; }
-      else if (r < tb) { sb = 0; db = 1; }
-      else if (r < tc) { sb = 1; db = 0; }
-      else { sb = 1; db = 1; }
-      s = (s << 1) | sb;
-      d = (d << 1) | db;
-    }
-    src[i] = (int32_t)s;
-    dst[i] = (int32_t)d;
-  }
-  mc_graph *g = new (std::nothrow) mc_graph();
-  if (!g) return MC_ERR_OOM;
-  int rc = mc::build_symmetric_csr(n, src, dst, g);
-  if (rc != MC_OK) {
-    delete g;
-    return rc;
-  }
-  *out = g;
-  return MC_OK;
+  int64_t n = 0;
+  int rc = mc::rmat_draws(scale, edge_factor, a, b, c, seed, &n, src, dst);
+  if (rc != MC_OK) return rc;
+  return finish_generated(n, src, dst, out);
 }
 
 int mc_gen_chung_lu(int64_t n, double gamma, double mean_degree, double max_weight,
                     uint64_t seed, mc_graph_t **out) {
-  if (!out || n < 2 || n > INT32_MAX || gamma <= 1.0 || mean_degree <= 0 || max_weight <= 0)
-    return MC_ERR_ARG;
+  if (!out) return MC_ERR_ARG;
   *out = nullptr;
-  std::vector<double> cdf;
   std::vector<int32_t> src, dst;
-  const int64_t pairs = (int64_t)std::llround((double)n * mean_degree / 2.0);
-  try {
-    cdf.resize(n);
-    src.resize(pairs);
-    dst.resize(pairs);
-  } catch (const std::bad_alloc &) {
-    return MC_ERR_OOM;
-  }
-  // Expected-degree weights w_i = (i+1)^(-1/(gamma-1)), scaled to the mean,
-  // then capped.
-  const double expo = -1.0 / (gamma - 1.0);
-  double sum = 0;
-  for (int64_t i = 0; i < n; ++i) sum += std::pow((double)(i + 1), expo);
-  const double scale = mean_degree * (double)n / sum;
-  double acc = 0;
-  for (int64_t i = 0; i < n; ++i) {
-    double w = std::min(scale * std::pow((double)(i + 1), expo), max_weight);
-    acc += w;
-    cdf[i] = acc;
-  }
-  const double total = acc;
-  const uint64_t key = mc::mix64(seed ^ 0xC1u);
-#pragma omp parallel for schedule(static)
-  for (int64_t i = 0; i < pairs; ++i) {
-    uint64_t r = mc::mix64(key + (uint64_t)i);
-    double u0 = (double)(r >> 32) * (1.0 / 4294967296.0) * total;
-    double u1 = (double)(r & 0xFFFFFFFFull) * (1.0 / 4294967296.0) * total;
-    src[i] = (int32_t)(std::upper_bound(cdf.begin(), cdf.end(), u0) - cdf.begin());
-    dst[i] = (int32_t)(std::upper_bound(cdf.begin(), cdf.end(), u1) - cdf.begin());
-    if (src[i] >= n) src[i] = (int32_t)(n - 1);
-    if (dst[i] >= n) dst[i] = (int32_t)(n - 1);
-  }
-  mc_graph *g = new (std::nothrow) mc_graph();
-  if (!g) return MC_ERR_OOM;
-  int rc = mc::build_symmetric_csr(n, src, dst, g);
-  if (rc != MC_OK) {
-    delete g;
-    return rc;
-  }
-  *out = g;
-  return MC_OK;
+  int rc = mc::chung_lu_draws(n, gamma, mean_degree, max_weight, seed, src, dst);
+  if (rc != MC_OK) return rc;
+  return finish_generated(n, src, dst, out);
 }
 
 }  // extern "C"

@@ -28,4 +28,19 @@ inline uint64_t mix64(uint64_t x) {
 int build_symmetric_csr(int64_t n, const std::vector<int32_t> &src,
                         const std::vector<int32_t> &dst, mc_graph *g);
 
+// Raw endpoint draws of the seeded generators (before any symmetrising).
+int rmat_draws(int scale, int edge_factor, double a, double b, double c, uint64_t seed,
+               int64_t *n_out, std::vector<int32_t> &src, std::vector<int32_t> &dst);
+int chung_lu_draws(int64_t n, double gamma, double mean_degree, double max_weight,
+                   uint64_t seed, std::vector<int32_t> &src, std::vector<int32_t> &dst);
+
+}  // namespace mc
+
+struct mc_edges {
+  int64_t n = 0;  // vertex count (ids in [0, n))
+  std::vector<int32_t> src, dst;
+};
+
+namespace mc {
+
 }  // namespace mc

@@ -153,6 +153,23 @@ class DeviceGraph:
         self.last_timing = Timing()
         return self
 
+    @classmethod
+    def _adopt(cls, h: C.c_void_p, n: int) -> "DeviceGraph":
+        self = cls.__new__(cls)
+        self._h = h
+        self.last_timing = Timing()
+        nn, nnz, md = C.c_int64(), C.c_int64(), C.c_int64()
+        check(lib().mc_dgraph_info(h, C.byref(nn), C.byref(nnz), C.byref(md)), "device graph info")
+        self.n, self.nnz, self.max_degree = nn.value, nnz.value, md.value
+        return self
+
+    def export_csr(self) -> Tuple[np.ndarray, np.ndarray]:
+        """The handle's symmetric CSR as host (rowptr, col)."""
+        rp = np.zeros(self.n + 1, dtype=np.int64)
+        col = np.zeros(max(self.nnz, 1), dtype=np.int32)
+        check(lib().mc_dgraph_export_csr(self._h, rp.ctypes.data, col.ctypes.data), "export csr")
+        return rp, col[: self.nnz]
+
     @property
     def stream(self) -> int:
         s = C.c_void_p()

@@ -45,6 +45,8 @@ def lib() -> C.CDLL:
         L.orc_tc.restype = C.c_uint64
         L.orc_pattern.argtypes = [C.c_int64, P, P, C.c_int, P]
         L.orc_pattern.restype = C.c_uint64
+        L.orc_csr_build.argtypes = [C.c_int64, C.c_int64, P, P, P, P]
+        L.orc_csr_build.restype = C.c_int64
         _lib = L
     return _lib
 
@@ -115,3 +117,35 @@ def pattern(rowptr, col, k: int, return_counters: bool = False):
     if return_counters:
         return r, int(c12[0]), int(c12[1])
     return r
+
+
+def csr_from_edges(src, dst, n: int):
+    """Symmetric CSR of the simple undirected graph on [0, n) given by the
+    pairs (numpy restatement: the entry set of a networkx Graph built from
+    the pairs, datasets/tsv2mtx.py:13, without self-loops, sorted)."""
+    src = np.asarray(src, dtype=np.int64)
+    dst = np.asarray(dst, dtype=np.int64)
+    if len(src) and (src.min() < 0 or dst.min() < 0 or src.max() >= n or dst.max() >= n):
+        raise ValueError("id outside [0, n)")
+    keep = src != dst
+    u = np.concatenate([src[keep], dst[keep]])
+    v = np.concatenate([dst[keep], src[keep]])
+    key = np.unique(u * max(n, 1) + v)
+    rows = key // max(n, 1)
+    rowptr = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(np.bincount(rows, minlength=n)[:n], out=rowptr[1:])
+    return rowptr, (key % max(n, 1)).astype(np.int32)
+
+
+def csr_build(src, dst, n: int):
+    """The same CSR from the C++/OpenMP restatement (parallel sort of packed
+    keys); the CPU baseline of the device build."""
+    src = np.ascontiguousarray(src, dtype=np.int32)
+    dst = np.ascontiguousarray(dst, dtype=np.int32)
+    rowptr = np.zeros(n + 1, dtype=np.int64)
+    col = np.zeros(max(2 * len(src), 1), dtype=np.int32)
+    nnz = lib().orc_csr_build(n, len(src), src.ctypes.data, dst.ctypes.data,
+                              rowptr.ctypes.data, col.ctypes.data)
+    if nnz < 0:
+        raise ValueError("id outside [0, n)")
+    return rowptr, col[:nnz]
