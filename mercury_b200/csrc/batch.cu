@@ -310,6 +310,7 @@ int batch_create(const int64_t *rowptr, const int32_t *col, bool device_csr, int
       if (*g->h_err) return fail(MC_ERR_FORMAT);  // an edge crosses two graphs
     }
     if (b->has_tc) {
+      g->batch.gid = b->d_gid;  // a batch handle: no degree ranks (see tc_alloc)
       rc = tc_alloc(g);
       if (rc != MC_OK) return fail(rc);
     }

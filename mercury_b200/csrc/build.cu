@@ -205,6 +205,7 @@ int csr_build_create(int64_t m, int64_t n, cudaStream_t s, CsrBuild **out) {
   int dev = 0;
   MC_CUDA_TRY(cudaGetDevice(&dev));
   MC_CUDA_TRY(cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, dev));
+  retain_pool_memory(dev);
   b->h_flags = new (std::nothrow) unsigned[8]();
   if (!b->h_flags) return MC_ERR_OOM;
   MC_CUDA_TRY(dev_alloc((void **)&b->flags, sizeof(unsigned) * 4, s));

@@ -18,6 +18,7 @@ enum DeviceError : unsigned {
   kErrAsymmetric = 1u << 4,   // u in N(v) but v not in N(u)
   kErrHashFull = 1u << 5,     // a shared-memory table had no free slot
   kErrCapacity = 1u << 6,     // a scratch list exceeded its capacity
+  kErrRank = 1u << 7,         // an out-list entry not ranked below its owner
 };
 
 #define MC_CUDA_TRY(expr)                                   \
@@ -34,6 +35,12 @@ void set_last_cuda_error(cudaError_t e);
 
 // Device buffers come from the stream-ordered allocator on the owning
 // handle's stream: freeing one never waits for the whole device.
+// retain_pool_memory() makes the device's default pool keep freed memory
+// mapped (the default threshold of 0 hands it back to the driver at every
+// synchronisation, and the next allocation maps it again), so repeated
+// calls reuse their buffers. The pool stays private to this process.
+void retain_pool_memory(int device);
+
 inline cudaError_t dev_alloc(void **p, size_t bytes, cudaStream_t s) {
   return cudaMallocAsync(p, bytes < 8 ? 8 : bytes, s);
 }

@@ -1,5 +1,6 @@
 // C ABI of the device graph handle and the triangle-count entry points.
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
 #include <new>
@@ -28,7 +29,8 @@ void release(mc_dgraph *g) {
                   g->dag_col,    g->keep,       g->tile_counts, g->tile_offsets,
                   g->hub_cnt,    g->leaf_cnt,   g->hub_off,  g->leaf_off,  g->hub_tasks,
                   g->leaf_tasks, g->scan_temp,  g->counters, g->err, g->pat_scratch,
-                  g->mega_cnt,   g->mega_off,   g->mega_tasks};
+                  g->mega_cnt,   g->mega_off,   g->mega_tasks, g->rank,
+                  g->dag_rank,   g->rank_keys,  g->rank_counts, g->rank_offsets};
   // Stream-ordered frees: no device-wide synchronisation, so other handles'
   // work keeps running while this one is released.
   for (void *p : bufs)
@@ -53,6 +55,7 @@ int create_common(int64_t n, int64_t nnz, void *stream, mc_dgraph **out, mc_dgra
   *gp = g;
   MC_CUDA_TRY(cudaGetDevice(&g->device));
   MC_CUDA_TRY(cudaDeviceGetAttribute(&g->num_sms, cudaDevAttrMultiProcessorCount, g->device));
+  retain_pool_memory(g->device);
   if (stream) {
     g->stream = static_cast<cudaStream_t>(stream);
   } else {
@@ -96,6 +99,18 @@ thread_local HostCache t_cache;
 }  // namespace
 
 void set_last_cuda_error(cudaError_t e) { t_last_cuda = e; }
+
+void retain_pool_memory(int device) {
+  static std::atomic<unsigned long long> done{0};  // one bit per device (first 64)
+  const unsigned long long bit = device < 64 ? 1ull << device : 0ull;
+  if (bit && (done.load(std::memory_order_relaxed) & bit)) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  done.fetch_or(bit, std::memory_order_relaxed);
+}
 
 int tc_stats(mc_dgraph *g, mc_tc_stats_t *st) {
   std::memset(st, 0, sizeof(*st));
@@ -300,7 +315,13 @@ int mc_tc_count_shard(mc_dgraph_t *g, int shard, int num_shards, uint64_t *count
   int lg = 8;
   while (lg < cap && (1ll << lg) < 4 * maxd) ++lg;
   g->hub_table_log2 = lg;
-
+  // MERCURY_TC_BITMAP_BITS caps the hub bitmaps (0: tables only), so that
+  // tests reach the table paths on graphs whose ranks would all fit.
+  g->bitmap_bits_cap = 0x7fffffff;
+  if (const char *env = std::getenv("MERCURY_TC_BITMAP_BITS")) {
+    const long v = std::atol(env);
+    if (v >= 0) g->bitmap_bits_cap = (int)std::min<long>(v, 0x7fffffff);
+  }
   MC_CUDA_TRY(cudaEventRecord(g->ev[4], s));
   rc = mc::tc_count_launch(g, g->ev[2], shard, num_shards);
   if (rc != MC_OK) return rc;

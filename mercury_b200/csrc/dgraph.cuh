@@ -19,6 +19,9 @@ constexpr int kHubTableLog2Max = 15;       // at most 32768 slots (128 KB smem)
 // occupancy); larger ones in a launch sized for the largest table.
 constexpr int kHubSmallMaxOut = 1024;
 constexpr int kHubSmallTableLog2 = 12;
+// Least shared memory of a hub CTA (also the bitmap capacity: 8 bits per
+// byte, so owners of degree rank below 262144 use bitmaps).
+constexpr int kHubBitmapBytes = 32768;
 }  // namespace mc
 
 namespace mc {
@@ -52,6 +55,14 @@ struct mc_dgraph {
   int2 *key = nullptr;            // n      {symmetric degree, DAG out-degree}
   int64_t *dag_rowptr = nullptr;  // n + 1
   int32_t *dag_col = nullptr;     // nnz (capacity; m+ used)
+  // Degree rank: vertices sorted by (degree desc, id desc), so every entry
+  // of N+(v) ranks below v. dag_rank holds dag_col's entries as ranks (a
+  // single graph only; a batch leaves both null).
+  int32_t *rank = nullptr;        // n
+  int32_t *dag_rank = nullptr;    // nnz (capacity)
+  unsigned long long *rank_keys = nullptr;  // 2 n sort keys
+  int32_t *rank_counts = nullptr;           // radix histograms
+  int64_t *rank_offsets = nullptr;
   uint16_t *keep = nullptr;       // one DAG keep mask per orientation thread
   int32_t *tile_counts = nullptr; // tiles
   int64_t *tile_offsets = nullptr;// tiles + 1
@@ -69,6 +80,7 @@ struct mc_dgraph {
   unsigned long long *h_counters = nullptr;
   unsigned *h_err = nullptr;
   int hub_table_log2 = 10;
+  int bitmap_bits_cap = 0x7fffffff;  // upper bound on hub bitmap capacity (bits)
   cudaEvent_t ev[6] = {};
   int64_t launches = 0;  // kernels launched by the current call
   mc::BatchView batch;   // set by a batch that owns this handle

@@ -25,6 +25,7 @@
 
 #include "dgraph.cuh"
 #include "device_common.cuh"
+#include "radix.cuh"
 #include "scan.cuh"
 
 namespace mc {
@@ -130,7 +131,8 @@ __device__ __forceinline__ int block_exclusive_int(int v, int *total) {
 __device__ __forceinline__ void write_span(const TileRows &tr, const int64_t *rowptr, int64_t t0,
                                            int64_t s, int64_t e_end, int64_t r,
                                            const int32_t (&vals)[kEdgesPerThread], unsigned keep,
-                                           int64_t pos, int64_t *out_rowptr, int32_t *out_col) {
+                                           int64_t pos, int64_t *out_rowptr, int32_t *out_col,
+                                           const int32_t *__restrict__ rank, int32_t *out_rank) {
   if (tr.at(r) == s) {
     // Rows starting exactly at s: row r and the empty rows just before it.
     // For s > t0 they all lie in the staged range; the tile's first span may
@@ -148,7 +150,11 @@ __device__ __forceinline__ void write_span(const TileRows &tr, const int64_t *ro
         out_rowptr[r] = pos;
         next = tr.at(r + 1);
       }
-      if (keep & (1u << k)) out_col[pos++] = vals[k];
+      if (keep & (1u << k)) {
+        out_col[pos] = vals[k];
+        if (out_rank) out_rank[pos] = __ldg(rank + vals[k]);
+        ++pos;
+      }
     }
   }
 }
@@ -156,12 +162,14 @@ __device__ __forceinline__ void write_span(const TileRows &tr, const int64_t *ro
 // Pass A (kWrite == false): DAG entries of every thread's span as a 16-bit
 // mask in keep[], per-tile counts, and d+ of every row by atomics on
 // key[].y (which starts at 0).  Pass B (kWrite == true): the kept entries
-// compacted into out_col and out_rowptr[r] = kept entries before rowptr[r].
+// compacted into out_col (and, when rank is given, their ranks into
+// out_rank) and out_rowptr[r] = kept entries before rowptr[r].
 template <bool kWrite>
 __global__ void __launch_bounds__(kTileThreads)
     dag_pass_kernel(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ col,
                     int64_t n, int64_t nnz, int2 *key, uint16_t *keep_masks, int32_t *counts_out,
-                    const int64_t *__restrict__ offs_in, int64_t *out_rowptr, int32_t *out_col) {
+                    const int64_t *__restrict__ offs_in, int64_t *out_rowptr, int32_t *out_col,
+                    const int32_t *__restrict__ rank, int32_t *out_rank) {
   __shared__ int64_t seg[kSegMax];
   const int64_t t0 = (int64_t)blockIdx.x * kTileEdges;
   const int64_t t1 = min(t0 + kTileEdges, nnz);
@@ -214,7 +222,8 @@ __global__ void __launch_bounds__(kTileThreads)
   int total = 0;
   const int64_t base = offs_in[blockIdx.x];
   const int64_t pos = base + block_exclusive_int(__popc(keep), &total);
-  if (s < t1) write_span(tr, rowptr, t0, s, e_end, r, vals, keep, pos, out_rowptr, out_col);
+  if (s < t1)
+    write_span(tr, rowptr, t0, s, e_end, r, vals, keep, pos, out_rowptr, out_col, rank, out_rank);
   // Rows after the last entry (trailing empty rows and q == n) start at nnz.
   if (t1 == nnz)
     for (int64_t q = tr.hi + 1 + threadIdx.x; q <= n; q += kTileThreads) out_rowptr[q] = base + total;
@@ -285,6 +294,24 @@ __global__ void validate_rowptr_kernel(const int64_t *rowptr, int64_t n, int64_t
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) d = max(d, __shfl_down_sync(kFull, d, o));
   if ((threadIdx.x & 31) == 0 && d > 0) atomicMax(max_deg, (unsigned long long)d);
+}
+
+// Degree-rank sort keys: position i holds vertex n-1-i, keyed by
+// (max_degree - degree) in the high word. A stable sort of the high word
+// keeps equal degrees in descending id order, so the sorted position is the
+// rank in (degree desc, id desc) order.
+__global__ void rank_keys_kernel(const int2 *__restrict__ key, int64_t n, int max_degree,
+                                 unsigned long long *__restrict__ keys) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n)
+    keys[i] = ((unsigned long long)(unsigned)(max_degree - key[n - 1 - i].x) << 32) |
+              (unsigned long long)i;
+}
+
+__global__ void rank_scatter_kernel(const unsigned long long *__restrict__ sorted, int64_t n,
+                                    int32_t *__restrict__ rank) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) rank[n - 1 - (int64_t)(uint32_t)sorted[p]] = (int32_t)p;
 }
 
 __global__ void init_key_kernel(const int64_t *rowptr, int64_t n, int2 *key) {
@@ -424,6 +451,8 @@ int tc_alloc(mc_dgraph *g) {
   // Each owner contributes ceil(deg / chunk) <= 1 + deg / chunk tasks.
   g->task_capacity = n + cap / std::min(kHubChunk, kLeafChunk) + 1;
   g->scan_temp_size = std::max(scan_temp_bytes(n + 1), scan_temp_bytes(tiles + 1));
+  const bool ranked = g->batch.gid == nullptr;
+  if (ranked) g->scan_temp_size = std::max(g->scan_temp_size, radix_temp_bytes(n));
 #define MC_ALLOC(ptr, count) \
   MC_CUDA_TRY(dev_alloc((void **)&(ptr), sizeof(*(ptr)) * (size_t)(count), g->stream))
   MC_ALLOC(g->key, n + 1);
@@ -441,6 +470,13 @@ int tc_alloc(mc_dgraph *g) {
   MC_ALLOC(g->mega_cnt, n + 1);
   MC_ALLOC(g->mega_off, n + 1);
   MC_ALLOC(g->mega_tasks, g->task_capacity);
+  if (ranked) {
+    MC_ALLOC(g->rank, n + 1);
+    MC_ALLOC(g->dag_rank, cap);
+    MC_ALLOC(g->rank_keys, 2 * n + 2);
+    MC_ALLOC(g->rank_counts, radix_entries(n) + 1);
+    MC_ALLOC(g->rank_offsets, radix_entries(n) + 1);
+  }
   MC_CUDA_TRY(dev_alloc(&g->scan_temp, g->scan_temp_size, g->stream));
 #undef MC_ALLOC
   g->tc_ready = true;
@@ -456,18 +492,32 @@ int tc_orient(mc_dgraph *g) {
   init_key_kernel<<<grid_for(n, 256), 256, 0, s>>>(g->rowptr, n, g->key);
   MC_CUDA_TRY(cudaGetLastError());
   g->launches += 1;
+  if (g->rank && !g->batch.gid) {
+    // Degree ranks (the hub kernel's bitmaps are indexed by them).
+    rank_keys_kernel<<<grid_for(n, 256), 256, 0, s>>>(g->key, n, (int)g->max_degree, g->rank_keys);
+    MC_CUDA_TRY(cudaGetLastError());
+    unsigned long long *sorted = nullptr;
+    MC_CUDA_TRY(radix_sort_u64(g->rank_keys, g->rank_keys + n, n, 32,
+                               32 + bit_width((uint64_t)g->max_degree), g->rank_counts,
+                               g->rank_offsets, g->scan_temp, s, &sorted, &g->launches));
+    rank_scatter_kernel<<<grid_for(n, 256), 256, 0, s>>>(sorted, n, g->rank);
+    MC_CUDA_TRY(cudaGetLastError());
+    g->launches += 2;
+  }
   if (tiles == 0) {
     MC_CUDA_TRY(cudaMemsetAsync(g->dag_rowptr, 0, sizeof(int64_t) * (n + 1), s));
   } else {
     const unsigned grid = (unsigned)tiles;
     dag_pass_kernel<false><<<grid, kTileThreads, 0, s>>>(g->rowptr, g->col, n, nnz, g->key,
                                                          g->keep, g->tile_counts, nullptr,
-                                                         nullptr, nullptr);
+                                                         nullptr, nullptr, nullptr, nullptr);
     MC_CUDA_TRY(cudaGetLastError());
     MC_CUDA_TRY(exclusive_scan(g->tile_counts, g->tile_offsets, tiles, g->scan_temp, s));
     dag_pass_kernel<true><<<grid, kTileThreads, 0, s>>>(g->rowptr, g->col, n, nnz, g->key,
                                                         g->keep, nullptr, g->tile_offsets,
-                                                        g->dag_rowptr, g->dag_col);
+                                                        g->dag_rowptr, g->dag_col,
+                                                        g->batch.gid ? nullptr : g->rank,
+                                                        g->batch.gid ? nullptr : g->dag_rank);
     MC_CUDA_TRY(cudaGetLastError());
     g->launches += 2 + scan_launches(tiles);
   }

@@ -39,6 +39,12 @@ struct CountArgs {
   unsigned long long *result;
   unsigned *err;
   int table_log2_max;
+  // Degree ranks: every entry of N+(v) ranks below v, so an owner x whose
+  // rank fits the launch's bitmap capacity keeps N+(x) as a bitmap of
+  // rank(x) bits (null rank: a batch, tables only).
+  const int32_t *__restrict__ rank;
+  const int32_t *__restrict__ dag_rank;  // N+ lists as ranks
+  int bitmap_bits;
   int shard, num_shards;  // this call counts tasks shard, shard + num_shards, ...
   BatchView bv;           // per-graph table factor and counts of a batch
 };
@@ -111,6 +117,21 @@ __device__ __forceinline__ bool cuckoo_insert(int *tab, int shift, int key) {
   return false;
 }
 
+// Membership in a bitmap over ranks [0, limit): an entry at or above the
+// owner's rank cannot be in N+(owner) and reads nothing.
+// The read is unconditional (an entry out of range reads word 0 and is
+// masked off), so a probe is straight-line code with no branch.
+struct BitmapProbe {
+  const unsigned *bits;
+  unsigned limit;
+  __device__ __forceinline__ unsigned operator()(int w) const {
+    const unsigned u = (unsigned)w;  // kNoKey (negative) is above every limit
+    const bool in = u < limit;
+    const unsigned c = in ? u : 0u;
+    return (bits[c >> 5] >> (c & 31)) & (unsigned)in;
+  }
+};
+
 // Binary search in a sorted global list: owners too large for the table, or
 // whose table could not be built.
 struct ListProbe {
@@ -133,36 +154,34 @@ __device__ __forceinline__ bool owns(int x, int px, int y, int py) {
   return py >= 1 && (px > py || (px == py && x > y));
 }
 
-// One warp streams one list col[st, st+len) through `probe`: each lane keeps
-// four 8-byte loads in flight, then probes the eight keys; an odd head and
-// tail are probed by lanes 0 and 1.  Returns this lane's hits.
+// One warp streams one list col[st, st+len) through `probe` with 16-byte
+// loads: lane l takes int4 groups l, l+32, ... of the aligned body, two
+// groups in flight; the at most 3 + 3 entries before the first and after
+// the last 16-byte boundary are probed by lanes 0-2 and 4-6. Returns this
+// lane's hits.
 template <class Probe>
-__device__ __forceinline__ unsigned stream_list(const int32_t *__restrict__ col, int64_t st,
-                                                int len, int lane, const Probe &probe) {
-  constexpr int kU = 4;
+__device__ __forceinline__ unsigned stream_list4(const int32_t *__restrict__ col, int64_t st,
+                                                 int len, int lane, const Probe &probe) {
   unsigned hits = 0;
-  const int head = (int)(st & 1) & (len > 0 ? 1 : 0);
-  const int64_t a = st + head;
-  const int rest = len - head;
-  const int body = rest >> 1;
-  if (head | (rest & 1)) {
-    const bool h = lane == 0 && head, t = lane == 1 && (rest & 1);
-    const int w = h ? __ldg(col + st) : (t ? __ldg(col + a + 2 * body) : kNoKey);
+  const int head = min(len, (int)((4 - (st & 3)) & 3));
+  const int body = (len - head) >> 2;
+  const int tail = len - head - 4 * body;
+  if (head + tail > 0) {
+    int w = kNoKey;
+    if (lane < head) w = __ldg(col + st + lane);
+    else if (lane >= 4 && lane < 4 + tail) w = __ldg(col + st + head + 4 * body + (lane - 4));
     hits += probe(w);
   }
-  const int2 *v = reinterpret_cast<const int2 *>(col + a);
-  for (int k0 = 0; k0 < body; k0 += kWarp * kU) {
-    int2 q[kU];
-    // Blocks of 32 pairs past the end are skipped (a warp-uniform test).
-#pragma unroll
-    for (int u = 0; u < kU; ++u) {
-      const int k = k0 + u * kWarp + lane;
-      q[u] = make_int2(kNoKey, kNoKey);
-      if (k0 + u * kWarp < body && k < body) q[u] = __ldg(v + k);
-    }
-#pragma unroll
-    for (int u = 0; u < kU; ++u)
-      if (k0 + u * kWarp < body) hits += probe(q[u].x) + probe(q[u].y);
+  const int4 *v = reinterpret_cast<const int4 *>(col + st + head);
+  int k = lane;
+  for (; k + kWarp < body; k += 2 * kWarp) {
+    const int4 p = __ldg(v + k), q = __ldg(v + k + kWarp);
+    hits += probe(p.x) + probe(p.y) + probe(p.z) + probe(p.w);
+    hits += probe(q.x) + probe(q.y) + probe(q.z) + probe(q.w);
+  }
+  if (k < body) {
+    const int4 p = __ldg(v + k);
+    hits += probe(p.x) + probe(p.y) + probe(p.z) + probe(p.w);
   }
   return hits;
 }
@@ -174,7 +193,8 @@ __device__ __forceinline__ unsigned stream_list(const int32_t *__restrict__ col,
 template <class Probe>
 __device__ __forceinline__ unsigned long long claim_and_stream(const CountArgs &a, int x, int px,
                                                                int64_t e0, int nc, int *next,
-                                                               int lane, const Probe &probe) {
+                                                               int lane, const Probe &probe,
+                                                               const int32_t *__restrict__ lists) {
   unsigned long long hits = 0;
   for (;;) {
     int g = 0;
@@ -206,7 +226,7 @@ __device__ __forceinline__ unsigned long long claim_and_stream(const CountArgs &
       m &= m - 1;
       const int64_t s = __shfl_sync(kFull, st, p);
       const int l = __shfl_sync(kFull, len, p);
-      h += stream_list(a.dag_col, s, l, lane, probe);
+      h += stream_list4(lists, s, l, lane, probe);
     }
     hits += h;
   }
@@ -242,9 +262,11 @@ __device__ __forceinline__ unsigned long long stream_flat(const int32_t *__restr
 
 __device__ __forceinline__ int ceil_log2(int v) { return v <= 1 ? 0 : 32 - __clz(v - 1); }
 
-// One CTA per hub task: N+(owner) into a cuckoo table of 2^lg slots (load
-// <= 1/4 when it fits, <= 1/2 at the size cap), then the 8 warps claim the
-// row chunk and stream each partner's list through the table.  Owners beyond
+// One CTA per hub task: N+(owner) into shared memory, then the 8 warps claim
+// the row chunk and stream each partner's list through it.  N+(owner) is
+// kept as a bitmap over ranks [0, rank(owner)) when that fits the launch's
+// shared memory (lists streamed as ranks), else as a cuckoo table of 2^lg
+// slots (load <= 1/4 when it fits, <= 1/2 at the size cap).  Owners beyond
 // the cap, or whose table could not be built, are probed by binary search in
 // global memory instead.
 __global__ void __launch_bounds__(kCountThreads, 5) tc_hub_kernel(CountArgs a) {
@@ -270,10 +292,29 @@ __global__ void __launch_bounds__(kCountThreads, 5) tc_hub_kernel(CountArgs a) {
     const int d = a.key[x].y;
     const int64_t e0 = a.rowptr[x] + (int64_t)chunk * kHubChunk;
     const int nc = (int)min((int64_t)kHubChunk, a.rowptr[x + 1] - e0);
+    const int R = a.rank ? __ldg(a.rank + x) : INT_MAX;
+    unsigned long long th = 0;
+    if (R <= a.bitmap_bits) {
+      unsigned *bits = reinterpret_cast<unsigned *>(table);
+      int4 *t4 = reinterpret_cast<int4 *>(table);
+      for (int i = threadIdx.x; i < (R + 127) >> 7; i += blockDim.x) t4[i] = make_int4(0, 0, 0, 0);
+      __syncthreads();
+      for (int i = threadIdx.x; i < d; i += blockDim.x) {
+        const unsigned r = (unsigned)__ldg(a.dag_rank + a0 + i);
+        if (r < (unsigned)R) atomicOr(bits + (r >> 5), 1u << (r & 31));
+        else atomicOr(a.err, kErrRank);  // never written outside the bitmap
+      }
+      __syncthreads();
+      th = claim_and_stream(a, x, d, e0, nc, &s_next, lane, BitmapProbe{bits, (unsigned)R},
+                            a.dag_rank);
+      hits += th;
+      flush_task(a, x, th, lane);
+      __syncthreads();  // the bitmap and the shared words are rewritten by the next task
+      continue;
+    }
     int lg = max(8, ceil_log2(d << table_factor_log2(a, x)));
     if (lg > a.table_log2_max && 2 * d <= (1 << a.table_log2_max)) lg = a.table_log2_max;
     bool use_table = lg <= a.table_log2_max;
-    unsigned long long th = 0;
     if (use_table) {
       const int size = 1 << lg;
       const int shift = 32 - lg;
@@ -287,10 +328,12 @@ __global__ void __launch_bounds__(kCountThreads, 5) tc_hub_kernel(CountArgs a) {
       __syncthreads();
       use_table = s_fail == 0;
       if (use_table)
-        th = claim_and_stream(a, x, d, e0, nc, &s_next, lane, CuckooProbe{table, shift});
+        th = claim_and_stream(a, x, d, e0, nc, &s_next, lane, CuckooProbe{table, shift},
+                              a.dag_col);
     }
     if (!use_table)
-      th = claim_and_stream(a, x, d, e0, nc, &s_next, lane, ListProbe{a.dag_col + a0, d});
+      th = claim_and_stream(a, x, d, e0, nc, &s_next, lane, ListProbe{a.dag_col + a0, d},
+                            a.dag_col);
     hits += th;
     flush_task(a, x, th, lane);
     __syncthreads();  // table and the shared words are rewritten by the next task
@@ -409,15 +452,23 @@ int tc_count_launch(mc_dgraph *g, cudaEvent_t after_hub, int shard, int num_shar
   // Owners with d+ <= kHubSmallMaxOut: tables of at most 2^12 slots (16 KB),
   // so many CTAs share an SM; the few larger owners run in a second launch
   // whose shared memory fits the largest table.
+  // Both launches get at least kHubBitmapBytes: at 5 CTAs per SM (the
+  // register bound) that costs no occupancy and lets owners of rank up to
+  // 8 x kHubBitmapBytes use bitmaps.
   const int small_lg = std::min(kHubSmallTableLog2, g->hub_table_log2);
   const int big_lg = std::max(kHubSmallTableLog2, g->hub_table_log2);
-  const size_t small_smem = sizeof(int) << small_lg, big_smem = sizeof(int) << big_lg;
+  const size_t small_smem = std::max<size_t>(sizeof(int) << small_lg, kHubBitmapBytes);
+  const size_t big_smem = std::max<size_t>(sizeof(int) << big_lg, kHubBitmapBytes);
+  const bool ranked = g->rank != nullptr && g->batch.gid == nullptr;
+  a.rank = ranked ? g->rank : nullptr;
+  a.dag_rank = ranked ? g->dag_rank : nullptr;
   MC_CUDA_TRY(cudaFuncSetAttribute(tc_hub_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)big_smem));
   a.table_log2_max = small_lg;
   a.tasks = g->hub_tasks;
   a.ntasks = g->hub_off + g->n;
   a.queue = g->counters + 1;
+  a.bitmap_bits = (int)std::min<size_t>(small_smem * 8, (size_t)g->bitmap_bits_cap);
   const int small_grid =
       g->num_sms * resident_blocks((const void *)tc_hub_kernel, kCountThreads, small_smem);
   tc_hub_kernel<<<small_grid, kCountThreads, small_smem, g->stream>>>(a);
@@ -426,6 +477,7 @@ int tc_count_launch(mc_dgraph *g, cudaEvent_t after_hub, int shard, int num_shar
   a.tasks = g->mega_tasks;
   a.ntasks = g->mega_off + g->n;
   a.queue = g->counters + 6;
+  a.bitmap_bits = (int)std::min<size_t>(big_smem * 8, (size_t)g->bitmap_bits_cap);
   const int big_grid =
       g->num_sms * resident_blocks((const void *)tc_hub_kernel, kCountThreads, big_smem);
   tc_hub_kernel<<<big_grid, kCountThreads, big_smem, g->stream>>>(a);

@@ -96,13 +96,30 @@ def test_shard_partials_sum_to_the_count(shards):
 
 
 def test_global_memory_fallback_for_large_out_lists(monkeypatch):
-    """With the table capped at 256 slots, owners with d+ > 128 take the
-    binary-search path; the count must not change."""
+    """With bitmaps off and the table capped at 256 slots, owners with
+    d+ > 128 take the binary-search path; the count must not change."""
     g = fixture("dense400")
+    monkeypatch.setenv("MERCURY_TC_BITMAP_BITS", "0")
     monkeypatch.setenv("MERCURY_TC_TABLE_LOG2_MAX", "8")
     with DeviceGraph(g) as d:
         assert d.tc_count() == GOLD["dense400"]["TC"]
         assert d.tc_stats()["max_out_degree"] > 128
+
+
+@pytest.mark.parametrize("cap", ["0", "96", "2048", "1000000"])
+@pytest.mark.parametrize("make", [lambda: Graph.rmat(15, 16, seed=21),
+                                  lambda: Graph.chung_lu(60000, 2.1, 20.0, 5000.0, seed=22),
+                                  lambda: fixture("dense400")])
+def test_hub_bitmap_and_table_paths_agree(monkeypatch, make, cap):
+    """Hub owners keep N+ as a rank bitmap when rank(owner) fits the cap, as a
+    cuckoo table otherwise (cap 0: tables only); every mix gives the oracle's
+    count."""
+    g = make()
+    want = orc.tc(g.rowptr, g.col)
+    monkeypatch.setenv("MERCURY_TC_BITMAP_BITS", cap)
+    with DeviceGraph(g) as d:
+        assert d.tc_count() == want
+        assert d.tc_count() == want
 
 
 def test_empty_and_edgeless_graphs():
