@@ -30,7 +30,8 @@ void release(mc_dgraph *g) {
                   g->hub_cnt,    g->leaf_cnt,   g->hub_off,  g->leaf_off,  g->hub_tasks,
                   g->leaf_tasks, g->scan_temp,  g->counters, g->err, g->pat_scratch,
                   g->mega_cnt,   g->mega_off,   g->mega_tasks, g->rank,
-                  g->dag_rank,   g->rank_keys,  g->rank_counts, g->rank_offsets};
+                  g->dag_rank,   g->rank_keys,  g->rank_counts, g->rank_offsets,
+                  g->center_scratch};
   // Stream-ordered frees: no device-wide synchronisation, so other handles'
   // work keeps running while this one is released.
   for (void *p : bufs)

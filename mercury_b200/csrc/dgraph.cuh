@@ -49,6 +49,8 @@ struct mc_dgraph {
   // ---- pattern-count scratch (frontier lists), grown on demand ----------
   void *pat_scratch = nullptr;
   size_t pat_scratch_bytes = 0;
+  void *center_scratch = nullptr;  // center classes of the bitmap kernels
+  size_t center_scratch_bytes = 0;
 
   // ---- triangle-count scratch, allocated on the first mc_tc_count -------
   bool tc_ready = false;

@@ -19,11 +19,13 @@
 // sign-extended).
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 
 #include "dgraph.cuh"
 #include "device_common.cuh"
+#include "scan.cuh"
 
 namespace mc {
 namespace {
@@ -41,6 +43,11 @@ struct PatArgs {
   int64_t cap;           // list capacity (max degree)
   unsigned long long *counters;  // [0] = c1, [1] = c2
   unsigned long long *queue;
+  // Optional restriction to the large centers (those the center-bitmap
+  // kernels leave out): edge task t of center v is t in
+  // [task_off[v], task_off[v+1]); star tasks skip vertices of degree <= skip_deg.
+  const int64_t *task_off = nullptr;
+  int skip_deg = -1;
 };
 
 __device__ __forceinline__ unsigned long long wrap_mul(int a, int b) {
@@ -217,7 +224,17 @@ __device__ void edge_pattern(const Warp &w, int v0, int v1, int32_t *L, int64_t 
     const int no = nA < nB ? nA : nB, ni = nA < nB ? nB : nA;
     for (int i = 0; i < no; ++i) {
       const int v2 = outer[i];
-      for (int j = w.lane; j < ni; j += kWarp) acc.c1 += !w.in(v2, inner[j]);
+      const int dv2 = w.deg(v2);
+      if (dv2 < ni) {
+        // #{y in inner : y not in N(v2)} = ni - |N(v2) & inner|, searching the
+        // shorter N(v2) in `inner` (the reference's size switch, :898-958).
+        const int32_t *nv2 = w.N(v2);
+        unsigned long long common = 0;
+        for (int j = w.lane; j < dv2; j += kWarp) common += bsearch(inner, ni, __ldg(nv2 + j));
+        acc.c1 += (w.lane == 0 ? (unsigned long long)ni : 0ull) - common;
+      } else {
+        for (int j = w.lane; j < ni; j += kWarp) acc.c1 += !w.in(v2, inner[j]);
+      }
     }
   } else if (P == 5) {  // P5_subgraph_matching (:574-734)
     const int nA = w.inter(n0, d0, v1, -1, L0);
@@ -323,7 +340,7 @@ __global__ void __launch_bounds__(kPatThreads) pattern_kernel(PatArgs a) {
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
   int32_t *L = a.scratch + gw * kLists * a.cap;
   const Warp w{a.rp, a.ci, lane};
-  const int64_t ntasks = kStar ? a.n : a.nnz;
+  const int64_t ntasks = kStar ? a.n : (a.task_off ? a.task_off[a.n] : a.nnz);
   Acc acc;
   for (;;) {
     unsigned long long t = 0;
@@ -331,7 +348,11 @@ __global__ void __launch_bounds__(kPatThreads) pattern_kernel(PatArgs a) {
     t = __shfl_sync(kFull, t, 0);
     if ((int64_t)t >= ntasks) break;
     if (kStar) {
-      vertex_star(w, (int)t, L, acc);
+      if (w.deg((int)t) > a.skip_deg) vertex_star(w, (int)t, L, acc);
+    } else if (a.task_off) {
+      const int v0 = (int)upper_row(a.task_off, 0, a.n - 1, (int64_t)t);
+      const int64_t e = __ldg(a.rp + v0) + ((int64_t)t - a.task_off[v0]);
+      edge_pattern<P>(w, v0, __ldg(a.ci + e), L, a.cap, acc);
     } else {
       const int v0 = (int)upper_row(a.rp, 0, a.n - 1, (int64_t)t);
       const int v1 = __ldg(a.ci + t);
@@ -342,6 +363,425 @@ __global__ void __launch_bounds__(kPatThreads) pattern_kernel(PatArgs a) {
   if (lane == 0) {
     if (c1) atomicAdd(a.counters + 0, c1);
     if (c2) atomicAdd(a.counters + 1, c2);
+  }
+}
+
+
+// ---- center bitmaps (P1, P3, P7) -------------------------------------------
+// Every edge (v0, v1) is taken with v0 as its center.  For these three
+// patterns every set of the reference's formula lies inside N0 = N(v0), so a
+// group of warps first builds M, the adjacency among N0: d0 rows of W words,
+// bit j of row i set iff N0[j] ~ N0[i].  v1 = N0[p] and, with A a mask over
+// N0 and below(q) / above(q) the positions before / after q:
+//   P3  A = N0 - N1 = ~M[p];   P7  A = N0 & N1 = M[p]
+//       count(q) = |A & ~M[q] & below(q)|, freq(q) = |A & ~M[q] & above(q)|
+//       c1 += count(q) * freq(q) (32-bit product) for q in A;
+//       c2 += sum over r in A & M[q] of |D & above(r) & ~M[r]|,
+//             D = A & ~M[q] & below(q)      (pattern_kernels.cuh:280-340, :386-449)
+//   P1  star: c1 += |~M[i] & below(i)| * |~M[i] & above(i)| over i
+//       correction: A = ~M[p] & below(p), B = M[p] & below(p),
+//       c2 += sum over r in B of |A & above(r) & ~M[r]|   (:6-133)
+// These are the reference's per-edge counts exactly (the same sets, sizes
+// and products), read off popcounts instead of binary searches.
+constexpr int kCenterMaxDeg = 1024;  // larger centers use pattern_kernel
+constexpr int kCenterClasses = 6;    // W = 1, 2, 4, 8, 16, 32 words per row
+
+__host__ __device__ constexpr int center_words(int cls) { return 1 << cls; }
+// Warps per center: one for small rows, the whole CTA from W = 16 on.
+__host__ __device__ constexpr int center_group(int W) { return W >= 16 ? kPatThreads / kWarp : 1; }
+// Patterns whose formulas also look outside N0: for every y in N1 - N0 - {v0}
+// they need R(y) = N(y) & N0 as a mask over N0.
+__host__ __device__ constexpr bool center_outer(int P) {
+  return P == 2 || P == 4 || P == 5 || P == 6 || P == 8;
+}
+// Shared memory of one group: M (32W rows of W words), N0 (32W ints) and,
+// for the outer patterns, per warp one R row per lane (32 x W words) and a
+// counter per N0 position (32W ints).
+__host__ __device__ constexpr size_t center_group_bytes(int P, int W) {
+  return sizeof(unsigned) * ((size_t)(32 * W) * W + (size_t)(32 * W) +
+                             (center_outer(P) ? (size_t)center_group(W) * (64 * W) : 0));
+}
+
+struct CenterArgs {
+  const int64_t *__restrict__ rp;
+  const int32_t *__restrict__ ci;
+  const int32_t *__restrict__ centers;  // this class's centers
+  const int32_t *__restrict__ count;    // how many
+  unsigned long long *queue;
+  unsigned long long *counters;         // [0] = c1, [1] = c2
+};
+
+// Word k of the mask of positions below q (q in [0, 32W)).
+__device__ __forceinline__ unsigned below_word(int k, int q) {
+  const int qw = q >> 5;
+  return k < qw ? ~0u : (k == qw ? ((1u << (q & 31)) - 1u) : 0u);
+}
+// Word k of the mask of positions above q.
+__device__ __forceinline__ unsigned above_word(int k, int q) {
+  const int qw = q >> 5;
+  return k > qw ? ~0u : (k == qw ? ~((2u << (q & 31)) - 1u) : 0u);
+}
+__device__ __forceinline__ unsigned full_word(int k, int d) {
+  const int b = d - 32 * k;
+  return b >= 32 ? ~0u : (b <= 0 ? 0u : ((1u << b) - 1u));
+}
+
+__device__ __forceinline__ int ceil_log2_int(int v) { return v <= 1 ? 1 : 32 - __clz(v - 1); }
+
+// Position of y in the sorted n0[0, d0), or -1.
+__device__ __forceinline__ int find_pos(const int32_t *n0, int d0, int y) {
+  int lo = 0, hi = d0 - 1;
+  while (lo <= hi) {
+    const int mid = (lo + hi) >> 1;
+    const int m = n0[mid];
+    if (m == y) return mid;
+    if (m < y) lo = mid + 1;
+    else hi = mid - 1;
+  }
+  return -1;
+}
+
+// Row of x over N0: bit j set iff N0[j] in N(x).  One lane owns the row (no
+// other lane writes it).  The cheapest of three walks is taken: each
+// neighbour of x searched in N0 (shared memory), each N0[j] searched in N(x)
+// (global), or a merge of the two sorted lists.
+template <int W>
+__device__ __forceinline__ void build_row(const int64_t *__restrict__ rp,
+                                          const int32_t *__restrict__ ci, const int32_t *n0,
+                                          int d0, int x, unsigned *row) {
+#pragma unroll
+  for (int k = 0; k < W; ++k) row[k] = 0;
+  const int64_t b = __ldg(rp + x), e = __ldg(rp + x + 1);
+  const int dx = (int)(e - b);
+  const int by_x = dx * ceil_log2_int(d0 + 1);
+  const int by_n0 = d0 * ceil_log2_int(dx + 1);
+  const int merge = dx + d0;
+  if (by_x <= by_n0 && by_x <= merge) {
+    for (int64_t t = b; t < e; ++t) {
+      const int j = find_pos(n0, d0, __ldg(ci + t));
+      if (j >= 0) row[j >> 5] |= 1u << (j & 31);
+    }
+  } else if (by_n0 <= merge) {
+    for (int j = 0; j < d0; ++j) {
+      const int y = n0[j];
+      int64_t lo = b, hi = e - 1;
+      while (lo <= hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        const int m = __ldg(ci + mid);
+        if (m == y) {
+          row[j >> 5] |= 1u << (j & 31);
+          break;
+        }
+        if (m < y) lo = mid + 1;
+        else hi = mid - 1;
+      }
+    }
+  } else {
+    int j = 0;
+    for (int64_t t = b; t < e && j < d0; ++t) {
+      const int y = __ldg(ci + t);
+      while (j < d0 && n0[j] < y) ++j;
+      if (j < d0 && n0[j] == y) row[j >> 5] |= 1u << (j & 31);
+    }
+  }
+}
+
+__device__ __forceinline__ bool bit_of(const unsigned *row, int j) {
+  return (row[j >> 5] >> (j & 31)) & 1u;
+}
+
+// Warp wg of the center's G warps takes edges p = wg, wg + G, ...; its lanes
+// split the positions q (P3, P7) or r (P1) of each edge.  Membership in A
+// and B is read from M's row p; the fully unrolled word loops keep A and D
+// in registers.
+template <int P, int W>
+__device__ __forceinline__ void center_edges(const unsigned *M, int d0, int wg, int G, int lane,
+                                             Acc &acc) {
+  for (int p = wg; p < d0; p += G) {
+    const unsigned *mp = M + p * W;
+    if (P == 1) {
+      unsigned A[W];
+#pragma unroll
+      for (int k = 0; k < W; ++k) A[k] = ~mp[k] & below_word(k, p) & full_word(k, d0);
+      for (int r = lane; r < p; r += kWarp) {
+        if (!bit_of(mp, r)) continue;  // r in B = N0 & N1 below p
+        const unsigned *mr = M + r * W;
+        int c = 0;
+#pragma unroll
+        for (int k = 0; k < W; ++k) c += __popc(A[k] & above_word(k, r) & ~mr[k]);
+        acc.c2 += (unsigned long long)c;
+      }
+    } else {
+      unsigned A[W];
+#pragma unroll
+      for (int k = 0; k < W; ++k) A[k] = (P == 3 ? ~mp[k] : mp[k]) & full_word(k, d0);
+      for (int q = lane; q < d0; q += kWarp) {
+        if (bit_of(mp, q) != (P == 7)) continue;  // q in A
+        const unsigned *mq = M + q * W;
+        unsigned D[W];
+        int cnt = 0, freq = 0;
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+          const unsigned nq = A[k] & ~mq[k];
+          D[k] = nq & below_word(k, q);
+          cnt += __popc(D[k]);
+          freq += __popc(nq & above_word(k, q));
+        }
+        acc.c1 += wrap_mul(cnt, freq);
+        if (cnt == 0) continue;  // D empty: no correction term
+        for (int k = 0; k < W; ++k) {
+          unsigned cw = (P == 3 ? ~mp[k] : mp[k]) & mq[k] & full_word(k, d0);  // A & N(q)
+          while (cw) {
+            const int r = 32 * k + __ffs(cw) - 1;
+            cw &= cw - 1;
+            const unsigned *mr = M + r * W;
+            int c = 0;
+#pragma unroll
+            for (int k2 = 0; k2 < W; ++k2) c += __popc(D[k2] & above_word(k2, r) & ~mr[k2]);
+            acc.c2 += (unsigned long long)c;
+          }
+        }
+      }
+    }
+  }
+}
+
+// P2, P4, P5, P6, P8 for the edges p = wg, wg + G, ... of center v0.  The
+// lanes split y over N1 = N(v1); each y outside N0 and other than v0 gets
+// its row R(y) in the lane's own scratch row, then (A, B masks over N0 in
+// registers, M in shared memory):
+//   P2/P8  A = N0 - N1 (P2) or N0 & N1 (P8): cnt[r]++ and
+//          c2 += |(A & ~R) & above(r) & ~M[r] (P2) / M[r] (P8)| for r in A & R;
+//          afterwards c1 += |A & ~M[q] / M[q] & below(q)| * ((|N1 - N0| - 1) - cnt[q])
+//          for q in A                             (:135-243, :461-572)
+//   P5     A = N0 & N1, B = N0 - N1: cnt[b]++ for b in B & R,
+//          c2 += |B & ~M[v2] & ~R| for v2 in A & R; afterwards
+//          c1 += ((|N1 - N0| - 1) - cnt[b]) * |A & ~M[b]| for b in B   (:574-734)
+//   P6     A = N0 & N1: c1 += |A & ~R & ~M[v2]| for v2 in A & ~R       (:736-853)
+//   P4     (v1 < v0 only) A = N0 - N1: c1 += |A & ~R|                 (:855-963)
+// v0 itself (in N1 - N0) is adjacent to every vertex of N0 and adds nothing
+// to any term, which the "- 1" accounts for.
+template <int P, int W>
+__device__ __forceinline__ void center_outer_edges(const int64_t *__restrict__ rp,
+                                                   const int32_t *__restrict__ ci,
+                                                   const unsigned *M, const int32_t *n0, int d0,
+                                                   int v0, int wg, int G, int lane,
+                                                   unsigned *Rl, int *cnt, Acc &acc) {
+  for (int p = wg; p < d0; p += G) {
+    const int v1 = n0[p];
+    if (P == 4 && !(v1 < v0)) continue;
+    const unsigned *mp = M + p * W;
+    unsigned A[W], B[W];
+    int in_both = 0;
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      const unsigned f = full_word(k, d0);
+      const bool a_out = (P == 2 || P == 4);  // A = N0 - N1
+      A[k] = (a_out ? ~mp[k] : mp[k]) & f;
+      B[k] = ~mp[k] & f;
+      in_both += __popc(mp[k]);
+    }
+    const bool counts = (P == 2 || P == 5 || P == 8);
+    if (counts) {
+      for (int i = lane; i < d0; i += kWarp) cnt[i] = 0;
+      __syncwarp();
+    }
+    const int64_t b1 = __ldg(rp + v1);
+    const int d1 = (int)(__ldg(rp + v1 + 1) - b1);
+    for (int j = lane; j < d1; j += kWarp) {
+      const int y = __ldg(ci + b1 + j);
+      if (y == v0 || find_pos(n0, d0, y) >= 0) continue;
+      build_row<W>(rp, ci, n0, d0, y, Rl);
+      if (P == 4) {
+        int c = 0;
+#pragma unroll
+        for (int k = 0; k < W; ++k) c += __popc(A[k] & ~Rl[k]);
+        acc.c1 += (unsigned long long)c;
+      } else if (P == 6) {
+        for (int k = 0; k < W; ++k) {
+          unsigned sw = mp[k] & full_word(k, d0) & ~Rl[k];  // A & ~R
+          while (sw) {
+            const int v2 = 32 * k + __ffs(sw) - 1;
+            sw &= sw - 1;
+            const unsigned *m2 = M + v2 * W;
+            int c = 0;
+#pragma unroll
+            for (int k2 = 0; k2 < W; ++k2) c += __popc(A[k2] & ~Rl[k2] & ~m2[k2]);
+            acc.c1 += (unsigned long long)c;
+          }
+        }
+      } else if (P == 5) {
+        for (int k = 0; k < W; ++k) {
+          unsigned bw = (~mp[k] & full_word(k, d0)) & Rl[k];  // B & R
+          while (bw) {
+            const int bpos = 32 * k + __ffs(bw) - 1;
+            bw &= bw - 1;
+            atomicAdd(cnt + bpos, 1);
+          }
+          unsigned aw = mp[k] & Rl[k];  // A & R
+          while (aw) {
+            const int v2 = 32 * k + __ffs(aw) - 1;
+            aw &= aw - 1;
+            const unsigned *m2 = M + v2 * W;
+            int c = 0;
+#pragma unroll
+            for (int k2 = 0; k2 < W; ++k2) c += __popc(B[k2] & ~m2[k2] & ~Rl[k2]);
+            acc.c2 += (unsigned long long)c;
+          }
+        }
+      } else {  // P2, P8
+        for (int k = 0; k < W; ++k) {
+          unsigned cw = ((P == 2 ? ~mp[k] : mp[k]) & full_word(k, d0)) & Rl[k];  // A & R
+          while (cw) {
+            const int r = 32 * k + __ffs(cw) - 1;
+            cw &= cw - 1;
+            atomicAdd(cnt + r, 1);
+            const unsigned *mr = M + r * W;
+            int c = 0;
+#pragma unroll
+            for (int k2 = 0; k2 < W; ++k2)
+              c += __popc(A[k2] & ~Rl[k2] & above_word(k2, r) & (P == 2 ? ~mr[k2] : mr[k2]));
+            acc.c2 += (unsigned long long)c;
+          }
+        }
+      }
+    }
+    if (counts) {
+      __syncwarp();
+      const int others = (d1 - in_both) - 1;  // |N1 - N0| without v0
+      if (P == 5) {
+        for (int q = lane; q < d0; q += kWarp) {
+          if (bit_of(mp, q)) continue;  // q in B = N0 - N1
+          const unsigned *mq = M + q * W;
+          int f = 0;
+#pragma unroll
+          for (int k = 0; k < W; ++k) f += __popc(A[k] & ~mq[k]);
+          acc.c1 += wrap_mul(others - cnt[q], f);
+        }
+      } else {
+        for (int q = lane; q < d0; q += kWarp) {
+          if (bit_of(mp, q) != (P == 8)) continue;  // q in A
+          const unsigned *mq = M + q * W;
+          int c = 0;
+#pragma unroll
+          for (int k = 0; k < W; ++k)
+            c += __popc(A[k] & (P == 2 ? ~mq[k] : mq[k]) & below_word(k, q));
+          acc.c1 += wrap_mul(c, others - cnt[q]);
+        }
+      }
+      __syncwarp();  // cnt is cleared for the next edge
+    }
+  }
+}
+
+// Persistent groups of G warps take centers of this class from the queue.
+template <int P, int W>
+__global__ void __launch_bounds__(kPatThreads) center_kernel(CenterArgs a) {
+  constexpr int G = center_group(W);
+  constexpr int kGroups = kPatThreads / kWarp / G;
+  extern __shared__ unsigned char smem[];
+  __shared__ int s_center[kGroups];
+  const int lane = threadIdx.x & (kWarp - 1), warp = threadIdx.x / kWarp;
+  const int grp = warp / G, wg = warp % G, gl = wg * kWarp + lane;  // lane within the group
+  unsigned *M = reinterpret_cast<unsigned *>(smem + grp * center_group_bytes(P, W));
+  int32_t *n0 = reinterpret_cast<int32_t *>(M + 32 * W * W);
+  // Outer patterns: this warp's R rows (one per lane) and position counters.
+  unsigned *Rw = reinterpret_cast<unsigned *>(n0 + 32 * W) + wg * (64 * W);
+  unsigned *Rl = Rw + lane * W;
+  int *cnt = reinterpret_cast<int *>(Rw + 32 * W);
+  const int total = *a.count;
+  Acc acc;
+  for (;;) {
+    if (gl == 0) {
+      const unsigned long long t = atomicAdd(a.queue, 1ull);
+      s_center[grp] = (int64_t)t < total ? a.centers[t] : -1;
+    }
+    if (G == 1) __syncwarp(); else __syncthreads();
+    const int v0 = s_center[grp];
+    if (v0 < 0) break;
+    const int64_t b0 = __ldg(a.rp + v0);
+    const int d0 = (int)(__ldg(a.rp + v0 + 1) - b0);
+    for (int i = gl; i < d0; i += G * kWarp) n0[i] = __ldg(a.ci + b0 + i);
+    if (G == 1) __syncwarp(); else __syncthreads();
+    for (int i = gl; i < d0; i += G * kWarp) build_row<W>(a.rp, a.ci, n0, d0, n0[i], M + i * W);
+    if (G == 1) __syncwarp(); else __syncthreads();
+    if (P == 1) {  // star term of v0 (P1_frequency_count)
+      for (int i = gl; i < d0; i += G * kWarp) {
+        const unsigned *mi = M + i * W;
+        int c = 0, f = 0;
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+          const unsigned non = ~mi[k] & full_word(k, d0);
+          c += __popc(non & below_word(k, i));
+          f += __popc(non & above_word(k, i));
+        }
+        acc.c1 += wrap_mul(c, f);
+      }
+    }
+    if constexpr (center_outer(P))
+      center_outer_edges<P, W>(a.rp, a.ci, M, n0, d0, v0, wg, G, lane, Rl, cnt, acc);
+    else
+      center_edges<P, W>(M, d0, wg, G, lane, acc);
+    if (G == 1) __syncwarp(); else __syncthreads();  // M and n0 are rewritten next
+  }
+  const unsigned long long c1 = warp_sum_u64(acc.c1), c2 = warp_sum_u64(acc.c2);
+  if (lane == 0) {
+    if (c1) atomicAdd(a.counters + 0, c1);
+    if (c2) atomicAdd(a.counters + 1, c2);
+  }
+}
+
+// Splits the vertices into the six center classes (1 <= degree <= 1024;
+// class c holds degrees in (16 * 2^c, 32 * 2^c], class 0 from 1) and marks
+// the larger ones: big_deg[v] = degree if above kCenterMaxDeg, else 0.
+__global__ void center_classes_kernel(const int64_t *__restrict__ rp, int64_t n,
+                                      int32_t *__restrict__ lists, int32_t *__restrict__ counts,
+                                      int32_t *__restrict__ big_deg) {
+  __shared__ int h[kCenterClasses], base[kCenterClasses];
+  if (threadIdx.x < kCenterClasses) h[threadIdx.x] = 0;
+  __syncthreads();
+  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int cls = -1, slot = 0;
+  if (v < n) {
+    const int d = (int)(rp[v + 1] - rp[v]);
+    big_deg[v] = d > kCenterMaxDeg ? d : 0;
+    if (d >= 1 && d <= kCenterMaxDeg) {
+      cls = 0;
+      while (32 * center_words(cls) < d) ++cls;
+      slot = atomicAdd(&h[cls], 1);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < kCenterClasses) base[threadIdx.x] = atomicAdd(counts + threadIdx.x, h[threadIdx.x]);
+  __syncthreads();
+  if (cls >= 0) lists[(int64_t)cls * n + base[cls] + slot] = (int32_t)v;
+}
+
+template <int P, int W>
+int launch_center(mc_dgraph *g, const CenterArgs &a, int num_sms) {
+  constexpr int G = center_group(W);
+  const size_t smem = center_group_bytes(P, W) * (kPatThreads / kWarp / G);
+  auto kern = center_kernel<P, W>;
+  MC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPatThreads, smem) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  kern<<<num_sms * per_sm, kPatThreads, smem, g->stream>>>(a);
+  MC_CUDA_TRY(cudaGetLastError());
+  g->launches += 1;
+  return MC_OK;
+}
+
+template <int P>
+int launch_center_class(mc_dgraph *g, const CenterArgs &a, int cls) {
+  switch (cls) {
+    case 0: return launch_center<P, 1>(g, a, g->num_sms);
+    case 1: return launch_center<P, 2>(g, a, g->num_sms);
+    case 2: return launch_center<P, 4>(g, a, g->num_sms);
+    case 3: return launch_center<P, 8>(g, a, g->num_sms);
+    case 4: return launch_center<P, 16>(g, a, g->num_sms);
+    default: return launch_center<P, 32>(g, a, g->num_sms);
   }
 }
 
@@ -451,6 +891,99 @@ int batch_pattern_grid(int num_sms, int64_t cap, int64_t *warps) {
 
 int pattern_lists() { return kLists; }
 
+namespace {
+
+// P1, P3, P7: centers of degree <= kCenterMaxDeg through the bitmap kernels
+// (one launch per class), the edges (and P1 stars) of larger centers
+// through pattern_kernel restricted to them.
+// Default route per pattern, from timings on a Chung-Lu graph (n 100,000,
+// mean degree 10, cap 200) on a B200: the center bitmaps win for P1 (2.1x
+// over the warp-per-edge kernel), P2 (1.4x) and P3 (17x).  P7's sets are
+// small, so building M costs more than its probes save, and for P4, P5, P6,
+// P8 building R(y) for every outer neighbour costs 6-30x more than the
+// warp-per-edge kernel's searches.
+bool pattern_uses_centers(int pattern) { return pattern == 1 || pattern == 2 || pattern == 3; }
+
+int center_path(mc_dgraph *g, int pattern, PatArgs a, int grid) {
+  cudaStream_t s = g->stream;
+  const int64_t n = g->n;
+  // Scratch: class lists (kCenterClasses * n), class counts and queues,
+  // big_deg (n), big_off (n + 1), scan temporary.
+  const size_t lists_b = sizeof(int32_t) * (size_t)(kCenterClasses * n);
+  const size_t words_b = 256;
+  const size_t deg_b = sizeof(int32_t) * (size_t)(n + 1);
+  const size_t off_b = sizeof(int64_t) * (size_t)(n + 1);
+  const size_t temp_b = scan_temp_bytes(n);
+  auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
+  const size_t need = up(lists_b) + words_b + up(deg_b) + up(off_b) + up(temp_b);
+  if (need > g->center_scratch_bytes) {
+    if (g->center_scratch) dev_free(g->center_scratch, s);
+    g->center_scratch = nullptr;
+    g->center_scratch_bytes = 0;
+    MC_CUDA_TRY(dev_alloc(&g->center_scratch, need, s));
+    g->center_scratch_bytes = need;
+  }
+  char *base = static_cast<char *>(g->center_scratch);
+  int32_t *lists = reinterpret_cast<int32_t *>(base);
+  char *words = base + up(lists_b);
+  int32_t *counts = reinterpret_cast<int32_t *>(words);                       // 6 ints
+  unsigned long long *queues = reinterpret_cast<unsigned long long *>(words + 64);  // 6 words
+  int32_t *big_deg = reinterpret_cast<int32_t *>(words + words_b);
+  int64_t *big_off = reinterpret_cast<int64_t *>(reinterpret_cast<char *>(big_deg) + up(deg_b));
+  void *temp = reinterpret_cast<char *>(big_off) + up(off_b);
+
+  MC_CUDA_TRY(cudaMemsetAsync(words, 0, words_b, s));
+  center_classes_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g->rowptr, n, lists, counts,
+                                                                   big_deg);
+  MC_CUDA_TRY(cudaGetLastError());
+  MC_CUDA_TRY(exclusive_scan(big_deg, big_off, n, temp, s));
+  g->launches += 1 + scan_launches(n);
+  int32_t h_counts[kCenterClasses];
+  int64_t big_total = 0;
+  MC_CUDA_TRY(cudaMemcpyAsync(h_counts, counts, sizeof(h_counts), cudaMemcpyDeviceToHost, s));
+  MC_CUDA_TRY(cudaMemcpyAsync(&big_total, big_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  MC_CUDA_TRY(cudaStreamSynchronize(s));
+  for (int c = 0; c < kCenterClasses; ++c) {
+    if (h_counts[c] == 0) continue;
+    CenterArgs ca{g->rowptr, g->col, lists + (int64_t)c * n, counts + c, queues + c, g->counters};
+    int rc = MC_OK;
+    switch (pattern) {
+      case 1: rc = launch_center_class<1>(g, ca, c); break;
+      case 2: rc = launch_center_class<2>(g, ca, c); break;
+      case 3: rc = launch_center_class<3>(g, ca, c); break;
+      case 4: rc = launch_center_class<4>(g, ca, c); break;
+      case 5: rc = launch_center_class<5>(g, ca, c); break;
+      case 6: rc = launch_center_class<6>(g, ca, c); break;
+      case 7: rc = launch_center_class<7>(g, ca, c); break;
+      default: rc = launch_center_class<8>(g, ca, c); break;
+    }
+    if (rc != MC_OK) return rc;
+  }
+  // Larger centers: the warp-per-edge kernel over their edges only.
+  a.skip_deg = kCenterMaxDeg;
+  if (pattern == 1) {
+    int rc = launch_pattern<1, true>(g, a, grid);  // stars of degree > kCenterMaxDeg
+    if (rc != MC_OK) return rc;
+    a.queue = g->counters + 3;
+  }
+  if (big_total > 0) {
+    a.task_off = big_off;
+    switch (pattern) {
+      case 1: return launch_pattern<1, false>(g, a, grid);
+      case 2: return launch_pattern<2, false>(g, a, grid);
+      case 3: return launch_pattern<3, false>(g, a, grid);
+      case 4: return launch_pattern<4, false>(g, a, grid);
+      case 5: return launch_pattern<5, false>(g, a, grid);
+      case 6: return launch_pattern<6, false>(g, a, grid);
+      case 7: return launch_pattern<7, false>(g, a, grid);
+      default: return launch_pattern<8, false>(g, a, grid);
+    }
+  }
+  return MC_OK;
+}
+
+}  // namespace
+
 int pattern_count(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12, mc_timing_t *timing) {
   cudaStream_t s = g->stream;
   const int64_t launches_before = g->launches;
@@ -472,22 +1005,32 @@ int pattern_count(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12, mc_ti
   MC_CUDA_TRY(cudaEventRecord(g->ev[0], s));
   int rc = MC_OK;
   if (g->n > 0 && g->nnz > 0) {
-    switch (pattern) {
-      case 1:
-        rc = launch_pattern<1, true>(g, a, grid);
-        if (rc == MC_OK) {
-          a.queue = g->counters + 3;
-          rc = launch_pattern<1, false>(g, a, grid);
-        }
-        break;
-      case 2: rc = launch_pattern<2, false>(g, a, grid); break;
-      case 3: rc = launch_pattern<3, false>(g, a, grid); break;
-      case 4: rc = launch_pattern<4, false>(g, a, grid); break;
-      case 5: rc = launch_pattern<5, false>(g, a, grid); break;
-      case 6: rc = launch_pattern<6, false>(g, a, grid); break;
-      case 7: rc = launch_pattern<7, false>(g, a, grid); break;
-      case 8: rc = launch_pattern<8, false>(g, a, grid); break;
-      default: return MC_ERR_ARG;
+    // MERCURY_PATTERN_KERNEL=edge / =centers forces one route for every
+    // pattern (the tests run all three settings; timing comparisons use it).
+    const char *route = std::getenv("MERCURY_PATTERN_KERNEL");
+    bool centers = pattern_uses_centers(pattern);
+    if (route && std::strcmp(route, "edge") == 0) centers = false;
+    if (route && std::strcmp(route, "centers") == 0) centers = true;
+    if (pattern < 1 || pattern > 8) return MC_ERR_ARG;
+    if (centers) {
+      rc = center_path(g, pattern, a, grid);
+    } else {
+      switch (pattern) {
+        case 1:
+          rc = launch_pattern<1, true>(g, a, grid);
+          if (rc == MC_OK) {
+            a.queue = g->counters + 3;
+            rc = launch_pattern<1, false>(g, a, grid);
+          }
+          break;
+        case 2: rc = launch_pattern<2, false>(g, a, grid); break;
+        case 3: rc = launch_pattern<3, false>(g, a, grid); break;
+        case 4: rc = launch_pattern<4, false>(g, a, grid); break;
+        case 5: rc = launch_pattern<5, false>(g, a, grid); break;
+        case 6: rc = launch_pattern<6, false>(g, a, grid); break;
+        case 7: rc = launch_pattern<7, false>(g, a, grid); break;
+        default: rc = launch_pattern<8, false>(g, a, grid); break;
+      }
     }
   }
   if (rc != MC_OK) return rc;

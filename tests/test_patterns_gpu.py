@@ -47,6 +47,67 @@ def test_patterns_chung_lu_vs_oracle():
             assert d.pattern_count(k) == orc.pattern(rp, col, k), k
 
 
+def center_class_graph():
+    """One center per degree class of the bitmap kernels (20, 50, 100, 200,
+    450, 900) and a hub of degree 1100 (above the bitmap limit), attached to a
+    pool of 3,993 vertices, with 2d chords inside each center's neighbourhood
+    and 8,000 random pool edges (seeded numpy)."""
+    rng = np.random.default_rng(2024)
+    n = 4000
+    centers = [(0, 20), (1, 50), (2, 100), (3, 200), (4, 450), (5, 900), (6, 1100)]
+    pool = np.arange(7, n)
+    edges = []
+    for c, d in centers:
+        nb = rng.choice(pool, d, replace=False)
+        edges += [(c, int(x)) for x in nb]
+        # chords inside the neighbourhood: triangles and 4-cliques through c
+        i, j = rng.integers(0, d, 2 * d), rng.integers(0, d, 2 * d)
+        edges += [(int(nb[x]), int(nb[y])) for x, y in zip(i, j)]
+    a, b = rng.integers(7, n, 8000), rng.integers(7, n, 8000)
+    edges += [(int(x), int(y)) for x, y in zip(a, b)]
+    return csr_from_edges(n, edges)
+
+
+@pytest.mark.parametrize("route", ["default", "centers", "edge"])
+def test_center_classes_and_big_centers_vs_oracle(monkeypatch, route):
+    """On the center route, centers of degree <= 1024 go through the bitmap
+    kernels (every class here) and larger ones through the warp-per-edge
+    kernel; MERCURY_PATTERN_KERNEL forces one route for every pattern. All
+    routes give the oracle's counts (tests/golden/make_center_golden.py)."""
+    with open(os.path.join(GOLDEN, "center_counts.json")) as f:
+        want = json.load(f)
+    if route != "default":
+        monkeypatch.setenv("MERCURY_PATTERN_KERNEL", route)
+    rp, col = center_class_graph()
+    assert len(col) == want["nnz"]
+    with DeviceGraph(rp, col) as d:
+        for k in range(1, 9):
+            assert d.pattern_count(k) == want[f"P{k}"], k
+
+
+@pytest.mark.parametrize("seed", [4])
+def test_center_patterns_chung_lu_vs_oracle(seed):
+    g = Graph.chung_lu(6000, 2.1, 8.0, 300.0, seed=seed)
+    rp, col = np.array(g.rowptr), np.array(g.col)
+    with DeviceGraph(g) as d:
+        for k in (1, 3, 7):
+            assert d.pattern_count(k) == orc.pattern(rp, col, k), k
+
+
+@pytest.mark.parametrize("make", [lambda: Graph.chung_lu(30000, 2.1, 12.0, 900.0, seed=7),
+                                  lambda: Graph.rmat(13, 16, seed=5)])
+def test_center_route_equals_edge_route(monkeypatch, make):
+    """Every pattern: the bitmap route equals the warp-per-edge route, on
+    graphs with centers in every class (too large for the oracle here)."""
+    g = make()
+    with DeviceGraph(g) as d:
+        monkeypatch.setenv("MERCURY_PATTERN_KERNEL", "centers")
+        fast = [d.pattern_count(k) for k in range(1, 9)]
+        monkeypatch.setenv("MERCURY_PATTERN_KERNEL", "edge")
+        slow = [d.pattern_count(k) for k in range(1, 9)]
+    assert fast == slow
+
+
 def test_pattern_relabel_invariance():
     g = Graph.rmat(9, 8, seed=3)
     rp, col = np.array(g.rowptr), np.array(g.col)
