@@ -282,16 +282,18 @@ def run_reference(a, rank, world):
 
 # ---------------------------------------------------------------- ranks
 def combine_ranks(partial_count: int, elapsed_ms: float, device):
-    """Sum of the ranks' partial counts and the max of their times (the
-    reference's MPI_Reduce SUM and MAX, tc_multigpu/tc_challenge_multigpu.cu
-    :198-206), over the default process group."""
+    """Sum of the ranks' partial counts modulo 2^64 (the counts are uint64;
+    pattern partials can wrap) and the max of their times (the reference's
+    MPI_Reduce SUM and MAX, tc_multigpu/tc_challenge_multigpu.cu:198-206),
+    over the default process group."""
     import torch
     import torch.distributed as dist
-    c = torch.tensor([partial_count], dtype=torch.int64, device=device)
+    u = partial_count % (1 << 64)
+    c = torch.tensor([u - (1 << 64) if u >= (1 << 63) else u], dtype=torch.int64, device=device)
     t = torch.tensor([elapsed_ms], dtype=torch.float64, device=device)
-    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)  # two's-complement sum = sum mod 2^64
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return int(c.item()), float(t.item())
+    return int(c.item()) % (1 << 64), float(t.item())
 
 
 def shard_of(rank: int, world: int):
@@ -577,27 +579,43 @@ def run_serve(a, local_rank):
     return 0
 
 
-def run_patterns(a, local_rank):
+def run_patterns(a, rank, world, local_rank):
     """P1..P8 on one seeded Chung-Lu graph: count and device time per
-    pattern (matches/s = count / kernel time; directed-edge tasks/s beside)."""
+    pattern (matches/s = count / kernel time; directed-edge tasks/s beside).
+    Under torchrun each rank holds the graph and counts its shard; the
+    partial counts are summed (mod 2^64) and the time is the max over ranks."""
     import torch
     from mercury_b200 import DeviceGraph, Graph
     torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     g = Graph.chung_lu(a.pat_n, 2.1, a.pat_mean, a.pat_cap, seed=1)
     per = []
     with DeviceGraph(g) as d:
+        def count(k):
+            if world == 1:
+                return d.pattern_count(k), d.last_timing.count_ms
+            part = d.pattern_count_shard(k, *shard_of(rank, world))
+            return combine_ranks(part, d.last_timing.count_ms, "cuda")
         for k in range(1, 9):
-            first = d.pattern_count(k)
+            first, _ = count(k)
             ts = []
             for _ in range(max(a.steps, 1)):
-                assert d.pattern_count(k) == first
-                ts.append(d.last_timing.count_ms)
+                c, ms = count(k)
+                assert c == first
+                ts.append(ms)
             ms = statistics.mean(ts)
             per.append({"pattern": f"P{k}", "count": first, "ms": ms,
                         "matches_per_s": first / (ms / 1e3) if ms > 0 else None,
                         "edge_tasks_per_s": g.nnz / (ms / 1e3) if ms > 0 else None})
+    if world > 1:
+        dist.destroy_process_group()
+        if rank != 0:
+            return 0
     line = {"metric": "P1-P8 matches/s", "value": statistics.mean(p["matches_per_s"] for p in per),
-            "unit": "matches/s", "n_gpus": 1, "higher_is_better": True, "vs_baseline": None,
+            "unit": "matches/s", "n_gpus": world, "higher_is_better": True, "vs_baseline": None,
             "dtype": "int32", "data": "synthetic",
             "config": {"workload": f"Chung-Lu n={a.pat_n} gamma 2.1 mean {a.pat_mean} cap "
                                    f"{a.pat_cap} seed 1", "n": g.n, "m": g.nnz // 2,
@@ -690,7 +708,9 @@ def main():
     if a.mode == "build":
         return run_build(a, int(os.environ.get("LOCAL_RANK", "0")))
     if a.mode == "patterns":
-        return run_patterns(a, int(os.environ.get("LOCAL_RANK", "0")))
+        return run_patterns(a, int(os.environ.get("RANK", "0")),
+                            int(os.environ.get("WORLD_SIZE", "1")),
+                            int(os.environ.get("LOCAL_RANK", "0")))
     if a.mode == "batch":
         return run_batch(a, 0, 1, int(os.environ.get("LOCAL_RANK", "0")))
     if a.mode == "serve":

@@ -237,6 +237,17 @@ int mc_dgraph_export_dag(const mc_dgraph_t *g, int64_t *rowptr_out,
  * entries per list, grown on first use and kept by the handle. */
 int mc_pattern_count(mc_dgraph_t *g, int pattern, uint64_t *count,
                      mc_timing_t *timing);
+/* One shard of mc_pattern_count for multi-GPU runs with the graph
+ * replicated on every GPU (the reference splits the edge list round-robin
+ * across MPI ranks and reduces with MPI_Reduce, sm_multigpu.cu:12-95,
+ * :206-232). Shard s of num_shards takes the centers v with
+ * v mod num_shards == s, and the matching share of the remaining edge and
+ * star tasks. Every pattern is c1 - c2 (or c1) of sums over edges and
+ * vertices, so the num_shards partial results sum to the count modulo
+ * 2^64. */
+int mc_pattern_count_shard(mc_dgraph_t *g, int pattern, int shard,
+                           int num_shards, uint64_t *partial,
+                           mc_timing_t *timing);
 
 /* Pattern count P<pattern> (1..8) of a symmetric CSR the caller already
  * holds in device memory (d_rowptr: int64[n+1], d_col: int32[nnz]), for

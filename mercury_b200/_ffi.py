@@ -115,6 +115,7 @@ SIGNATURES = {
     "mc_dgraph_export_dag": (C.c_int, [_P, _P, _P]),
     "mc_tc_count_host": (C.c_int, [_P, _P, _I64, _I64, _PU64, C.POINTER(Timing)]),
     "mc_pattern_count": (C.c_int, [_P, C.c_int, _PU64, C.POINTER(Timing)]),
+    "mc_pattern_count_shard": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _PU64, C.POINTER(Timing)]),
     "mc_pattern_count_static": (C.c_int, [_P, _P, _I64, _I64, C.c_int, _PU64, _P]),
     "mc_batch_create": (C.c_int, [_P, _P, _I64, _I64, _P, C.c_int, _P, _P, _PP]),
     "mc_batch_autotune": (C.c_int, [_P, _P]),

@@ -102,7 +102,10 @@ int validate_csr_words(const int64_t *rowptr, const int32_t *col, int64_t n, int
 // tc.cu
 int tc_count_launch(mc_dgraph *g, cudaEvent_t after_hub, int shard, int num_shards);
 // patterns.cu: result of P<pattern>; c12 (optional) receives counters 1 and 2.
-int pattern_count(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12, mc_timing_t *timing);
+// Shard `shard` of `num_shards` (0 of 1: the whole count); partial results
+// of all shards sum to the count modulo 2^64.
+int pattern_count(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12, mc_timing_t *timing,
+                  int shard = 0, int num_shards = 1);
 
 // Pattern tasks of a batch (see batch.cu): pattern graphs 0..num_graphs-1.
 struct BatchPatternArgs {

@@ -48,6 +48,9 @@ struct PatArgs {
   // [task_off[v], task_off[v+1]); star tasks skip vertices of degree <= skip_deg.
   const int64_t *task_off = nullptr;
   int skip_deg = -1;
+  // Shard `shard` of `num_shards` takes queue positions t -> task
+  // t * num_shards + shard (partial counts of all shards sum to the count).
+  int shard = 0, num_shards = 1;
 };
 
 __device__ __forceinline__ unsigned long long wrap_mul(int a, int b) {
@@ -340,13 +343,15 @@ __global__ void __launch_bounds__(kPatThreads) pattern_kernel(PatArgs a) {
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
   int32_t *L = a.scratch + gw * kLists * a.cap;
   const Warp w{a.rp, a.ci, lane};
-  const int64_t ntasks = kStar ? a.n : (a.task_off ? a.task_off[a.n] : a.nnz);
+  const int64_t all = kStar ? a.n : (a.task_off ? a.task_off[a.n] : a.nnz);
+  const int64_t ntasks = all > a.shard ? (all - a.shard + a.num_shards - 1) / a.num_shards : 0;
   Acc acc;
   for (;;) {
     unsigned long long t = 0;
     if (lane == 0) t = atomicAdd(a.queue, 1ull);
     t = __shfl_sync(kFull, t, 0);
     if ((int64_t)t >= ntasks) break;
+    t = t * (unsigned long long)a.num_shards + (unsigned long long)a.shard;
     if (kStar) {
       if (w.deg((int)t) > a.skip_deg) vertex_star(w, (int)t, L, acc);
     } else if (a.task_off) {
@@ -734,8 +739,9 @@ __global__ void __launch_bounds__(kPatThreads) center_kernel(CenterArgs a) {
 // Splits the vertices into the six center classes (1 <= degree <= 1024;
 // class c holds degrees in (16 * 2^c, 32 * 2^c], class 0 from 1) and marks
 // the larger ones: big_deg[v] = degree if above kCenterMaxDeg, else 0.
-__global__ void center_classes_kernel(const int64_t *__restrict__ rp, int64_t n,
-                                      int32_t *__restrict__ lists, int32_t *__restrict__ counts,
+__global__ void center_classes_kernel(const int64_t *__restrict__ rp, int64_t n, int shard,
+                                      int num_shards, int32_t *__restrict__ lists,
+                                      int32_t *__restrict__ counts,
                                       int32_t *__restrict__ big_deg) {
   __shared__ int h[kCenterClasses], base[kCenterClasses];
   if (threadIdx.x < kCenterClasses) h[threadIdx.x] = 0;
@@ -745,7 +751,9 @@ __global__ void center_classes_kernel(const int64_t *__restrict__ rp, int64_t n,
   if (v < n) {
     const int d = (int)(rp[v + 1] - rp[v]);
     big_deg[v] = d > kCenterMaxDeg ? d : 0;
-    if (d >= 1 && d <= kCenterMaxDeg) {
+    // A shard keeps the centers v = shard (mod num_shards); the large
+    // centers' edge tasks are split by pattern_kernel itself.
+    if (d >= 1 && d <= kCenterMaxDeg && v % num_shards == shard) {
       cls = 0;
       while (32 * center_words(cls) < d) ++cls;
       slot = atomicAdd(&h[cls], 1);
@@ -933,8 +941,8 @@ int center_path(mc_dgraph *g, int pattern, PatArgs a, int grid) {
   void *temp = reinterpret_cast<char *>(big_off) + up(off_b);
 
   MC_CUDA_TRY(cudaMemsetAsync(words, 0, words_b, s));
-  center_classes_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g->rowptr, n, lists, counts,
-                                                                   big_deg);
+  center_classes_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
+      g->rowptr, n, a.shard, a.num_shards, lists, counts, big_deg);
   MC_CUDA_TRY(cudaGetLastError());
   MC_CUDA_TRY(exclusive_scan(big_deg, big_off, n, temp, s));
   g->launches += 1 + scan_launches(n);
@@ -984,7 +992,8 @@ int center_path(mc_dgraph *g, int pattern, PatArgs a, int grid) {
 
 }  // namespace
 
-int pattern_count(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12, mc_timing_t *timing) {
+int pattern_count(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12, mc_timing_t *timing,
+                  int shard, int num_shards) {
   cudaStream_t s = g->stream;
   const int64_t launches_before = g->launches;
   MC_CUDA_TRY(cudaMemsetAsync(g->counters, 0, sizeof(unsigned long long) * 8, s));
@@ -1002,6 +1011,8 @@ int pattern_count(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12, mc_ti
   }
   PatArgs a{g->rowptr, g->col, g->n, g->nnz, static_cast<int32_t *>(g->pat_scratch), cap,
             g->counters + 0, g->counters + 2};
+  a.shard = shard;
+  a.num_shards = num_shards;
   MC_CUDA_TRY(cudaEventRecord(g->ev[0], s));
   int rc = MC_OK;
   if (g->n > 0 && g->nnz > 0) {
@@ -1058,9 +1069,15 @@ int pattern_count(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12, mc_ti
 }  // namespace mc
 
 extern "C" int mc_pattern_count(mc_dgraph_t *g, int pattern, uint64_t *count, mc_timing_t *timing) {
-  if (!g || !count || pattern < 1 || pattern > 8) return MC_ERR_ARG;
+  return mc_pattern_count_shard(g, pattern, 0, 1, count, timing);
+}
+
+extern "C" int mc_pattern_count_shard(mc_dgraph_t *g, int pattern, int shard, int num_shards,
+                                      uint64_t *partial, mc_timing_t *timing) {
+  if (!g || !partial || pattern < 1 || pattern > 8) return MC_ERR_ARG;
+  if (num_shards < 1 || shard < 0 || shard >= num_shards) return MC_ERR_ARG;
   MC_CUDA_TRY(cudaSetDevice(g->device));
-  return mc::pattern_count(g, pattern, count, nullptr, timing);
+  return mc::pattern_count(g, pattern, partial, nullptr, timing, shard, num_shards);
 }
 
 // ---- pattern count without allocation --------------------------------------

@@ -1,10 +1,10 @@
 // Triangle-count kernels.  count = sum over DAG edges {x, y} of
 // |N+(x) & N+(y)|, where x is the edge's owner (larger d+, ties to the larger
 // id) and y its partner.  A task is (owner, chunk of the owner's symmetric
-// row): N+(owner) goes into a shared-memory cuckoo table, the chunk's
-// neighbours are filtered down to partners (owner rule on d+), and each
-// partner's list N+(y) -- never longer than N+(owner) -- is streamed through
-// the table.
+// row): N+(owner) goes into shared memory (a degree-rank bitmap or a cuckoo
+// table), the chunk's neighbours are filtered down to partners (owner rule
+// on d+), and each partner's list N+(y) -- never longer than N+(owner) -- is
+// streamed through it.
 //
 // Reference counterparts: hashIndex_for_large_degree (CTA per large vertex,
 // 1019-bin hash staged through a 256 MiB global scratch, bin scanned
@@ -13,7 +13,8 @@
 // shared memory, gpu_kernels/tc_challenge.cuh:195-303), each with an atomic
 // work counter (DYNAMIC_MODE, gpu_kernels/tuning_schedules.cuh:1-21).  Here
 // the queues hold bounded (owner, row-chunk) tasks, the tables live in shared
-// memory only, and a probe is two fixed table reads with no branch.
+// memory only, and a probe is one bitmap word or two fixed table reads with
+// no branch.
 #include <algorithm>
 #include <climits>
 
@@ -23,7 +24,6 @@
 namespace mc {
 namespace {
 
-constexpr int kClaim = 32;     // owner-row entries a hub warp claims at a time
 constexpr int kMaxKicks = 64;  // cuckoo displacements allowed per inserted key
 constexpr int kNoKey = INT_MIN;  // probe value that matches no slot
 
@@ -154,82 +154,161 @@ __device__ __forceinline__ bool owns(int x, int px, int y, int py) {
   return py >= 1 && (px > py || (px == py && x > y));
 }
 
-// One warp streams one list col[st, st+len) through `probe` with 16-byte
-// loads: lane l takes int4 groups l, l+32, ... of the aligned body, two
-// groups in flight; the at most 3 + 3 entries before the first and after
-// the last 16-byte boundary are probed by lanes 0-2 and 4-6. Returns this
-// lane's hits.
+// Partner lists at least this long are streamed by one warp each; shorter
+// ones are concatenated and streamed flat by the whole CTA.
+constexpr int kLongList = 64;
+
+// Partners of one hub task, compacted in row order.  Thread t examines
+// neighbours 2t and 2t+1 of the chunk; one block scan of (long partners,
+// short partners, short list lengths) packed in 64 bits places every
+// partner.  Long list j (j < nl): start base[j], length off[j].  Short list
+// j: elements [off[nl+j], off[nl+j+1]) of the short stream, element f of it
+// at lists[base[nl+j] + f] (base = list start - offset).  Returns nl and the
+// short stream length.
+struct Partners {
+  int nl;     // long lists
+  int total;  // elements of the short stream
+};
+
+__device__ __forceinline__ Partners find_partners(const CountArgs &a, int x, int px, int64_t e0,
+                                                  int nc, long long *s_base, int *s_off,
+                                                  unsigned long long *s_warp) {
+  static_assert(kHubChunk == 2 * kCountThreads, "two neighbours per thread");
+  constexpr int kWarps = kCountThreads / kWarp;
+  const int lane = threadIdx.x & (kWarp - 1), warp = threadIdx.x / kWarp;
+  int len[2] = {0, 0};
+  long long st[2] = {0, 0};
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int i = 2 * threadIdx.x + r;
+    if (i < nc) {
+      const int y = __ldg(a.col + e0 + i);
+      const int py = __ldg(&a.key[y].y);
+      if (owns(x, px, y, py)) {
+        len[r] = py;
+        st[r] = __ldg(a.dag_rowptr + y);
+      }
+    }
+  }
+  unsigned long long mine = 0;
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    if (len[r] >= kLongList) mine += 1ull << 48;
+    else if (len[r] > 0) mine += (1ull << 32) + (unsigned)len[r];
+  }
+  unsigned long long incl = mine;
+#pragma unroll
+  for (int o = 1; o < kWarp; o <<= 1) {
+    const unsigned long long v = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == kWarp - 1) s_warp[warp] = incl;
+  __syncthreads();
+  unsigned long long before = 0, all = 0;
+#pragma unroll
+  for (int w = 0; w < kWarps; ++w) {
+    const unsigned long long v = s_warp[w];
+    if (w < warp) before += v;
+    all += v;
+  }
+  const unsigned long long excl = before + incl - mine;
+  const int nl = (int)(all >> 48), ns = (int)((all >> 32) & 0xffff);
+  int lslot = (int)(excl >> 48);
+  int sslot = nl + (int)((excl >> 32) & 0xffff), off = (int)(unsigned)excl;
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    if (len[r] >= kLongList) {
+      s_base[lslot] = st[r];
+      s_off[lslot] = len[r];
+      ++lslot;
+    } else if (len[r] > 0) {
+      s_base[sslot] = st[r] - off;
+      s_off[sslot] = off;
+      ++sslot;
+      off += len[r];
+    }
+  }
+  const int total = (int)(unsigned)all;
+  if (threadIdx.x == 0) s_off[nl + ns] = total;
+  __syncthreads();
+  return Partners{nl, total};
+}
+
+// One warp streams one list lists[st, st + len) with lane-per-element loads
+// (128 bytes per instruction): every load of a 256-element batch is issued
+// before the first probe, so a list of up to 256 entries costs one memory
+// latency; 32-element groups past the end are skipped whole.
 template <class Probe>
-__device__ __forceinline__ unsigned stream_list4(const int32_t *__restrict__ col, int64_t st,
-                                                 int len, int lane, const Probe &probe) {
+__device__ __forceinline__ unsigned stream_one(const int32_t *__restrict__ lists, long long st,
+                                               int len, int lane, const Probe &probe) {
+  constexpr int kB = 8;
+  const int32_t *p = lists + st;
+  unsigned h = 0;
+  for (int base = 0; base < len; base += kB * kWarp) {
+    int w[kB];
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      const int k = base + u * kWarp + lane;
+      w[u] = k < len ? __ldg(p + k) : kNoKey;
+    }
+#pragma unroll
+    for (int u = 0; u < kB; ++u)
+      if (base + u * kWarp < len) h += probe(w[u]);
+  }
+  return h;
+}
+
+// The short stream: warp w takes windows of 32 x kU consecutive elements
+// (w, w + 8, ...), lane l element window + 32u + l, so every load
+// instruction reads one 128-byte span and every lane has kU loads in
+// flight.  An element's list is found by walking forward from the window's
+// first list (lists are at least one element long).
+template <class Probe>
+__device__ __forceinline__ unsigned stream_short(const int32_t *__restrict__ lists,
+                                                 const long long *s_base, const int *s_off,
+                                                 int total, int warp, int lane,
+                                                 const Probe &probe) {
+  constexpr int kU = 4;
+  constexpr int kWarps = kCountThreads / kWarp;
   unsigned hits = 0;
-  const int head = min(len, (int)((4 - (st & 3)) & 3));
-  const int body = (len - head) >> 2;
-  const int tail = len - head - 4 * body;
-  if (head + tail > 0) {
-    int w = kNoKey;
-    if (lane < head) w = __ldg(col + st + lane);
-    else if (lane >= 4 && lane < 4 + tail) w = __ldg(col + st + head + 4 * body + (lane - 4));
-    hits += probe(w);
-  }
-  const int4 *v = reinterpret_cast<const int4 *>(col + st + head);
-  int k = lane;
-  for (; k + kWarp < body; k += 2 * kWarp) {
-    const int4 p = __ldg(v + k), q = __ldg(v + k + kWarp);
-    hits += probe(p.x) + probe(p.y) + probe(p.z) + probe(p.w);
-    hits += probe(q.x) + probe(q.y) + probe(q.z) + probe(q.w);
-  }
-  if (k < body) {
-    const int4 p = __ldg(v + k);
-    hits += probe(p.x) + probe(p.y) + probe(p.z) + probe(p.w);
+  int j = 0;  // list holding the warp's window start (the same on every lane)
+  for (int wb = warp * kWarp * kU; wb < total; wb += kWarps * kWarp * kU) {
+    while (s_off[j + 1] <= wb) ++j;
+    int w[kU];
+    int jj = j;
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const int f = wb + u * kWarp + lane;
+      w[u] = kNoKey;
+      if (f < total) {
+        while (s_off[jj + 1] <= f) ++jj;
+        w[u] = __ldg(lists + s_base[jj] + f);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kU; ++u) hits += probe(w[u]);
   }
   return hits;
 }
 
-// Entries [e0, e0 + nc) of owner x's symmetric row, claimed by the CTA's warps
-// from the shared counter *next (kClaim at a time, smaller claims as the
-// chunk runs out); each claimed neighbour that is a partner has its list
-// streamed by the whole warp.
+// All partner lists of the task: the long ones claimed a list at a time by
+// the warps, then the short stream.  Returns this thread's hits.
 template <class Probe>
-__device__ __forceinline__ unsigned long long claim_and_stream(const CountArgs &a, int x, int px,
-                                                               int64_t e0, int nc, int *next,
-                                                               int lane, const Probe &probe,
-                                                               const int32_t *__restrict__ lists) {
+__device__ __forceinline__ unsigned long long stream_partners(const int32_t *__restrict__ lists,
+                                                              const long long *s_base,
+                                                              const int *s_off, Partners pt,
+                                                              int *s_next, int warp, int lane,
+                                                              const Probe &probe) {
   unsigned long long hits = 0;
   for (;;) {
-    int g = 0;
-    if (lane == 0) {
-      const int seen = *(volatile int *)next;
-      const int size = max(1, min(kClaim, (nc - seen) / 16));
-      g = atomicAdd(next, size) | (size << 20);
-    }
-    g = __shfl_sync(kFull, g, 0);
-    const int size = g >> 20;
-    g &= (1 << 20) - 1;
-    if (g >= nc) break;
-    bool part = false;
-    int64_t st = 0;
-    int len = 0;
-    if (lane < size && g + lane < nc) {
-      const int y = __ldg(a.col + e0 + g + lane);
-      const int py = __ldg(&a.key[y].y);
-      if (owns(x, px, y, py)) {
-        part = true;
-        st = __ldg(a.dag_rowptr + y);
-        len = py;
-      }
-    }
-    unsigned m = __ballot_sync(kFull, part);
-    unsigned h = 0;
-    while (m) {
-      const int p = __ffs(m) - 1;
-      m &= m - 1;
-      const int64_t s = __shfl_sync(kFull, st, p);
-      const int l = __shfl_sync(kFull, len, p);
-      h += stream_list4(lists, s, l, lane, probe);
-    }
-    hits += h;
+    int j = 0;
+    if (lane == 0) j = atomicAdd(s_next, 1);
+    j = __shfl_sync(kFull, j, 0);
+    if (j >= pt.nl) break;
+    hits += stream_one(lists, s_base[j], s_off[j], lane, probe);
   }
+  if (pt.total > 0)
+    hits += stream_short(lists, s_base + pt.nl, s_off + pt.nl, pt.total, warp, lane, probe);
   return hits;
 }
 
@@ -262,25 +341,28 @@ __device__ __forceinline__ unsigned long long stream_flat(const int32_t *__restr
 
 __device__ __forceinline__ int ceil_log2(int v) { return v <= 1 ? 0 : 32 - __clz(v - 1); }
 
-// One CTA per hub task: N+(owner) into shared memory, then the 8 warps claim
-// the row chunk and stream each partner's list through it.  N+(owner) is
-// kept as a bitmap over ranks [0, rank(owner)) when that fits the launch's
-// shared memory (lists streamed as ranks), else as a cuckoo table of 2^lg
-// slots (load <= 1/4 when it fits, <= 1/2 at the size cap).  Owners beyond
-// the cap, or whose table could not be built, are probed by binary search in
-// global memory instead.
+// One CTA per hub task: N+(owner) into shared memory; the chunk's partners
+// are found in one pass and compacted; then the whole CTA streams their
+// concatenated lists through it.  N+(owner) is kept as a bitmap over ranks
+// [0, rank(owner)) when that fits the launch's shared memory (lists streamed
+// as ranks), else as a cuckoo table of 2^lg slots (load <= 1/4 when it fits,
+// <= 1/2 at the size cap).  Owners beyond the cap, or whose table could not
+// be built, are probed by binary search in global memory instead.
 __global__ void __launch_bounds__(kCountThreads, 5) tc_hub_kernel(CountArgs a) {
   extern __shared__ int table[];
   __shared__ unsigned long long s_task;
-  __shared__ int s_next, s_fail;
-  const int lane = threadIdx.x & (kWarp - 1);
+  __shared__ int s_fail, s_next;
+  __shared__ long long s_base[kHubChunk];
+  __shared__ int s_off[kHubChunk + 1];
+  __shared__ unsigned long long s_warp[kCountThreads / kWarp];
+  const int lane = threadIdx.x & (kWarp - 1), warp = threadIdx.x / kWarp;
   const int64_t ntasks = shard_tasks(a);
   unsigned long long hits = 0;
   for (;;) {
     if (threadIdx.x == 0) {
       s_task = atomicAdd(a.queue, 1ull);
-      s_next = 0;
       s_fail = 0;
+      s_next = 0;
     }
     __syncthreads();
     const unsigned long long t = s_task;
@@ -293,50 +375,48 @@ __global__ void __launch_bounds__(kCountThreads, 5) tc_hub_kernel(CountArgs a) {
     const int64_t e0 = a.rowptr[x] + (int64_t)chunk * kHubChunk;
     const int nc = (int)min((int64_t)kHubChunk, a.rowptr[x + 1] - e0);
     const int R = a.rank ? __ldg(a.rank + x) : INT_MAX;
-    unsigned long long th = 0;
-    if (R <= a.bitmap_bits) {
-      unsigned *bits = reinterpret_cast<unsigned *>(table);
-      int4 *t4 = reinterpret_cast<int4 *>(table);
+    const bool bitmap = R <= a.bitmap_bits;
+    int lg = max(8, ceil_log2(d << table_factor_log2(a, x)));
+    if (lg > a.table_log2_max && 2 * d <= (1 << a.table_log2_max)) lg = a.table_log2_max;
+    bool use_table = !bitmap && lg <= a.table_log2_max;
+    const int shift = 32 - lg;
+    // Clear the bitmap / table, then find the partners (their loads overlap).
+    int4 *t4 = reinterpret_cast<int4 *>(table);
+    if (bitmap) {
       for (int i = threadIdx.x; i < (R + 127) >> 7; i += blockDim.x) t4[i] = make_int4(0, 0, 0, 0);
-      __syncthreads();
+    } else if (use_table) {
+      for (int i = threadIdx.x; i < (1 << lg) / 4; i += blockDim.x) t4[i] = make_int4(-1, -1, -1, -1);
+    }
+    const Partners pt = find_partners(a, x, d, e0, nc, s_base, s_off, s_warp);
+    // N+(x) into shared memory.
+    if (bitmap) {
+      unsigned *bits = reinterpret_cast<unsigned *>(table);
       for (int i = threadIdx.x; i < d; i += blockDim.x) {
         const unsigned r = (unsigned)__ldg(a.dag_rank + a0 + i);
         if (r < (unsigned)R) atomicOr(bits + (r >> 5), 1u << (r & 31));
         else atomicOr(a.err, kErrRank);  // never written outside the bitmap
       }
-      __syncthreads();
-      th = claim_and_stream(a, x, d, e0, nc, &s_next, lane, BitmapProbe{bits, (unsigned)R},
-                            a.dag_rank);
-      hits += th;
-      flush_task(a, x, th, lane);
-      __syncthreads();  // the bitmap and the shared words are rewritten by the next task
-      continue;
-    }
-    int lg = max(8, ceil_log2(d << table_factor_log2(a, x)));
-    if (lg > a.table_log2_max && 2 * d <= (1 << a.table_log2_max)) lg = a.table_log2_max;
-    bool use_table = lg <= a.table_log2_max;
-    if (use_table) {
-      const int size = 1 << lg;
-      const int shift = 32 - lg;
-      int4 *t4 = reinterpret_cast<int4 *>(table);
-      for (int i = threadIdx.x; i < size / 4; i += blockDim.x) t4[i] = make_int4(-1, -1, -1, -1);
-      __syncthreads();
+    } else if (use_table) {
       bool ok = true;
       for (int i = threadIdx.x; i < d; i += blockDim.x)
         ok &= cuckoo_insert(table, shift, __ldg(a.dag_col + a0 + i));
       if (!ok) s_fail = 1;
-      __syncthreads();
-      use_table = s_fail == 0;
-      if (use_table)
-        th = claim_and_stream(a, x, d, e0, nc, &s_next, lane, CuckooProbe{table, shift},
-                              a.dag_col);
     }
-    if (!use_table)
-      th = claim_and_stream(a, x, d, e0, nc, &s_next, lane, ListProbe{a.dag_col + a0, d},
-                            a.dag_col);
+    __syncthreads();
+    use_table = use_table && s_fail == 0;
+    unsigned long long th = 0;
+    if (bitmap)
+      th = stream_partners(a.dag_rank, s_base, s_off, pt, &s_next, warp, lane,
+                           BitmapProbe{reinterpret_cast<const unsigned *>(table), (unsigned)R});
+    else if (use_table)
+      th = stream_partners(a.dag_col, s_base, s_off, pt, &s_next, warp, lane,
+                           CuckooProbe{table, shift});
+    else
+      th = stream_partners(a.dag_col, s_base, s_off, pt, &s_next, warp, lane,
+                           ListProbe{a.dag_col + a0, d});
     hits += th;
     flush_task(a, x, th, lane);
-    __syncthreads();  // table and the shared words are rewritten by the next task
+    __syncthreads();  // shared memory is rewritten by the next task
   }
   hits = warp_sum_u64(hits);
   if (lane == 0 && hits) atomicAdd(a.result, hits);

@@ -196,6 +196,14 @@ class DeviceGraph:
               f"pattern P{k}")
         return out.value
 
+    def pattern_count_shard(self, pattern, shard: int, num_shards: int) -> int:
+        """Partial count of one shard (partials of all shards sum to the count mod 2^64)."""
+        k = int(str(pattern).upper().lstrip("P"))
+        out = C.c_uint64()
+        check(lib().mc_pattern_count_shard(self._h, k, shard, num_shards, C.byref(out),
+                                           C.byref(self.last_timing)), f"pattern P{k} shard")
+        return out.value
+
     def tc_stats(self) -> dict:
         st = TcStats()
         check(lib().mc_tc_stats(self._h, C.byref(st)), "tc stats")

@@ -135,3 +135,21 @@ def test_cli_sm_prints_reference_lines():
     out = subprocess.run([exe, prefix, "P4"], capture_output=True, text=True, check=True).stdout
     assert "Total runtime  = " in out
     assert f"total_num_triangles = {GOLD['rmat8']['P4']}" in out
+
+
+@pytest.mark.parametrize("route", ["default", "centers", "edge"])
+@pytest.mark.parametrize("shards", [2, 3])
+def test_pattern_shards_sum_to_the_count(monkeypatch, route, shards):
+    """mc_pattern_count_shard: the partial counts of all shards (centers by
+    id, remaining edge and star tasks round-robin) sum to the count mod 2^64,
+    on every route, including the large centers of the warp-per-edge kernel."""
+    if route != "default":
+        monkeypatch.setenv("MERCURY_PATTERN_KERNEL", route)
+    rp, col = center_class_graph()
+    with DeviceGraph(rp, col) as d:
+        for k in range(1, 9):
+            full = d.pattern_count(k)
+            parts = [d.pattern_count_shard(k, s, shards) for s in range(shards)]
+            assert sum(parts) % (1 << 64) == full, k
+        with pytest.raises(Exception):
+            d.pattern_count_shard(1, shards, shards)

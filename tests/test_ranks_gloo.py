@@ -49,6 +49,27 @@ def test_two_ranks_sum_counts_and_take_max_time():
     assert all(r[4] == max(times) for r in res)
 
 
+def test_two_ranks_sum_wrapping_pattern_partials():
+    """Pattern partials are c1 - c2 of per-shard sums: a shard's value can
+    wrap below zero (mod 2^64); the combined count is their sum mod 2^64."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    full = 123_456_789
+    partials = [(full + 5 - (1 << 40)) % (1 << 64), ((1 << 40) - 5) % (1 << 64)]
+    partials[1] = (full - partials[0]) % (1 << 64)
+    assert partials[0] >= (1 << 63) or partials[1] >= (1 << 63)
+    times = [3.0, 2.0]
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, partials, times, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert all(r[3] == full for r in res)
+
+
 def test_shard_of_rejects_bad_rank():
     import sys
     sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
