@@ -17,8 +17,24 @@ __device__ __forceinline__ unsigned digit_of(u64 key, int shift) {
   return (unsigned)(key >> shift) & (kRadixBins - 1);
 }
 
-// Upsweep: the digit histogram of every tile, stored as counts[d * tiles + t]
-// so that one exclusive scan orders the runs digit-major, tile-minor.
+// Lanes of the warp holding a real key with the same digit as this lane: the
+// intersection over the digit's 8 bits of each bit's ballot (or its
+// complement), restricted to the lanes with a key.  The same set that
+// __match_any_sync returns, from plain votes.
+__device__ __forceinline__ unsigned digit_peers(unsigned d, bool ok) {
+  unsigned peers = __ballot_sync(kFull, ok);
+#pragma unroll
+  for (int b = 0; b < kRadixBits; ++b) {
+    const unsigned bit = (d >> b) & 1u;
+    const unsigned m = __ballot_sync(kFull, bit);
+    peers &= bit ? m : ~m;
+  }
+  return peers;
+}
+
+// Upsweep: the digit histogram of every tile (shared-memory atomics into a
+// per-warp row), stored as counts[d * tiles + t] so that one exclusive scan
+// orders the runs digit-major, tile-minor.
 __global__ void __launch_bounds__(kSortThreads) radix_count_kernel(const u64 *__restrict__ keys,
                                                                    int64_t count, int shift,
                                                                    int64_t tiles,
@@ -31,15 +47,8 @@ __global__ void __launch_bounds__(kSortThreads) radix_count_kernel(const u64 *__
   u64 k[kSortRounds];
   load_warp_keys(keys, count, first, k);
 #pragma unroll
-  for (int r = 0; r < kSortRounds; ++r) {
-    const bool ok = first + r * kWarp < count;
-    const unsigned d = ok ? digit_of(k[r], shift) : kRadixBins;  // kRadixBins: no key
-    const unsigned peers = __match_any_sync(kFull, d);
-    // One leader per distinct digit adds the group's size: no two lanes of
-    // the warp write the same counter, and each warp owns its own row.
-    if (ok && lane == __ffs(peers) - 1) hist[w][d] += __popc(peers);
-    __syncwarp();
-  }
+  for (int r = 0; r < kSortRounds; ++r)
+    if (first + r * kWarp < count) atomicAdd(&hist[w][digit_of(k[r], shift)], 1);
   __syncthreads();
   int s = 0;
 #pragma unroll
@@ -50,7 +59,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_count_kernel(const u64 *__
 // Downsweep: ranks every key of the tile stably by digit (warp order, then
 // round, then lane = input order), stages the tile in shared memory in digit
 // order, then stores each digit's run to its slot range.
-__global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(
+__global__ void __launch_bounds__(kSortThreads, 3) radix_scatter_kernel(
     const u64 *__restrict__ keys_in, u64 *__restrict__ keys_out, int64_t count, int shift,
     int64_t tiles, const int64_t *__restrict__ offsets) {
   __shared__ int hist[kSortWarps][kRadixBins];  // running counts, then warp prefixes
@@ -70,8 +79,8 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(
 #pragma unroll
   for (int r = 0; r < kSortRounds; ++r) {
     const bool ok = first + r * kWarp < count;
-    const unsigned d = ok ? digit_of(k[r], shift) : kRadixBins;
-    const unsigned peers = __match_any_sync(kFull, d);
+    const unsigned d = ok ? digit_of(k[r], shift) : 0u;
+    const unsigned peers = digit_peers(d, ok);
     const int before = ok ? hist[w][d] : 0;
     __syncwarp();
     if (ok && lane == __ffs(peers) - 1) hist[w][d] = before + __popc(peers);
