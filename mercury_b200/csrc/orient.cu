@@ -365,15 +365,17 @@ __global__ void task_fill_kernel(const int32_t *hub_cnt, const int64_t *hub_off,
   for (int32_t c = 0, m = mega_cnt[v]; c < m; ++c) mega_tasks[mega_off[v] + c] = hi | (uint32_t)c;
 }
 
-// Partner edges (owner rule) and their streamed-list work, for statistics.
+// Partner edges (owner rule) and their streamed-list work, for statistics:
+// one warp per row, lanes over its entries.
 __global__ void partner_stats_kernel(const int64_t *rowptr, const int32_t *col, const int2 *key,
                                      int64_t n, unsigned long long *out) {
   unsigned long long pe = 0, work = 0;
-  for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n;
-       x += (int64_t)gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int64_t warps = (int64_t)gridDim.x * blockDim.x / kWarp;
+  for (int64_t x = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; x < n; x += warps) {
     const int px = key[x].y;
     if (px < 1) continue;
-    for (int64_t e = rowptr[x]; e < rowptr[x + 1]; ++e) {
+    for (int64_t e = rowptr[x] + lane; e < rowptr[x + 1]; e += kWarp) {
       const int y = col[e];
       const int py = key[y].y;
       if (py >= 1 && (px > py || (px == py && (int)x > y))) {
