@@ -167,7 +167,8 @@ __device__ __forceinline__ void write_span(const TileRows &tr, const int64_t *ro
 template <bool kWrite>
 __global__ void __launch_bounds__(kTileThreads)
     dag_pass_kernel(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ col,
-                    int64_t n, int64_t nnz, int2 *key, uint16_t *keep_masks, int32_t *counts_out,
+                    const int32_t *__restrict__ deg, int64_t n, int64_t nnz, int2 *key,
+                    uint16_t *keep_masks, int32_t *counts_out,
                     const int64_t *__restrict__ offs_in, int64_t *out_rowptr, int32_t *out_col,
                     const int32_t *__restrict__ rank, int32_t *out_rank) {
   __shared__ int64_t seg[kSegMax];
@@ -185,7 +186,7 @@ __global__ void __launch_bounds__(kTileThreads)
     r = tr.row_of(s);
     if (!kWrite) {
       int64_t v = r, next = tr.at(r + 1);
-      int dv = key[v].x;
+      int dv = __ldg(deg + v);
       int run = 0;  // DAG entries of row v seen in this span
 #pragma unroll
       for (int k = 0; k < kEdgesPerThread; ++k) {
@@ -198,10 +199,10 @@ __global__ void __launch_bounds__(kTileThreads)
             }
             ++v;
             next = tr.at(v + 1);
-            dv = key[v].x;
+            dv = __ldg(deg + v);
           }
           const int u = vals[k];
-          const int du = key[u].x;
+          const int du = __ldg(deg + u);
           if (du > dv || (du == dv && u > (int)v)) {
             keep |= 1u << k;
             ++run;
@@ -314,9 +315,14 @@ __global__ void rank_scatter_kernel(const unsigned long long *__restrict__ sorte
   if (p < n) rank[n - 1 - (int64_t)(uint32_t)sorted[p]] = (int32_t)p;
 }
 
-__global__ void init_key_kernel(const int64_t *rowptr, int64_t n, int2 *key) {
+// key[v] = {degree, 0}; deg[v] = degree alone (4 bytes per gather in pass A).
+__global__ void init_key_kernel(const int64_t *rowptr, int64_t n, int2 *key, int32_t *deg) {
   const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (v < n) key[v] = make_int2((int)(rowptr[v + 1] - rowptr[v]), 0);
+  if (v < n) {
+    const int d = (int)(rowptr[v + 1] - rowptr[v]);
+    key[v] = make_int2(d, 0);
+    deg[v] = d;
+  }
 }
 
 // Tasks each owner contributes to the hub, large-table hub and leaf queues
@@ -491,7 +497,10 @@ int tc_orient(mc_dgraph *g) {
   MC_CUDA_TRY(cudaMemsetAsync(g->counters, 0, sizeof(unsigned long long) * 7, s));
   if (n == 0) return MC_OK;
   const int64_t tiles = (nnz + kTileEdges - 1) / kTileEdges;
-  init_key_kernel<<<grid_for(n, 256), 256, 0, s>>>(g->rowptr, n, g->key);
+  // The degrees alone, for pass A's gathers, in mega_cnt (unused until the
+  // task counts are written after pass B).
+  int32_t *deg = g->mega_cnt;
+  init_key_kernel<<<grid_for(n, 256), 256, 0, s>>>(g->rowptr, n, g->key, deg);
   MC_CUDA_TRY(cudaGetLastError());
   g->launches += 1;
   if (g->rank && !g->batch.gid) {
@@ -510,12 +519,12 @@ int tc_orient(mc_dgraph *g) {
     MC_CUDA_TRY(cudaMemsetAsync(g->dag_rowptr, 0, sizeof(int64_t) * (n + 1), s));
   } else {
     const unsigned grid = (unsigned)tiles;
-    dag_pass_kernel<false><<<grid, kTileThreads, 0, s>>>(g->rowptr, g->col, n, nnz, g->key,
+    dag_pass_kernel<false><<<grid, kTileThreads, 0, s>>>(g->rowptr, g->col, deg, n, nnz, g->key,
                                                          g->keep, g->tile_counts, nullptr,
                                                          nullptr, nullptr, nullptr, nullptr);
     MC_CUDA_TRY(cudaGetLastError());
     MC_CUDA_TRY(exclusive_scan(g->tile_counts, g->tile_offsets, tiles, g->scan_temp, s));
-    dag_pass_kernel<true><<<grid, kTileThreads, 0, s>>>(g->rowptr, g->col, n, nnz, g->key,
+    dag_pass_kernel<true><<<grid, kTileThreads, 0, s>>>(g->rowptr, g->col, deg, n, nnz, g->key,
                                                         g->keep, nullptr, g->tile_offsets,
                                                         g->dag_rowptr, g->dag_col,
                                                         g->batch.gid ? nullptr : g->rank,
