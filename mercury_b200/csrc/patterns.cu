@@ -402,9 +402,15 @@ __host__ __device__ constexpr bool center_outer(int P) {
 // Shared memory of one group: M (32W rows of W words), N0 (32W ints) and,
 // for the outer patterns, per warp one R row per lane (32 x W words) and a
 // counter per N0 position (32W ints).
+// (Per warp, the outer patterns keep 32 R rows, 32W counters and 32 vertex
+// slots.)  Outer patterns with rows of 4+ words also keep a position hash of N0
+// (64W slots: keys, then positions), so that R(y) looks each neighbour of y
+// up in about one read instead of a binary search.
+__host__ __device__ constexpr bool center_hash(int P, int W) { return center_outer(P) && W >= 4; }
 __host__ __device__ constexpr size_t center_group_bytes(int P, int W) {
   return sizeof(unsigned) * ((size_t)(32 * W) * W + (size_t)(32 * W) +
-                             (center_outer(P) ? (size_t)center_group(W) * (64 * W) : 0));
+                             (center_outer(P) ? (size_t)center_group(W) * (64 * W + 32) : 0) +
+                             (center_hash(P, W) ? (size_t)(128 * W) : 0));
 }
 
 struct CenterArgs {
@@ -446,14 +452,39 @@ __device__ __forceinline__ int find_pos(const int32_t *n0, int d0, int y) {
   return -1;
 }
 
+// Where y sits in N0 (-1: absent): the group's position hash when it has
+// one (linear probing, load <= 1/2, so an empty slot ends every probe),
+// else a binary search of n0.
+struct PosIndex {
+  const int32_t *n0;
+  int d0;
+  const int *hkeys;  // null: no hash
+  const int *hpos;
+  int lg;
+  __device__ __forceinline__ int find(int y) const {
+    if (!hkeys) return find_pos(n0, d0, y);
+    const unsigned mask = (1u << lg) - 1u;
+    unsigned h = ((unsigned)y * 2654435769u) >> (32 - lg);
+    for (int step = 0; step <= (int)mask; ++step) {
+      const int k = hkeys[h];
+      if (k == y) return hpos[h];
+      if (k < 0) return -1;
+      h = (h + 1u) & mask;
+    }
+    return -1;
+  }
+};
+
 // Row of x over N0: bit j set iff N0[j] in N(x).  One lane owns the row (no
 // other lane writes it).  The cheapest of three walks is taken: each
 // neighbour of x searched in N0 (shared memory), each N0[j] searched in N(x)
 // (global), or a merge of the two sorted lists.
 template <int W>
 __device__ __forceinline__ void build_row(const int64_t *__restrict__ rp,
-                                          const int32_t *__restrict__ ci, const int32_t *n0,
-                                          int d0, int x, unsigned *row) {
+                                          const int32_t *__restrict__ ci, const PosIndex &idx,
+                                          int x, unsigned *row) {
+  const int32_t *n0 = idx.n0;
+  const int d0 = idx.d0;
 #pragma unroll
   for (int k = 0; k < W; ++k) row[k] = 0;
   const int64_t b = __ldg(rp + x), e = __ldg(rp + x + 1);
@@ -463,7 +494,7 @@ __device__ __forceinline__ void build_row(const int64_t *__restrict__ rp,
   const int merge = dx + d0;
   if (by_x <= by_n0 && by_x <= merge) {
     for (int64_t t = b; t < e; ++t) {
-      const int j = find_pos(n0, d0, __ldg(ci + t));
+      const int j = idx.find(__ldg(ci + t));
       if (j >= 0) row[j >> 5] |= 1u << (j & 31);
     }
   } else if (by_n0 <= merge) {
@@ -569,9 +600,13 @@ __device__ __forceinline__ void center_edges(const unsigned *M, int d0, int wg, 
 template <int P, int W>
 __device__ __forceinline__ void center_outer_edges(const int64_t *__restrict__ rp,
                                                    const int32_t *__restrict__ ci,
-                                                   const unsigned *M, const int32_t *n0, int d0,
+                                                   const unsigned *M, const PosIndex &idx,
                                                    int v0, int wg, int G, int lane,
-                                                   unsigned *Rl, int *cnt, Acc &acc) {
+                                                   unsigned *Rw, int *cnt, int *slots, Acc &acc) {
+  const int32_t *n0 = idx.n0;
+  const int d0 = idx.d0;
+  unsigned *Rl = Rw + lane * W;
+  const unsigned upto = lane == kWarp - 1 ? kFull : ((2u << lane) - 1u);
   for (int p = wg; p < d0; p += G) {
     const int v1 = n0[p];
     if (P == 4 && !(v1 < v0)) continue;
@@ -593,10 +628,52 @@ __device__ __forceinline__ void center_outer_edges(const int64_t *__restrict__ r
     }
     const int64_t b1 = __ldg(rp + v1);
     const int d1 = (int)(__ldg(rp + v1 + 1) - b1);
-    for (int j = lane; j < d1; j += kWarp) {
-      const int y = __ldg(ci + b1 + j);
-      if (y == v0 || find_pos(n0, d0, y) >= 0) continue;
-      build_row<W>(rp, ci, n0, d0, y, Rl);
+    // N1 in chunks of 32: the outer neighbours y of a chunk are compacted
+    // into lanes 0..nu-1, their rows R(y) built by a flat walk of their
+    // concatenated lists (every lane one entry per step, entry -> owner lane
+    // by counting the list starts in the window), then each lane applies
+    // its y's terms.
+    for (int c0 = 0; c0 < d1; c0 += kWarp) {
+      bool use = false;
+      int y = 0;
+      if (c0 + lane < d1) {
+        y = __ldg(ci + b1 + c0 + lane);
+        use = y != v0 && idx.find(y) < 0;
+      }
+      const unsigned um = __ballot_sync(kFull, use);
+      if (use) slots[__popc(um & ((1u << lane) - 1u))] = y;
+      const int nu = __popc(um);
+      __syncwarp();
+#pragma unroll
+      for (int k = 0; k < W; ++k) Rl[k] = 0;
+      const bool mine = lane < nu;
+      int64_t ys = 0;
+      int dy = 0;
+      if (mine) {
+        const int yl = slots[lane];
+        ys = __ldg(rp + yl);
+        dy = (int)(__ldg(rp + yl + 1) - ys);  // >= 1: yl is adjacent to v1
+      }
+      const int incl = warp_inclusive_scan(dy, lane);
+      const int excl = incl - dy;
+      const int total = __shfl_sync(kFull, incl, kWarp - 1);
+      __syncwarp();  // rows cleared before other lanes set their bits
+      int started = 0;  // lists started before window F
+      for (int F = 0; F < total; F += kWarp) {
+        const unsigned bit = (dy > 0 && excl >= F && excl < F + kWarp) ? (1u << (excl - F)) : 0u;
+        const unsigned starts = __reduce_or_sync(kFull, bit);
+        const int o = max(started + __popc(starts & upto) - 1, 0);
+        const int64_t oys = __shfl_sync(kFull, ys, o);
+        const int oex = __shfl_sync(kFull, excl, o);
+        const int f = F + lane;
+        if (f < total) {
+          const int pos = idx.find(__ldg(ci + oys + (f - oex)));
+          if (pos >= 0) atomicOr(Rw + o * W + (pos >> 5), 1u << (pos & 31));
+        }
+        started += __popc(starts);
+      }
+      __syncwarp();
+      if (mine) {
       if (P == 4) {
         int c = 0;
 #pragma unroll
@@ -650,6 +727,8 @@ __device__ __forceinline__ void center_outer_edges(const int64_t *__restrict__ r
           }
         }
       }
+      }  // mine
+      __syncwarp();  // rows and slots are rewritten by the next chunk
     }
     if (counts) {
       __syncwarp();
@@ -691,9 +770,12 @@ __global__ void __launch_bounds__(kPatThreads) center_kernel(CenterArgs a) {
   unsigned *M = reinterpret_cast<unsigned *>(smem + grp * center_group_bytes(P, W));
   int32_t *n0 = reinterpret_cast<int32_t *>(M + 32 * W * W);
   // Outer patterns: this warp's R rows (one per lane) and position counters.
-  unsigned *Rw = reinterpret_cast<unsigned *>(n0 + 32 * W) + wg * (64 * W);
-  unsigned *Rl = Rw + lane * W;
+  unsigned *Rw = reinterpret_cast<unsigned *>(n0 + 32 * W) + wg * (64 * W + 32);
   int *cnt = reinterpret_cast<int *>(Rw + 32 * W);
+  int *slots = cnt + 32 * W;
+  // Position hash of N0 (outer patterns, W >= 4), after all warps' scratch.
+  int *hkeys = reinterpret_cast<int *>(n0 + 32 * W) +
+               (center_outer(P) ? center_group(W) * (64 * W + 32) : 0);
   const int total = *a.count;
   Acc acc;
   for (;;) {
@@ -707,8 +789,28 @@ __global__ void __launch_bounds__(kPatThreads) center_kernel(CenterArgs a) {
     const int64_t b0 = __ldg(a.rp + v0);
     const int d0 = (int)(__ldg(a.rp + v0 + 1) - b0);
     for (int i = gl; i < d0; i += G * kWarp) n0[i] = __ldg(a.ci + b0 + i);
+    PosIndex idx{n0, d0, nullptr, nullptr, 0};
+    if constexpr (center_hash(P, W)) {
+      constexpr int kLg = 6 + (W >= 8) + (W >= 16) + (W >= 32) + 2;  // 64W slots
+      static_assert((1 << kLg) == 64 * W, "hash size");
+      for (int i = gl; i < (1 << kLg); i += G * kWarp) hkeys[i] = -1;
+      if (G == 1) __syncwarp(); else __syncthreads();
+      for (int i = gl; i < d0; i += G * kWarp) {
+        const int y = n0[i];
+        unsigned h = ((unsigned)y * 2654435769u) >> (32 - kLg);
+        // Keys are distinct and the load is <= 1/2: an empty slot is found.
+        for (int step = 0; step < (1 << kLg); ++step) {
+          if (atomicCAS(hkeys + h, -1, y) == -1) {
+            hkeys[(1 << kLg) + h] = i;
+            break;
+          }
+          h = (h + 1u) & ((1u << kLg) - 1u);
+        }
+      }
+      idx = PosIndex{n0, d0, hkeys, hkeys + (1 << kLg), kLg};
+    }
     if (G == 1) __syncwarp(); else __syncthreads();
-    for (int i = gl; i < d0; i += G * kWarp) build_row<W>(a.rp, a.ci, n0, d0, n0[i], M + i * W);
+    for (int i = gl; i < d0; i += G * kWarp) build_row<W>(a.rp, a.ci, idx, n0[i], M + i * W);
     if (G == 1) __syncwarp(); else __syncthreads();
     if (P == 1) {  // star term of v0 (P1_frequency_count)
       for (int i = gl; i < d0; i += G * kWarp) {
@@ -724,7 +826,7 @@ __global__ void __launch_bounds__(kPatThreads) center_kernel(CenterArgs a) {
       }
     }
     if constexpr (center_outer(P))
-      center_outer_edges<P, W>(a.rp, a.ci, M, n0, d0, v0, wg, G, lane, Rl, cnt, acc);
+      center_outer_edges<P, W>(a.rp, a.ci, M, idx, v0, wg, G, lane, Rw, cnt, slots, acc);
     else
       center_edges<P, W>(M, d0, wg, G, lane, acc);
     if (G == 1) __syncwarp(); else __syncthreads();  // M and n0 are rewritten next
