@@ -135,7 +135,7 @@ def lib() -> C.CDLL:
     if _lib is None:
         if not os.path.exists(LIB_PATH):
             raise FileNotFoundError(
-                f"{LIB_PATH} is missing: run `python -c 'import __graft_entry__ as g; g.build()'` "
+                f"{LIB_PATH} is missing: run `python -c 'from mercury_b200.build import build; build()'` "
                 "(or `make -C mercury_b200/csrc`) first; there is no CPU fallback")
         handle = C.CDLL(LIB_PATH)
         for name, (res, args) in SIGNATURES.items():

@@ -1,7 +1,7 @@
 """Runs the reference's own programs (built from its sources into oracle/_ref/
 by oracle/ref.mk) on a GPU and records their counts and runtimes.
 
-  python tests/golden/run_reference.py [--out gpurun_out/reference_run.json]
+  python tests/golden/run_reference.py [--out reference_run.json]
                                        [--scales 16,20,22] [--repeats 3]
 
 * Fixture counts: oracle/_ref/tc_challenge and oracle/_ref/sm_patterns
@@ -191,7 +191,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--patterns", default="", help="n,mean,cap of a Chung-Lu graph to time P1..P8")
     ap.add_argument("--tc-chung-lu", type=int, default=0, help="vertices of a Chung-Lu TC timing")
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "reference_run.json"))
+    ap.add_argument("--out", default="reference_run.json")
     ap.add_argument("--scales", default="16,20,22")
     ap.add_argument("--repeats", type=int, default=3)
     ap.add_argument("--timeout", type=float, default=120.0)
@@ -208,7 +208,8 @@ def main():
         result["patterns"] = pattern_timing(int(pn), float(pm), float(pc), a.repeats, a.timeout)
     if a.tc_chung_lu:
         result["tc_chung_lu"] = tc_chung_lu_timing(a.tc_chung_lu, a.repeats, a.timeout)
-    os.makedirs(os.path.dirname(a.out), exist_ok=True)
+    if os.path.dirname(a.out):
+        os.makedirs(os.path.dirname(a.out), exist_ok=True)
     with open(a.out, "w") as f:
         json.dump(result, f, indent=1)
 
