@@ -383,6 +383,7 @@ int mc_batch_create(const int64_t *rowptr, const int32_t *col, int64_t n, int64_
 }
 
 int mc_batch_count(mc_batch_t *b, uint64_t *counts, mc_timing_t *timing) {
+  mc::NvtxRange range("mc_batch_count");
   if (!b || !counts) return MC_ERR_ARG;
   MC_CUDA_TRY(cudaSetDevice(b->g->device));
   cudaStream_t s = b->g->stream;

@@ -240,6 +240,7 @@ int csr_build_input(CsrBuild *b, const int32_t *src, const int32_t *dst, bool de
 }
 
 int csr_build_sort(CsrBuild *b, int64_t *nnz) {
+  NvtxRange range("csr_build_sort");
   cudaStream_t s = b->s;
   MC_CUDA_TRY(cudaMemsetAsync(b->flags, 0, sizeof(unsigned) * 4, s));
   *nnz = 0;
@@ -272,6 +273,7 @@ int csr_build_sort(CsrBuild *b, int64_t *nnz) {
 }
 
 int csr_build_emit(CsrBuild *b, int64_t *rowptr, int32_t *col, int64_t *max_degree) {
+  NvtxRange range("csr_build_emit");
   cudaStream_t s = b->s;
   *max_degree = 0;
   if (b->n == 0) {
@@ -343,6 +345,7 @@ float span_ms(cudaEvent_t a, cudaEvent_t b) {
 
 extern "C" int mc_csr_build(const int32_t *src, const int32_t *dst, int64_t num_edges, int64_t n,
                             unsigned flags, void *stream, mc_graph_t **out, mc_timing_t *timing) {
+  mc::NvtxRange range("mc_csr_build");
   if (!out || num_edges < 0 || n < 0 || (num_edges > 0 && (!src || !dst))) return MC_ERR_ARG;
   *out = nullptr;
   if (timing) std::memset(timing, 0, sizeof(*timing));

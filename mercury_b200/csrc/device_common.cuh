@@ -2,6 +2,7 @@
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include "mercury.h"
 
 namespace mc {
@@ -32,6 +33,16 @@ enum DeviceError : unsigned {
   } while (0)
 
 void set_last_cuda_error(cudaError_t e);
+
+// A named NVTX range for the lifetime of the object: the library's phases
+// (upload, orientation, counting, builds, batches) show up by name in a
+// timeline profiler; without a tool attached a range costs a few ns.
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 // Device buffers come from the stream-ordered allocator on the owning
 // handle's stream: freeing one never waits for the whole device.

@@ -166,6 +166,7 @@ const char *mc_version(void) { return "mercury_b200 0.1.0 sm_100a"; }
 
 int mc_dgraph_create(const int64_t *rowptr, const int32_t *col, int64_t n, int64_t nnz,
                      void *stream, unsigned flags, mc_dgraph_t **out) {
+  mc::NvtxRange range("mc_dgraph_create");
   if (!rowptr || (nnz > 0 && !col)) return MC_ERR_ARG;
   mc_dgraph *g = nullptr;
   int rc = mc::create_common(n, nnz, stream, out, &g);
@@ -206,6 +207,7 @@ int mc_dgraph_create_device(const int64_t *d_rowptr, const int32_t *d_col, int64
 
 int mc_dgraph_from_edges(const int32_t *src, const int32_t *dst, int64_t num_edges, int64_t n,
                          unsigned flags, void *stream, mc_dgraph_t **out, mc_timing_t *timing) {
+  mc::NvtxRange range("mc_dgraph_from_edges");
   if (!out || num_edges < 0 || (num_edges > 0 && (!src || !dst))) return MC_ERR_ARG;
   if (timing) std::memset(timing, 0, sizeof(*timing));
   mc_dgraph *g = nullptr;
@@ -290,6 +292,7 @@ int mc_tc_count(mc_dgraph_t *g, uint64_t *count, mc_timing_t *timing) {
 
 int mc_tc_count_shard(mc_dgraph_t *g, int shard, int num_shards, uint64_t *count,
                       mc_timing_t *timing) {
+  mc::NvtxRange range("mc_tc_count");
   if (!g || !count || num_shards < 1 || shard < 0 || shard >= num_shards) return MC_ERR_ARG;
   MC_CUDA_TRY(cudaSetDevice(g->device));
   int rc = mc::tc_alloc(g);

@@ -405,6 +405,7 @@ unsigned grid_for(int64_t items, int threads) {
 }  // namespace
 
 int validate_graph(mc_dgraph *g, unsigned flags) {
+  NvtxRange range("validate_graph");
   MC_CUDA_TRY(cudaMemsetAsync(g->err, 0, sizeof(unsigned), g->stream));
   MC_CUDA_TRY(cudaMemsetAsync(g->counters + 7, 0, sizeof(unsigned long long), g->stream));
   validate_rowptr_kernel<<<grid_for(g->n + 1, 256), 256, 0, g->stream>>>(
@@ -492,6 +493,7 @@ int tc_alloc(mc_dgraph *g) {
 }
 
 int tc_orient(mc_dgraph *g) {
+  NvtxRange range("tc_orient");
   const int64_t n = g->n, nnz = g->nnz;
   cudaStream_t s = g->stream;
   MC_CUDA_TRY(cudaMemsetAsync(g->counters, 0, sizeof(unsigned long long) * 7, s));

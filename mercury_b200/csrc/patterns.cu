@@ -1096,6 +1096,7 @@ int center_path(mc_dgraph *g, int pattern, PatArgs a, int grid) {
 
 int pattern_count(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12, mc_timing_t *timing,
                   int shard, int num_shards) {
+  NvtxRange range("pattern_count");
   cudaStream_t s = g->stream;
   const int64_t launches_before = g->launches;
   MC_CUDA_TRY(cudaMemsetAsync(g->counters, 0, sizeof(unsigned long long) * 8, s));

@@ -512,6 +512,7 @@ int resident_blocks(const void *kernel, int threads, size_t smem) {
 }  // namespace
 
 int tc_count_launch(mc_dgraph *g, cudaEvent_t after_hub, int shard, int num_shards) {
+  NvtxRange range("tc_count_launch");
   if (g->n == 0) {
     if (after_hub) MC_CUDA_TRY(cudaEventRecord(after_hub, g->stream));
     return MC_OK;
