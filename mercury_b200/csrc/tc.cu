@@ -425,6 +425,49 @@ __global__ void __launch_bounds__(kCountThreads, 5) tc_hub_kernel(CountArgs a) {
 // One warp per leaf task (owner d+ <= kLeafMaxOut): a private 256-slot cuckoo
 // table (load <= 1/4); the chunk's neighbours are filtered to partners whose
 // (short) lists are walked flat.
+// A leaf task as the warp holds it: the owner, its out-list (two entries per
+// lane, d+ <= kLeafMaxOut) and the chunk's neighbours (two per lane).
+struct LeafTask {
+  bool valid;
+  int x, d;
+  int64_t a0;
+  int y[2];   // neighbour ids, -1 past the chunk
+  int ow[2];  // owner out-list entries, kNoKey past d+
+};
+
+__device__ __forceinline__ LeafTask leaf_fetch(const CountArgs &a, int64_t ntasks,
+                                               unsigned long long t, int lane) {
+  LeafTask k;
+  k.valid = (int64_t)t < ntasks;
+  k.x = 0;
+  k.d = 0;
+  k.a0 = 0;
+  k.y[0] = k.y[1] = -1;
+  k.ow[0] = k.ow[1] = kNoKey;
+  if (!k.valid) return k;
+  const uint64_t task = shard_task(a, t);
+  k.x = (int)(task >> 32);
+  const int chunk = (int)(task & 0xffffffffu);
+  k.a0 = a.dag_rowptr[k.x];
+  k.d = a.key[k.x].y;
+  const int64_t e0 = a.rowptr[k.x] + (int64_t)chunk * kLeafChunk;
+  const int nc = (int)min((int64_t)kLeafChunk, a.rowptr[k.x + 1] - e0);
+  static_assert(kLeafChunk == 2 * kWarp && kLeafMaxOut <= 2 * kWarp, "two entries per lane");
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int i = r * kWarp + lane;
+    if (i < nc) k.y[r] = __ldg(a.col + e0 + i);
+    if (i < k.d) k.ow[r] = __ldg(a.dag_col + k.a0 + i);
+  }
+  return k;
+}
+
+// One warp per leaf task (owner d+ <= kLeafMaxOut): a private 256-slot cuckoo
+// table (load <= 1/4); the chunk's neighbours are filtered to partners whose
+// (short) lists are walked flat.  Every load of a task is a short dependent
+// chain (task -> owner row -> neighbours -> their d+ -> their list start ->
+// list entries), so the warp fetches the next task's owner, out-list and
+// neighbours while it works on the current one.
 __global__ void __launch_bounds__(kCountThreads) tc_leaf_kernel(CountArgs a) {
   __shared__ int tables[kCountThreads / kWarp][kLeafSlots];
   __shared__ int64_t c_st[kCountThreads / kWarp][kWarp];
@@ -437,66 +480,73 @@ __global__ void __launch_bounds__(kCountThreads) tc_leaf_kernel(CountArgs a) {
   const CuckooProbe probe{tab, 32 - lg};
   const int64_t ntasks = shard_tasks(a);
   unsigned long long hits = 0;
-  for (;;) {
-    unsigned long long t = 0;
-    if (lane == 0) t = atomicAdd(a.queue, 1ull);
-    t = __shfl_sync(kFull, t, 0);
-    if ((int64_t)t >= ntasks) break;
-    const uint64_t task = shard_task(a, t);
-    const int x = (int)(task >> 32);
-    const int chunk = (int)(task & 0xffffffffu);
-    const int64_t a0 = a.dag_rowptr[x];
-    const int d = a.key[x].y;
-    const int64_t e0 = a.rowptr[x] + (int64_t)chunk * kLeafChunk;
-    const int nc = (int)min((int64_t)kLeafChunk, a.rowptr[x + 1] - e0);
-    // Partners of the chunk first (kLeafChunk / 32 per lane); no table is
-    // built for a chunk without partners.
-    static_assert(kLeafChunk == 2 * kWarp, "two neighbours per lane");
+  // Tasks are claimed kLeafClaim at a time: one queue atomic per 16 tasks
+  // instead of per task (millions of them contend on one address).
+  constexpr unsigned long long kLeafClaim = 16;
+  unsigned long long batch = 0, used = kLeafClaim;
+  auto next_ticket = [&]() {
+    if (used == kLeafClaim) {
+      unsigned long long b = 0;
+      if (lane == 0) b = atomicAdd(a.queue, kLeafClaim);
+      batch = __shfl_sync(kFull, b, 0);
+      used = 0;
+    }
+    return batch + used++;
+  };
+  LeafTask cur = leaf_fetch(a, ntasks, next_ticket(), lane);
+  while (cur.valid) {
+    // Partners of the current chunk: d+ of each neighbour, then the list start.
+    int py[2];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) py[r] = cur.y[r] >= 0 ? __ldg(&a.key[cur.y[r]].y) : 0;
+    // The next task (claimed while those loads are in flight).
+    const unsigned long long tn = next_ticket();
     int64_t pst[2] = {0, 0};
     int plen[2] = {0, 0};
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
-      const int i = r * kWarp + lane;
-      if (i < nc) {
-        const int y = __ldg(a.col + e0 + i);
-        const int py = __ldg(&a.key[y].y);
-        if (owns(x, d, y, py)) {
-          pst[r] = __ldg(a.dag_rowptr + y);
-          plen[r] = py;
-        }
+      if (cur.y[r] >= 0 && owns(cur.x, cur.d, cur.y[r], py[r])) {
+        pst[r] = __ldg(a.dag_rowptr + cur.y[r]);
+        plen[r] = py[r];
       }
     }
-    if (!__any_sync(kFull, plen[0] > 0 || plen[1] > 0)) continue;
-    int4 *t4 = reinterpret_cast<int4 *>(tab);
-    for (int i = lane; i < kLeafSlots / 4; i += kWarp) t4[i] = make_int4(-1, -1, -1, -1);
-    __syncwarp();
-    bool ok = true;
-    for (int i = lane; i < d; i += kWarp) ok &= cuckoo_insert(tab, 32 - lg, __ldg(a.dag_col + a0 + i));
-    const bool use_table = __all_sync(kFull, ok);
-    __syncwarp();
-    unsigned long long th = 0;
+    // The next task's owner row, out-list and neighbours.
+    const LeafTask next = leaf_fetch(a, ntasks, tn, lane);
+    if (__any_sync(kFull, plen[0] > 0 || plen[1] > 0)) {
+      int4 *t4 = reinterpret_cast<int4 *>(tab);
+      for (int i = lane; i < kLeafSlots / 4; i += kWarp) t4[i] = make_int4(-1, -1, -1, -1);
+      __syncwarp();
+      bool ok = true;
 #pragma unroll
-    for (int r = 0; r < 2; ++r) {
-      int64_t st = pst[r];
-      int len = plen[r];
-      // Compact the partners into lanes 0..k-1.
-      const unsigned m = __ballot_sync(kFull, len > 0);
-      if (len > 0) {
-        const int rank = __popc(m & ((1u << lane) - 1u));
-        c_st[warp][rank] = st;
-        c_len[warp][rank] = len;
+      for (int r = 0; r < 2; ++r)
+        if (cur.ow[r] != kNoKey) ok &= cuckoo_insert(tab, 32 - lg, cur.ow[r]);
+      const bool use_table = __all_sync(kFull, ok);
+      __syncwarp();
+      unsigned long long th = 0;
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        int64_t st = pst[r];
+        int len = plen[r];
+        // Compact the partners into lanes 0..k-1.
+        const unsigned m = __ballot_sync(kFull, len > 0);
+        if (len > 0) {
+          const int rank = __popc(m & ((1u << lane) - 1u));
+          c_st[warp][rank] = st;
+          c_len[warp][rank] = len;
+        }
+        __syncwarp();
+        const int k = __popc(m);
+        st = lane < k ? c_st[warp][lane] : 0;
+        len = lane < k ? c_len[warp][lane] : 0;
+        __syncwarp();
+        if (use_table) th += stream_flat(a.dag_col, st, len, lane, probe);
+        else th += stream_flat(a.dag_col, st, len, lane, ListProbe{a.dag_col + cur.a0, cur.d});
       }
+      hits += th;
+      flush_task(a, cur.x, th, lane);
       __syncwarp();
-      const int k = __popc(m);
-      st = lane < k ? c_st[warp][lane] : 0;
-      len = lane < k ? c_len[warp][lane] : 0;
-      __syncwarp();
-      if (use_table) th += stream_flat(a.dag_col, st, len, lane, probe);
-      else th += stream_flat(a.dag_col, st, len, lane, ListProbe{a.dag_col + a0, d});
     }
-    hits += th;
-    flush_task(a, x, th, lane);
-    __syncwarp();
+    cur = next;
   }
   hits = warp_sum_u64(hits);
   if (lane == 0 && hits) atomicAdd(a.result, hits);
