@@ -2,11 +2,17 @@
 //
 // Reference: subgraph_matching/pattern_kernels.cuh (kernels P1_frequency_count,
 // P1_count_correction, P2..P8_subgraph_matching) and the host combine of
-// subgraph_matching/sm_multigpu.cu:206-232.  Each kernel walks the 2m
-// directed edges (v0, v1) of the symmetric CSR (graph.cc:336-365) with one
-// warp per edge, materialises the frontier lists of the pattern in a
-// per-warp slice of global scratch and accumulates two 64-bit counters; the
-// result is counters[1] for P4/P6 and counters[1] - counters[2] otherwise.
+// subgraph_matching/sm_multigpu.cu:206-232.  Every count is a sum over the
+// 2m directed edges (v0, v1) of the symmetric CSR (graph.cc:336-365), plus
+// P1's sum over vertices, of two 64-bit counters; the result is counters[1]
+// for P4/P6 and counters[1] - counters[2] otherwise.  Two routes compute the
+// same per-edge terms (each pattern takes the faster; see
+// pattern_uses_centers):
+//  * warp per directed edge: the frontier lists of the pattern materialised
+//    in a per-warp slice of global scratch, membership by binary search;
+//  * center bitmaps: a group of warps per center v0 holds the adjacency among
+//    N(v0) as bit rows in shared memory and reads each term off popcounts
+//    (centers of degree above kCenterMaxDeg stay on the first route).
 //
 // The warp set operations return the same sets as the reference's
 // difference_set / intersect / difference_num / intersect_num
