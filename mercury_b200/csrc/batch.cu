@@ -14,6 +14,7 @@
 // (subgraph_matching/sm_multigpu.cu:97).
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -243,7 +244,16 @@ int batch_create(const int64_t *rowptr, const int32_t *col, bool device_csr, int
   b->job.assign(jobs, jobs + num_graphs);
   b->bucket.assign(num_graphs, -1);
   b->dplus_bound.assign(num_graphs, 0);
-  b->param.assign(num_graphs, make_int2(kLeafMaxOut, 2));
+  // MERCURY_BATCH_LEAF_MAX (one of the autotuner's thresholds, 16..128)
+  // overrides the default warp/CTA threshold, so that tests reach every
+  // schedule the autotuner may pick.
+  int leaf_max = kLeafMaxOut;
+  if (const char *env = std::getenv("MERCURY_BATCH_LEAF_MAX")) {
+    const int v = std::atoi(env);
+    for (int c : kLeafChoices)
+      if (v == c) leaf_max = v;
+  }
+  b->param.assign(num_graphs, make_int2(leaf_max, 2));
   for (auto &row : b->tuned) row[0] = row[1] = -1;
   auto fail = [&](int rc) {
     batch_release(b);

@@ -425,8 +425,9 @@ __global__ void __launch_bounds__(kCountThreads, 5) tc_hub_kernel(CountArgs a) {
 // One warp per leaf task (owner d+ <= kLeafMaxOut): a private 256-slot cuckoo
 // table (load <= 1/4); the chunk's neighbours are filtered to partners whose
 // (short) lists are walked flat.
-// A leaf task as the warp holds it: the owner, its out-list (two entries per
-// lane, d+ <= kLeafMaxOut) and the chunk's neighbours (two per lane).
+// A leaf task as the warp holds it: the owner, the first 64 entries of its
+// out-list (two per lane; kLeafMaxOut is 64, a batch may route up to 128)
+// and the chunk's neighbours (two per lane).
 struct LeafTask {
   bool valid;
   int x, d;
@@ -452,7 +453,7 @@ __device__ __forceinline__ LeafTask leaf_fetch(const CountArgs &a, int64_t ntask
   k.d = a.key[k.x].y;
   const int64_t e0 = a.rowptr[k.x] + (int64_t)chunk * kLeafChunk;
   const int nc = (int)min((int64_t)kLeafChunk, a.rowptr[k.x + 1] - e0);
-  static_assert(kLeafChunk == 2 * kWarp && kLeafMaxOut <= 2 * kWarp, "two entries per lane");
+  static_assert(kLeafChunk == 2 * kWarp, "two neighbours per lane");
 #pragma unroll
   for (int r = 0; r < 2; ++r) {
     const int i = r * kWarp + lane;
@@ -520,6 +521,10 @@ __global__ void __launch_bounds__(kCountThreads) tc_leaf_kernel(CountArgs a) {
 #pragma unroll
       for (int r = 0; r < 2; ++r)
         if (cur.ow[r] != kNoKey) ok &= cuckoo_insert(tab, 32 - lg, cur.ow[r]);
+      // A batch's autotuner may route owners of d+ up to 128 here: the
+      // entries past the 64 fetched ahead come from memory.
+      for (int i = 2 * kWarp + lane; i < cur.d; i += kWarp)
+        ok &= cuckoo_insert(tab, 32 - lg, __ldg(a.dag_col + cur.a0 + i));
       const bool use_table = __all_sync(kFull, ok);
       __syncwarp();
       unsigned long long th = 0;

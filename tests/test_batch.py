@@ -63,6 +63,24 @@ def test_batch_counts_equal_single_graph_counts():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("leaf_max", [16, 32, 64, 128])
+def test_every_autotuner_threshold_gives_single_graph_counts(monkeypatch, leaf_max):
+    """Each warp/CTA threshold the autotuner can pick (owners of d+ up to
+    128 on the warp kernel) gives the single-graph counts, on triangle graphs
+    whose owners span d+ 1..~250."""
+    graphs = [Graph.rmat(s, ef, seed=s * 7 + ef) for s, ef in ((12, 16), (14, 24), (15, 32))]
+    graphs += [Graph.chung_lu(20000, 2.1, 16.0, 2000.0, seed=5)]
+    jobs = [0] * len(graphs)
+    want = []
+    for g in graphs:
+        with DeviceGraph(g) as d:
+            want.append(d.tc_count())
+    monkeypatch.setenv("MERCURY_BATCH_LEAF_MAX", str(leaf_max))
+    with Batch(graphs, jobs) as b:
+        assert b.count().tolist() == want
+
+
+@pytest.mark.gpu
 def test_batch_against_oracle_and_fixtures():
     names = ["k5", "star9", "petersen", "rand13", "isolated", "rmat8", "rmat10", "dense400"]
     graphs = [Graph(os.path.join(GOLDEN, "graphs", nm, "graph")) for nm in names]
