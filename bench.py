@@ -52,6 +52,9 @@ def parse_args():
     p.add_argument("--cpu-seconds", type=float, default=12.0,
                    help="target CPU time of the bounded CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--host-columns", action="store_true",
+                   help="TC mode: keep the column array in host memory (the placement the "
+                        "library picks for graphs larger than the device)")
     p.add_argument("--mode", choices=["tc", "batch", "serve", "patterns", "build"], default="tc",
                    help="tc: plain triangle count (the headline); batch: batched graphs/s; "
                         "serve: Poisson request stream, p50/p99 latency; patterns: P1..P8 "
@@ -70,12 +73,16 @@ def parse_args():
 
 
 def workload_config(a):
-    return {
+    cfg = {
         "workload": f"plain TC, RMAT scale {a.scale} edge factor {a.edge_factor} "
                     f"(0.57,0.19,0.19,0.05) seed {a.seed}, device orientation + count",
         "scale": a.scale, "edge_factor": a.edge_factor, "seed": a.seed,
         "l2": "no flush: inputs larger than L2 (symmetric CSR > 126 MB per step)",
     }
+    if getattr(a, "host_columns", False):
+        cfg["workload"] += ", column array in pinned host memory read through the device mapping"
+        cfg["columns"] = "host"
+    return cfg
 
 
 # ---------------------------------------------------------------- clocks
@@ -317,7 +324,10 @@ def run_ours(a, rank, world, local_rank):
     g = Graph.rmat(a.scale, a.edge_factor, seed=a.seed)
     n, nnz = g.n, g.nnz
     m = nnz // 2
-    dg = DeviceGraph(g)
+    if a.host_columns:
+        # The one-shot call below then takes the host-column placement too.
+        os.environ["MERCURY_DEVICE_BYTES"] = "1"
+    dg = DeviceGraph(g, host_columns=a.host_columns)
     stream = torch.cuda.ExternalStream(dg.stream)
 
     def step():

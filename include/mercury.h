@@ -40,6 +40,15 @@ extern "C" {
 
 /* ---- flags for mc_dgraph_create ----------------------------------------- */
 #define MC_VALIDATE_SYMMETRY 0x1u
+/* Keep the column array in pinned host memory that the device reads through
+ * its mapping (the row offsets, the DAG and all scratch stay in device
+ * memory).  mc_dgraph_create, mc_dgraph_create_device and mc_tc_count_host
+ * choose this placement by themselves when the device's free memory cannot
+ * hold the columns together with the triangle-count scratch.  Replaces the
+ * reference's unified-memory fallback for graphs larger than the GPU
+ * (include/graph_gpu.h:102-119).  Every pass over the columns then runs at
+ * the host link's bandwidth instead of HBM's. */
+#define MC_HOST_COLUMNS 0x2u
 
 /* Opaque handles. */
 typedef struct mc_graph mc_graph_t;   /* host CSR (loaded or generated)      */
@@ -204,6 +213,9 @@ int mc_dgraph_info(const mc_dgraph_t *g, int64_t *n, int64_t *nnz,
  * (col_out may be NULL for the offsets only). */
 int mc_dgraph_export_csr(const mc_dgraph_t *g, int64_t *rowptr_out,
                          int32_t *col_out);
+/* *on_host = 1 when the handle's columns are in host memory
+ * (MC_HOST_COLUMNS, asked for or chosen), else 0. */
+int mc_dgraph_columns_on_host(const mc_dgraph_t *g, int *on_host);
 void mc_dgraph_free(mc_dgraph_t *g);
 
 /* Triangle count.  Replaces TCSolver(Graph&, uint64_t&) (tc_challenge.cu:11,
@@ -334,7 +346,9 @@ void mc_server_free(mc_server_t *s);
 /* One-shot drop-in for TCSolver: host CSR in, count out.  Uploads, orients,
  * counts and copies the result back inside the call (timing->h2d_ms etc.).
  * Device buffers are cached in a per-thread context and reused while the
- * graph fits, so repeated calls do not re-allocate. */
+ * graph fits, so repeated calls do not re-allocate.  A graph the device
+ * cannot hold is counted with its columns in host memory (MC_HOST_COLUMNS),
+ * through a handle made for that call. */
 int mc_tc_count_host(const int64_t *rowptr, const int32_t *col, int64_t n,
                      int64_t nnz, uint64_t *count, mc_timing_t *timing);
 

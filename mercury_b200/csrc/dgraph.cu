@@ -1,6 +1,7 @@
 // C ABI of the device graph handle and the triangle-count entry points.
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cstdlib>
 #include <cstring>
 #include <new>
@@ -13,6 +14,13 @@ namespace mc {
 
 namespace {
 thread_local cudaError_t t_last_cuda = cudaSuccess;
+
+struct HostTimer {
+  std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+  double ms() const {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
+  }
+};
 
 double elapsed(cudaEvent_t a, cudaEvent_t b) {
   float ms = 0.f;
@@ -32,11 +40,13 @@ void release(mc_dgraph *g) {
                   g->mega_cnt,   g->mega_off,   g->mega_tasks, g->rank,
                   g->dag_rank,   g->rank_keys,  g->rank_counts, g->rank_offsets,
                   g->center_scratch};
+  if (g->col_host) bufs[1] = nullptr;  // pinned host memory, freed below
   // Stream-ordered frees: no device-wide synchronisation, so other handles'
   // work keeps running while this one is released.
   for (void *p : bufs)
     if (p) dev_free(p, g->stream);
   if (g->stream) cudaStreamSynchronize(g->stream);
+  if (g->col_host && g->col_h) cudaFreeHost(g->col_h);
   delete[] g->h_counters;
   for (cudaEvent_t e : g->ev)
     if (e) cudaEventDestroy(e);
@@ -45,7 +55,59 @@ void release(mc_dgraph *g) {
   delete g;
 }
 
-int create_common(int64_t n, int64_t nnz, void *stream, mc_dgraph **out, mc_dgraph **gp) {
+// Free device memory for the placement decision: what the driver reports
+// plus what this process's pool holds unused. MERCURY_DEVICE_BYTES replaces
+// the figure (tests reach the host-column fallback with it on small graphs).
+int device_bytes_available(int device, int64_t *avail) {
+  size_t free_b = 0, total_b = 0;
+  MC_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+  int64_t a = (int64_t)free_b;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t reserved = 0, used = 0;
+    if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess &&
+        reserved > used)
+      a += (int64_t)(reserved - used);
+  }
+  if (const char *env = std::getenv("MERCURY_DEVICE_BYTES")) {
+    const long long v = std::atoll(env);
+    if (v > 0) a = v;
+  }
+  *avail = a;
+  return MC_OK;
+}
+
+// Where a graph's column array goes. In device memory when the device can
+// hold it together with the triangle-count scratch (and a margin);
+// otherwise, or when the caller asks, in pinned host memory that the
+// kernels read through the device's mapping of it.
+constexpr int64_t kPlacementMargin = 256ll << 20;
+constexpr unsigned kDeviceColumns = 0x80000000u;  // internal: skip the decision
+int columns_on_host(int device, int64_t n, int64_t nnz, unsigned flags, bool *host) {
+  *host = (flags & MC_HOST_COLUMNS) != 0;
+  if (*host || nnz == 0 || (flags & kDeviceColumns)) return MC_OK;
+  int64_t avail = 0;
+  const int rc = device_bytes_available(device, &avail);
+  if (rc != MC_OK) return rc;
+  const int64_t in_core = 8 * (n + 1) + 4 * nnz + tc_device_bytes(n, nnz, false);
+  *host = in_core + kPlacementMargin > avail;
+  return MC_OK;
+}
+
+// Host-to-pinned copy of a large column array, split over the host threads.
+void copy_to_pinned(int32_t *dst, const int32_t *src, int64_t count) {
+  constexpr int64_t kPiece = 1 << 22;  // 16 MB of entries per piece
+  const int64_t pieces = (count + kPiece - 1) / kPiece;
+#pragma omp parallel for schedule(static)
+  for (int64_t p = 0; p < pieces; ++p) {
+    const int64_t a = p * kPiece, b = std::min(count, a + kPiece);
+    std::memcpy(dst + a, src + a, sizeof(int32_t) * (size_t)(b - a));
+  }
+}
+
+int create_common(int64_t n, int64_t nnz, void *stream, mc_dgraph **out, mc_dgraph **gp,
+                  unsigned flags = 0) {
   if (!out || n < 0 || nnz < 0) return MC_ERR_ARG;
   if (n > INT32_MAX - 1) return MC_ERR_UNSUPPORTED;
   *out = nullptr;
@@ -66,8 +128,15 @@ int create_common(int64_t n, int64_t nnz, void *stream, mc_dgraph **out, mc_dgra
   g->n = n;
   g->nnz = nnz;
   MC_CUDA_TRY(dev_alloc((void **)&g->rowptr, sizeof(int64_t) * (size_t)(n + 1), g->stream));
-  MC_CUDA_TRY(dev_alloc((void **)&g->col, sizeof(int32_t) * (size_t)std::max<int64_t>(nnz, 1),
-                        g->stream));
+  const int rc = columns_on_host(g->device, n, nnz, flags, &g->col_host);
+  if (rc != MC_OK) return rc;
+  const size_t col_bytes = sizeof(int32_t) * (size_t)std::max<int64_t>(nnz, 1);
+  if (g->col_host) {
+    MC_CUDA_TRY(cudaHostAlloc((void **)&g->col_h, col_bytes, cudaHostAllocMapped));
+    MC_CUDA_TRY(cudaHostGetDevicePointer((void **)&g->col, g->col_h, 0));
+  } else {
+    MC_CUDA_TRY(dev_alloc((void **)&g->col, col_bytes, g->stream));
+  }
   MC_CUDA_TRY(dev_alloc((void **)&g->counters, sizeof(unsigned long long) * 8, g->stream));
   MC_CUDA_TRY(dev_alloc((void **)&g->err, sizeof(unsigned), g->stream));
   // Host mirror of the counters (read after a stream synchronisation).
@@ -169,7 +238,7 @@ int mc_dgraph_create(const int64_t *rowptr, const int32_t *col, int64_t n, int64
   mc::NvtxRange range("mc_dgraph_create");
   if (!rowptr || (nnz > 0 && !col)) return MC_ERR_ARG;
   mc_dgraph *g = nullptr;
-  int rc = mc::create_common(n, nnz, stream, out, &g);
+  int rc = mc::create_common(n, nnz, stream, out, &g, flags);
   if (rc != MC_OK) {
     release(g);
     return rc;
@@ -177,7 +246,9 @@ int mc_dgraph_create(const int64_t *rowptr, const int32_t *col, int64_t n, int64
   auto up = [&]() -> int {
     MC_CUDA_TRY(cudaMemcpyAsync(g->rowptr, rowptr, sizeof(int64_t) * (size_t)(n + 1),
                                 cudaMemcpyHostToDevice, g->stream));
-    if (nnz > 0)
+    if (nnz > 0 && g->col_host)
+      mc::copy_to_pinned(g->col_h, col, nnz);
+    else if (nnz > 0)
       MC_CUDA_TRY(cudaMemcpyAsync(g->col, col, sizeof(int32_t) * (size_t)nnz,
                                   cudaMemcpyHostToDevice, g->stream));
     return MC_OK;
@@ -189,7 +260,7 @@ int mc_dgraph_create_device(const int64_t *d_rowptr, const int32_t *d_col, int64
                             void *stream, unsigned flags, mc_dgraph_t **out) {
   if (!d_rowptr || (nnz > 0 && !d_col)) return MC_ERR_ARG;
   mc_dgraph *g = nullptr;
-  int rc = mc::create_common(n, nnz, stream, out, &g);
+  int rc = mc::create_common(n, nnz, stream, out, &g, flags);
   if (rc != MC_OK) {
     release(g);
     return rc;
@@ -198,8 +269,10 @@ int mc_dgraph_create_device(const int64_t *d_rowptr, const int32_t *d_col, int64
     MC_CUDA_TRY(cudaMemcpyAsync(g->rowptr, d_rowptr, sizeof(int64_t) * (size_t)(n + 1),
                                 cudaMemcpyDeviceToDevice, g->stream));
     if (nnz > 0)
-      MC_CUDA_TRY(cudaMemcpyAsync(g->col, d_col, sizeof(int32_t) * (size_t)nnz,
-                                  cudaMemcpyDeviceToDevice, g->stream));
+      MC_CUDA_TRY(cudaMemcpyAsync(g->col_host ? g->col_h : g->col, d_col,
+                                  sizeof(int32_t) * (size_t)nnz,
+                                  g->col_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                                  g->stream));
     return MC_OK;
   };
   return mc::finish_create(g, flags, out, up());
@@ -213,7 +286,7 @@ int mc_dgraph_from_edges(const int32_t *src, const int32_t *dst, int64_t num_edg
   mc_dgraph *g = nullptr;
   // The handle starts with an empty column array; it is sized once the
   // build has counted the distinct entries.
-  int rc = mc::create_common(n, 0, stream, out, &g);
+  int rc = mc::create_common(n, 0, stream, out, &g, mc::kDeviceColumns);
   if (rc != MC_OK) {
     release(g);
     return rc;
@@ -271,10 +344,20 @@ int mc_dgraph_export_csr(const mc_dgraph_t *g, int64_t *rowptr_out, int32_t *col
   MC_CUDA_TRY(cudaSetDevice(g->device));
   MC_CUDA_TRY(cudaMemcpyAsync(rowptr_out, g->rowptr, sizeof(int64_t) * (size_t)(g->n + 1),
                               cudaMemcpyDeviceToHost, g->stream));
-  if (col_out && g->nnz > 0)
+  MC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  if (col_out && g->nnz > 0 && g->col_host) {
+    std::memcpy(col_out, g->col_h, sizeof(int32_t) * (size_t)g->nnz);
+  } else if (col_out && g->nnz > 0) {
     MC_CUDA_TRY(cudaMemcpyAsync(col_out, g->col, sizeof(int32_t) * (size_t)g->nnz,
                                 cudaMemcpyDeviceToHost, g->stream));
-  MC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    MC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  }
+  return MC_OK;
+}
+
+int mc_dgraph_columns_on_host(const mc_dgraph_t *g, int *on_host) {
+  if (!g || !on_host) return MC_ERR_ARG;
+  *on_host = g->col_host ? 1 : 0;
   return MC_OK;
 }
 
@@ -380,10 +463,30 @@ int mc_tc_count_host(const int64_t *rowptr, const int32_t *col, int64_t n, int64
     release(c.g);
     c.g = nullptr;
   }
+  // A graph the device cannot hold is counted through a handle with host
+  // columns (made for this call alone).
+  bool host = false;
+  if (!c.g) {
+    const int prc = mc::columns_on_host(dev, n, nnz, 0, &host);
+    if (prc != MC_OK) return prc;
+  }
+  if (host) {
+    mc::HostTimer t0;
+    mc_dgraph *g = nullptr;
+    int rc = mc_dgraph_create(rowptr, col, n, nnz, nullptr, MC_HOST_COLUMNS, &g);
+    const double create_ms = t0.ms();
+    if (rc == MC_OK) rc = mc_tc_count(g, count, timing);
+    if (rc == MC_OK && timing) {
+      timing->h2d_ms = create_ms;  // pinned copy of the columns and the contract check
+      timing->total_ms += create_ms;
+    }
+    release(g);
+    return rc;
+  }
   if (!c.g) {
     mc_dgraph *g = nullptr;
     mc_dgraph *tmp = nullptr;
-    int rc = mc::create_common(n, nnz, nullptr, &tmp, &g);
+    int rc = mc::create_common(n, nnz, nullptr, &tmp, &g, mc::kDeviceColumns);
     if (rc != MC_OK) {
       release(g);
       return rc;

@@ -45,6 +45,11 @@ struct mc_dgraph {
   int64_t max_degree = 0;     // set by validation on upload
   int64_t *rowptr = nullptr;  // n + 1
   int32_t *col = nullptr;     // nnz
+  // Column placement: false, col is device memory; true, col is pinned host
+  // memory mapped into the device's address space (graphs whose columns do
+  // not fit the device; every kernel reads them over the host link).
+  bool col_host = false;
+  int32_t *col_h = nullptr;   // host view of col when col_host
 
   // ---- pattern-count scratch (frontier lists), grown on demand ----------
   void *pat_scratch = nullptr;
@@ -56,12 +61,13 @@ struct mc_dgraph {
   bool tc_ready = false;
   int2 *key = nullptr;            // n      {symmetric degree, DAG out-degree}
   int64_t *dag_rowptr = nullptr;  // n + 1
-  int32_t *dag_col = nullptr;     // nnz (capacity; m+ used)
+  int32_t *dag_col = nullptr;     // dag_cap (m+ used)
+  int64_t dag_cap = 0;            // nnz; nnz / 2 + 1 with host columns
   // Degree rank: vertices sorted by (degree desc, id desc), so every entry
   // of N+(v) ranks below v. dag_rank holds dag_col's entries as ranks (a
   // single graph only; a batch leaves both null).
   int32_t *rank = nullptr;        // n
-  int32_t *dag_rank = nullptr;    // nnz (capacity)
+  int32_t *dag_rank = nullptr;    // dag_cap
   unsigned long long *rank_keys = nullptr;  // 2 n sort keys
   int32_t *rank_counts = nullptr;           // radix histograms
   int64_t *rank_offsets = nullptr;
@@ -92,6 +98,9 @@ namespace mc {
 // orient.cu
 int validate_graph(mc_dgraph *g, unsigned flags);
 int tc_alloc(mc_dgraph *g);
+// Device bytes tc_alloc takes for a single graph of n vertices and nnz
+// entries (the DAG at half the entries when the columns are on the host).
+int64_t tc_device_bytes(int64_t n, int64_t nnz, bool col_host);
 int tc_orient(mc_dgraph *g);
 int tc_partner_stats(mc_dgraph *g, unsigned long long *partner_edges, unsigned long long *work);
 // Contract checks of a caller-owned device CSR with caller-provided device

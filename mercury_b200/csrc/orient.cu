@@ -453,10 +453,30 @@ int validate_csr_words(const int64_t *rowptr, const int32_t *col, int64_t n, int
   return h_err ? MC_ERR_FORMAT : MC_OK;
 }
 
+namespace {
+// DAG capacity: every entry in device memory; with host columns the exact
+// m+ = nnz / 2 of a symmetric simple graph (tc_orient refuses more).
+int64_t dag_capacity(int64_t nnz, bool col_host) {
+  return col_host ? nnz / 2 + 1 : std::max<int64_t>(nnz, 1);
+}
+}  // namespace
+
+int64_t tc_device_bytes(int64_t n, int64_t nnz, bool col_host) {
+  const int64_t cap = std::max<int64_t>(nnz, 1);
+  const int64_t tiles = std::max<int64_t>((nnz + kTileEdges - 1) / kTileEdges, 1);
+  const int64_t tasks = n + cap / std::min(kHubChunk, kLeafChunk) + 1;
+  const int64_t scan = (int64_t)std::max(std::max(scan_temp_bytes(n + 1), scan_temp_bytes(tiles + 1)),
+                                         radix_temp_bytes(n));
+  return (n + 1) * (8 + 8 + 3 * 4 + 3 * 8 + 4 + 16) + 3 * 8 * tasks +
+         2 * 4 * dag_capacity(nnz, col_host) + tiles * (2 * kTileThreads + 12) +
+         2 * 12 * (radix_entries(n) + 1) + scan;
+}
+
 int tc_alloc(mc_dgraph *g) {
   if (g->tc_ready) return MC_OK;
   const int64_t n = g->n, cap = std::max<int64_t>(g->nnz, 1);
   const int64_t tiles = std::max<int64_t>((g->nnz + kTileEdges - 1) / kTileEdges, 1);
+  g->dag_cap = dag_capacity(g->nnz, g->col_host);
   // Each owner contributes ceil(deg / chunk) <= 1 + deg / chunk tasks.
   g->task_capacity = n + cap / std::min(kHubChunk, kLeafChunk) + 1;
   g->scan_temp_size = std::max(scan_temp_bytes(n + 1), scan_temp_bytes(tiles + 1));
@@ -466,7 +486,7 @@ int tc_alloc(mc_dgraph *g) {
   MC_CUDA_TRY(dev_alloc((void **)&(ptr), sizeof(*(ptr)) * (size_t)(count), g->stream))
   MC_ALLOC(g->key, n + 1);
   MC_ALLOC(g->dag_rowptr, n + 1);
-  MC_ALLOC(g->dag_col, cap);
+  MC_ALLOC(g->dag_col, g->dag_cap);
   MC_ALLOC(g->keep, tiles * kTileThreads);
   MC_ALLOC(g->tile_counts, tiles);
   MC_ALLOC(g->tile_offsets, tiles + 1);
@@ -481,7 +501,7 @@ int tc_alloc(mc_dgraph *g) {
   MC_ALLOC(g->mega_tasks, g->task_capacity);
   if (ranked) {
     MC_ALLOC(g->rank, n + 1);
-    MC_ALLOC(g->dag_rank, cap);
+    MC_ALLOC(g->dag_rank, g->dag_cap);
     MC_ALLOC(g->rank_keys, 2 * n + 2);
     MC_ALLOC(g->rank_counts, radix_entries(n) + 1);
     MC_ALLOC(g->rank_offsets, radix_entries(n) + 1);
@@ -526,6 +546,15 @@ int tc_orient(mc_dgraph *g) {
                                                          nullptr, nullptr, nullptr, nullptr);
     MC_CUDA_TRY(cudaGetLastError());
     MC_CUDA_TRY(exclusive_scan(g->tile_counts, g->tile_offsets, tiles, g->scan_temp, s));
+    if (g->dag_cap < nnz) {
+      // An exact-size DAG: a graph that keeps more than nnz / 2 entries is
+      // not symmetric, and pass B would write past the arrays.
+      int64_t m_plus = 0;
+      MC_CUDA_TRY(cudaMemcpyAsync(&m_plus, g->tile_offsets + tiles, sizeof(m_plus),
+                                  cudaMemcpyDeviceToHost, s));
+      MC_CUDA_TRY(cudaStreamSynchronize(s));
+      if (m_plus > g->dag_cap) return MC_ERR_FORMAT;
+    }
     dag_pass_kernel<true><<<grid, kTileThreads, 0, s>>>(g->rowptr, g->col, deg, n, nnz, g->key,
                                                         g->keep, nullptr, g->tile_offsets,
                                                         g->dag_rowptr, g->dag_col,

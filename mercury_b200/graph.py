@@ -126,7 +126,10 @@ class DeviceGraph:
     """Device-resident symmetric CSR (``mc_dgraph_t``) on the current GPU."""
 
     def __init__(self, rowptr, col=None, *, stream: Optional[int] = None,
-                 validate_symmetry: bool = False):
+                 validate_symmetry: bool = False, host_columns: bool = False):
+        """host_columns=True keeps the column array in pinned host memory that
+        the kernels read through the device's mapping (MC_HOST_COLUMNS); the
+        library also chooses it when the device cannot hold the graph."""
         if isinstance(rowptr, Graph):
             g = rowptr
             rowptr, col = g.rowptr, g.col
@@ -135,6 +138,8 @@ class DeviceGraph:
         self.nnz = len(col)
         self._h = C.c_void_p()
         flags = _ffi.MC_VALIDATE_SYMMETRY if validate_symmetry else 0
+        if host_columns:
+            flags |= _ffi.MC_HOST_COLUMNS
         check(lib().mc_dgraph_create(rowptr.ctypes.data, col.ctypes.data if self.nnz else None,
                                      self.n, self.nnz, stream, flags, C.byref(self._h)),
               "uploading the graph")
@@ -142,12 +147,15 @@ class DeviceGraph:
 
     @classmethod
     def from_device(cls, d_rowptr_ptr: int, d_col_ptr: int, n: int, nnz: int,
-                    stream: Optional[int] = None, validate_symmetry: bool = False) -> "DeviceGraph":
+                    stream: Optional[int] = None, validate_symmetry: bool = False,
+                    host_columns: bool = False) -> "DeviceGraph":
         """From a CSR already in device memory (e.g. torch tensors' data_ptr())."""
         self = cls.__new__(cls)
         self.n, self.nnz = n, nnz
         self._h = C.c_void_p()
         flags = _ffi.MC_VALIDATE_SYMMETRY if validate_symmetry else 0
+        if host_columns:
+            flags |= _ffi.MC_HOST_COLUMNS
         check(lib().mc_dgraph_create_device(d_rowptr_ptr, d_col_ptr, n, nnz, stream, flags,
                                             C.byref(self._h)), "adopting a device CSR")
         self.last_timing = Timing()
@@ -169,6 +177,14 @@ class DeviceGraph:
         col = np.zeros(max(self.nnz, 1), dtype=np.int32)
         check(lib().mc_dgraph_export_csr(self._h, rp.ctypes.data, col.ctypes.data), "export csr")
         return rp, col[: self.nnz]
+
+    @property
+    def columns_on_host(self) -> bool:
+        """True when the column array lives in host memory (asked for, or
+        chosen because the device could not hold the graph)."""
+        v = C.c_int()
+        check(lib().mc_dgraph_columns_on_host(self._h, C.byref(v)), "column placement")
+        return bool(v.value)
 
     @property
     def stream(self) -> int:

@@ -1,0 +1,123 @@
+"""Graphs whose column array stays in host memory (MC_HOST_COLUMNS).
+
+The reference moves a graph that does not fit the GPU into unified memory
+(include/graph_gpu.h:102-119) and runs the same kernels on it. Here the
+column array goes to pinned host memory that the kernels read through the
+device's mapping, chosen by the caller or by the library when the device
+cannot hold the graph. Every count must equal the device-resident one and
+the fixtures' golden values, bit for bit; all calls go through the C ABI.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from mercury_b200 import DeviceGraph, Graph, McError, tc_count_host
+from mercury_b200._ffi import MC_ERR_FORMAT
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+with open(os.path.join(GOLDEN, "golden.json")) as f:
+    GOLD = json.load(f)
+
+
+def fixture(name):
+    return Graph(os.path.join(GOLDEN, "graphs", name, "graph"))
+
+
+@pytest.mark.parametrize("name", sorted(GOLD))
+def test_golden_counts_with_host_columns(name):
+    g = fixture(name)
+    with DeviceGraph(g, host_columns=True) as d:
+        assert d.columns_on_host
+        assert d.tc_count() == GOLD[name]["TC"]
+        assert d.tc_count() == GOLD[name]["TC"]
+        for k in range(1, 9):
+            if f"P{k}" in GOLD[name]:
+                assert d.pattern_count(k) == GOLD[name][f"P{k}"], f"P{k}"
+
+
+@pytest.mark.parametrize("gen", [("rmat", 14, 16), ("rmat", 16, 16), ("cl", 40_000, 2_000)])
+def test_triangles_equal_device_columns(gen):
+    if gen[0] == "rmat":
+        g = Graph.rmat(gen[1], gen[2], seed=3)
+    else:
+        g = Graph.chung_lu(gen[1], 2.1, 16.0, float(gen[2]), seed=4)
+    with DeviceGraph(g) as d:
+        assert not d.columns_on_host
+        want = d.tc_count()
+        want_shards = [d.tc_count_shard(s, 3) for s in range(3)]
+    with DeviceGraph(g, host_columns=True) as h:
+        assert h.tc_count() == want
+        assert [h.tc_count_shard(s, 3) for s in range(3)] == want_shards
+    if gen == ("rmat", 14, 16):
+        assert want == orc.tc(g.rowptr, g.col)
+
+
+@pytest.mark.parametrize("route", ["edge", "centers"])
+def test_patterns_equal_device_columns_on_both_routes(route, monkeypatch):
+    monkeypatch.setenv("MERCURY_PATTERN_KERNEL", route)
+    g = Graph.rmat(9, 8, seed=11)
+    with DeviceGraph(g) as d:
+        want = [d.pattern_count(k) for k in range(1, 9)]
+    with DeviceGraph(g, host_columns=True) as h:
+        assert [h.pattern_count(k) for k in range(1, 9)] == want
+
+
+def test_export_and_device_source_with_host_columns():
+    import torch
+    g = Graph.rmat(12, 8, seed=5)
+    rp, col = np.asarray(g.rowptr), np.asarray(g.col)
+    with DeviceGraph(g, host_columns=True) as h:
+        r2, c2 = h.export_csr()
+        assert np.array_equal(r2, rp) and np.array_equal(c2, col)
+        want = h.tc_count()
+    trp, tcol = torch.from_numpy(rp).cuda(), torch.from_numpy(col).cuda()
+    torch.cuda.synchronize()
+    with DeviceGraph.from_device(trp.data_ptr(), tcol.data_ptr(), g.n, g.nnz,
+                                 host_columns=True) as h2:
+        assert h2.columns_on_host
+        assert h2.tc_count() == want == orc.tc(rp, col)
+
+
+def test_small_device_budget_chooses_host_columns(monkeypatch):
+    """MERCURY_DEVICE_BYTES stands in for the device's free memory: a budget
+    below the graph's in-core footprint moves the columns to the host."""
+    g = Graph.rmat(13, 16, seed=2)
+    want = orc.tc(g.rowptr, g.col)
+    with DeviceGraph(g) as d:
+        want_p4 = d.pattern_count(4)
+    monkeypatch.setenv("MERCURY_DEVICE_BYTES", str(1 << 20))
+    with DeviceGraph(g) as h:
+        assert h.columns_on_host
+        assert h.tc_count() == want
+        assert h.pattern_count(4) == want_p4
+    assert tc_count_host(g.rowptr, g.col) == want  # the one-shot path falls back too
+    monkeypatch.setenv("MERCURY_DEVICE_BYTES", str(1 << 40))
+    with DeviceGraph(g) as d:
+        assert not d.columns_on_host
+        assert d.tc_count() == want
+    assert tc_count_host(g.rowptr, g.col) == want
+
+
+def test_empty_and_edgeless_graphs_with_host_columns():
+    with DeviceGraph(np.zeros(1, np.int64), np.zeros(0, np.int32), host_columns=True) as h:
+        assert h.tc_count() == 0
+    with DeviceGraph(np.zeros(6, np.int64), np.zeros(0, np.int32), host_columns=True) as h:
+        assert h.tc_count() == 0 and h.pattern_count(3) == 0
+
+
+def test_asymmetric_rows_are_refused_before_the_dag_is_written():
+    """With host columns the DAG holds exactly nnz / 2 entries. A directed
+    path (each row lists only its successor) keeps every entry, more than
+    nnz / 2: the count is refused instead of writing past the DAG."""
+    n = 1000
+    rowptr = np.concatenate([np.arange(n, dtype=np.int64), [n - 1]]).astype(np.int64)
+    col = np.arange(1, n, dtype=np.int32)
+    with DeviceGraph(rowptr, col, host_columns=True) as h:
+        with pytest.raises(McError) as ex:
+            h.tc_count()
+        assert ex.value.status == MC_ERR_FORMAT
