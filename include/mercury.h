@@ -347,8 +347,8 @@ void mc_server_free(mc_server_t *s);
  * counts and copies the result back inside the call (timing->h2d_ms etc.).
  * Device buffers are cached in a per-thread context and reused while the
  * graph fits, so repeated calls do not re-allocate.  A graph the device
- * cannot hold is counted with its columns in host memory (MC_HOST_COLUMNS),
- * through a handle made for that call. */
+ * cannot hold is counted with its columns in host memory (MC_HOST_COLUMNS);
+ * that context is kept while later graphs also need it. */
 int mc_tc_count_host(const int64_t *rowptr, const int32_t *col, int64_t n,
                      int64_t nnz, uint64_t *count, mc_timing_t *timing);
 

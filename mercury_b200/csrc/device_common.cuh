@@ -20,6 +20,7 @@ enum DeviceError : unsigned {
   kErrHashFull = 1u << 5,     // a shared-memory table had no free slot
   kErrCapacity = 1u << 6,     // a scratch list exceeded its capacity
   kErrRank = 1u << 7,         // an out-list entry not ranked below its owner
+  kErrDagCapacity = 1u << 8,  // more DAG entries than an exact-size DAG holds
 };
 
 #define MC_CUDA_TRY(expr)                                   \

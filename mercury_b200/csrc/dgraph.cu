@@ -1,7 +1,6 @@
 // C ABI of the device graph handle and the triangle-count entry points.
 #include <algorithm>
 #include <atomic>
-#include <chrono>
 #include <cstdlib>
 #include <cstring>
 #include <new>
@@ -14,13 +13,6 @@ namespace mc {
 
 namespace {
 thread_local cudaError_t t_last_cuda = cudaSuccess;
-
-struct HostTimer {
-  std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
-  double ms() const {
-    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
-  }
-};
 
 double elapsed(cudaEvent_t a, cudaEvent_t b) {
   float ms = 0.f;
@@ -39,7 +31,7 @@ void release(mc_dgraph *g) {
                   g->leaf_tasks, g->scan_temp,  g->counters, g->err, g->pat_scratch,
                   g->mega_cnt,   g->mega_off,   g->mega_tasks, g->rank,
                   g->dag_rank,   g->rank_keys,  g->rank_counts, g->rank_offsets,
-                  g->center_scratch};
+                  g->center_scratch, g->stage, g->chunk_offsets};
   if (g->col_host) bufs[1] = nullptr;  // pinned host memory, freed below
   // Stream-ordered frees: no device-wide synchronisation, so other handles'
   // work keeps running while this one is released.
@@ -50,6 +42,9 @@ void release(mc_dgraph *g) {
   delete[] g->h_counters;
   for (cudaEvent_t e : g->ev)
     if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : g->stage_ev)
+    if (e) cudaEventDestroy(e);
+  if (g->copy_stream) cudaStreamDestroy(g->copy_stream);
   if (g->own_stream && g->stream) cudaStreamDestroy(g->stream);
   if (prev >= 0) cudaSetDevice(prev);
   delete g;
@@ -389,7 +384,11 @@ int mc_tc_count_shard(mc_dgraph_t *g, int shard, int num_shards, uint64_t *count
   // The hub table size follows the largest DAG out-degree (load <= 1/4).
   MC_CUDA_TRY(cudaMemcpyAsync(g->h_counters + 3, g->counters + 3, sizeof(unsigned long long),
                               cudaMemcpyDeviceToHost, s));
+  MC_CUDA_TRY(cudaMemcpyAsync(g->h_err, g->err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
   MC_CUDA_TRY(cudaStreamSynchronize(s));
+  // An exact-size DAG (host columns) that the rows overran: the input is not
+  // symmetric, and the DAG was left unwritten.
+  if (*g->h_err & mc::kErrDagCapacity) return MC_ERR_FORMAT;
   const long long maxd = (long long)g->h_counters[3];
   // MERCURY_TC_TABLE_LOG2_MAX (8..15) lowers the shared-memory table cap;
   // owners whose list no longer fits are then probed by binary search in
@@ -463,30 +462,23 @@ int mc_tc_count_host(const int64_t *rowptr, const int32_t *col, int64_t n, int64
     release(c.g);
     c.g = nullptr;
   }
-  // A graph the device cannot hold is counted through a handle with host
-  // columns (made for this call alone).
+  // A graph the device cannot hold is counted with its columns in host
+  // memory. A cached handle of that kind is kept only while the graphs
+  // still need it.
   bool host = false;
-  if (!c.g) {
+  if (!c.g || c.g->col_host) {
     const int prc = mc::columns_on_host(dev, n, nnz, 0, &host);
     if (prc != MC_OK) return prc;
-  }
-  if (host) {
-    mc::HostTimer t0;
-    mc_dgraph *g = nullptr;
-    int rc = mc_dgraph_create(rowptr, col, n, nnz, nullptr, MC_HOST_COLUMNS, &g);
-    const double create_ms = t0.ms();
-    if (rc == MC_OK) rc = mc_tc_count(g, count, timing);
-    if (rc == MC_OK && timing) {
-      timing->h2d_ms = create_ms;  // pinned copy of the columns and the contract check
-      timing->total_ms += create_ms;
+    if (c.g && !host) {
+      release(c.g);
+      c.g = nullptr;
     }
-    release(g);
-    return rc;
   }
   if (!c.g) {
     mc_dgraph *g = nullptr;
     mc_dgraph *tmp = nullptr;
-    int rc = mc::create_common(n, nnz, nullptr, &tmp, &g, mc::kDeviceColumns);
+    int rc = mc::create_common(n, nnz, nullptr, &tmp, &g,
+                               host ? MC_HOST_COLUMNS : mc::kDeviceColumns);
     if (rc != MC_OK) {
       release(g);
       return rc;
@@ -510,7 +502,9 @@ int mc_tc_count_host(const int64_t *rowptr, const int32_t *col, int64_t n, int64
   MC_CUDA_TRY(cudaEventRecord(e0, g->stream));
   MC_CUDA_TRY(cudaMemcpyAsync(g->rowptr, rowptr, sizeof(int64_t) * (size_t)(n + 1),
                               cudaMemcpyHostToDevice, g->stream));
-  if (nnz > 0)
+  if (nnz > 0 && g->col_host)
+    mc::copy_to_pinned(g->col_h, col, nnz);  // while the offsets upload
+  else if (nnz > 0)
     MC_CUDA_TRY(cudaMemcpyAsync(g->col, col, sizeof(int32_t) * (size_t)nnz, cudaMemcpyHostToDevice,
                                 g->stream));
   MC_CUDA_TRY(cudaEventRecord(e1, g->stream));

@@ -78,6 +78,14 @@ struct mc_dgraph {
   int64_t *hub_off = nullptr, *leaf_off = nullptr, *mega_off = nullptr;    // n + 1
   uint64_t *hub_tasks = nullptr, *leaf_tasks = nullptr, *mega_tasks = nullptr;  // capacity
   int64_t task_capacity = 0;
+  // Host columns: two DMA staging buffers of stage_edges entries each, the
+  // stream that fills them, events {copied[2], drained[2]}, and the tile
+  // offsets of one chunk.
+  int32_t *stage = nullptr;
+  int64_t stage_edges = 0;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t stage_ev[4] = {};
+  int64_t *chunk_offsets = nullptr;
   void *scan_temp = nullptr;
   size_t scan_temp_size = 0;
   // 0: result, 1: hub queue, 2: leaf queue, 3: max d+, 4-5: partner

@@ -22,6 +22,7 @@
 // Each vertex's (degree, d+) pair is one 8-byte word (key[]).
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 
 #include "dgraph.cuh"
 #include "device_common.cuh"
@@ -33,10 +34,11 @@ namespace {
 
 constexpr int kSegMax = 2048;  // row offsets of a tile kept in shared memory
 
-__device__ __forceinline__ void load_span(const int32_t *__restrict__ col, int64_t s, int64_t nnz,
+// The span's entries from p (16-byte aligned), `avail` of them valid.
+__device__ __forceinline__ void load_span(const int32_t *__restrict__ p32, int64_t avail,
                                           int32_t (&vals)[kEdgesPerThread]) {
-  if (s + kEdgesPerThread <= nnz) {
-    const int4 *p = reinterpret_cast<const int4 *>(col + s);
+  if (avail >= kEdgesPerThread) {
+    const int4 *p = reinterpret_cast<const int4 *>(p32);
 #pragma unroll
     for (int k = 0; k < kEdgesPerThread / 4; ++k) {
       int4 q = __ldg(p + k);
@@ -47,7 +49,7 @@ __device__ __forceinline__ void load_span(const int32_t *__restrict__ col, int64
     }
   } else {
 #pragma unroll
-    for (int k = 0; k < kEdgesPerThread; ++k) vals[k] = s + k < nnz ? __ldg(col + s + k) : 0;
+    for (int k = 0; k < kEdgesPerThread; ++k) vals[k] = k < avail ? __ldg(p32 + k) : 0;
   }
 }
 
@@ -159,30 +161,44 @@ __device__ __forceinline__ void write_span(const TileRows &tr, const int64_t *ro
   }
 }
 
+// Where a pass finds its tiles' column entries: the whole array (col_base
+// 0, tile_base 0), or a staged chunk of it holding entries from col_base on
+// for the tiles from tile_base on (chunks start on tile boundaries).
+struct ColumnChunk {
+  const int32_t *col;
+  int64_t col_base;
+  int64_t tile_base;
+};
+
 // Pass A (kWrite == false): DAG entries of every thread's span as a 16-bit
 // mask in keep[], per-tile counts, and d+ of every row by atomics on
 // key[].y (which starts at 0).  Pass B (kWrite == true): the kept entries
 // compacted into out_col (and, when rank is given, their ranks into
-// out_rank) and out_rowptr[r] = kept entries before rowptr[r].
+// out_rank) and out_rowptr[r] = kept entries before rowptr[r].  With
+// chunk_end given, pass B writes nothing when *chunk_end (the DAG entries
+// up to the end of this chunk) exceeds cap.
 template <bool kWrite>
 __global__ void __launch_bounds__(kTileThreads)
-    dag_pass_kernel(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ col,
+    dag_pass_kernel(const int64_t *__restrict__ rowptr, ColumnChunk cc,
                     const int32_t *__restrict__ deg, int64_t n, int64_t nnz, int2 *key,
                     uint16_t *keep_masks, int32_t *counts_out,
                     const int64_t *__restrict__ offs_in, int64_t *out_rowptr, int32_t *out_col,
-                    const int32_t *__restrict__ rank, int32_t *out_rank) {
+                    const int32_t *__restrict__ rank, int32_t *out_rank,
+                    const int64_t *chunk_end, int64_t cap) {
   __shared__ int64_t seg[kSegMax];
-  const int64_t t0 = (int64_t)blockIdx.x * kTileEdges;
+  if (kWrite && chunk_end && *chunk_end > cap) return;  // the same for the whole CTA
+  const int64_t tile = cc.tile_base + blockIdx.x;
+  const int64_t t0 = tile * kTileEdges;
   const int64_t t1 = min(t0 + kTileEdges, nnz);
   const TileRows tr = load_tile_rows(rowptr, n, t0, t1, seg);
   const int64_t s = t0 + (int64_t)threadIdx.x * kEdgesPerThread;
   const int64_t e_end = min(s + kEdgesPerThread, t1);
-  const int64_t slot = (int64_t)blockIdx.x * kTileThreads + threadIdx.x;
+  const int64_t slot = tile * kTileThreads + threadIdx.x;
   int32_t vals[kEdgesPerThread];
   unsigned keep = 0;
   int64_t r = 0;
   if (s < t1) {
-    load_span(col, s, nnz, vals);
+    load_span(cc.col + (s - cc.col_base), nnz - s, vals);
     r = tr.row_of(s);
     if (!kWrite) {
       int64_t v = r, next = tr.at(r + 1);
@@ -217,17 +233,31 @@ __global__ void __launch_bounds__(kTileThreads)
   }
   if (!kWrite) {
     const int t = block_sum_int(__popc(keep));
-    if (threadIdx.x == 0) counts_out[blockIdx.x] = t;
+    if (threadIdx.x == 0) counts_out[tile] = t;
     return;
   }
   int total = 0;
-  const int64_t base = offs_in[blockIdx.x];
+  const int64_t base = offs_in[tile];
   const int64_t pos = base + block_exclusive_int(__popc(keep), &total);
   if (s < t1)
     write_span(tr, rowptr, t0, s, e_end, r, vals, keep, pos, out_rowptr, out_col, rank, out_rank);
   // Rows after the last entry (trailing empty rows and q == n) start at nnz.
   if (t1 == nnz)
     for (int64_t q = tr.hi + 1 + threadIdx.x; q <= n; q += kTileThreads) out_rowptr[q] = base + total;
+}
+
+// Tile offsets of one staged chunk: offs[0] holds the DAG entries of the
+// earlier chunks; offs[i] = offs[0] + local[i] for i in [0, count] (local is
+// the chunk's exclusive scan, local[0] = 0, so offs[0] is rewritten with its
+// own value). The chunk's end above cap raises kErrDagCapacity.
+__global__ void chunk_offsets_kernel(const int64_t *__restrict__ local, int64_t count,
+                                     int64_t *offs, int64_t cap, unsigned *err) {
+  const int64_t base = offs[0];
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > count) return;
+  const int64_t v = base + local[i];
+  offs[i] = v;
+  if (i == count && v > cap) atomicOr(err, (unsigned)kErrDagCapacity);
 }
 
 // Contract checks that need the row of each entry: ids in range, strictly
@@ -461,15 +491,29 @@ int64_t dag_capacity(int64_t nnz, bool col_host) {
 }
 }  // namespace
 
+// Column entries per staging buffer with host columns (two buffers): 64 MB,
+// or MERCURY_STAGE_EDGES rounded down to whole tiles (tests use it to run
+// many chunks on small graphs).
+int64_t stage_capacity(int64_t nnz) {
+  int64_t stage = 1ll << 24;
+  if (const char *env = std::getenv("MERCURY_STAGE_EDGES")) {
+    const long long v = std::atoll(env);
+    if (v > 0) stage = std::max<int64_t>(kTileEdges, v / kTileEdges * kTileEdges);
+  }
+  return std::min(stage, std::max<int64_t>((nnz + kTileEdges - 1) / kTileEdges, 1) * kTileEdges);
+}
+
 int64_t tc_device_bytes(int64_t n, int64_t nnz, bool col_host) {
   const int64_t cap = std::max<int64_t>(nnz, 1);
   const int64_t tiles = std::max<int64_t>((nnz + kTileEdges - 1) / kTileEdges, 1);
   const int64_t tasks = n + cap / std::min(kHubChunk, kLeafChunk) + 1;
   const int64_t scan = (int64_t)std::max(std::max(scan_temp_bytes(n + 1), scan_temp_bytes(tiles + 1)),
                                          radix_temp_bytes(n));
+  const int64_t staging =
+      col_host ? 2 * 4 * stage_capacity(nnz) + 8 * (stage_capacity(nnz) / kTileEdges + 1) : 0;
   return (n + 1) * (8 + 8 + 3 * 4 + 3 * 8 + 4 + 16) + 3 * 8 * tasks +
          2 * 4 * dag_capacity(nnz, col_host) + tiles * (2 * kTileThreads + 12) +
-         2 * 12 * (radix_entries(n) + 1) + scan;
+         2 * 12 * (radix_entries(n) + 1) + scan + staging;
 }
 
 int tc_alloc(mc_dgraph *g) {
@@ -506,9 +550,63 @@ int tc_alloc(mc_dgraph *g) {
     MC_ALLOC(g->rank_counts, radix_entries(n) + 1);
     MC_ALLOC(g->rank_offsets, radix_entries(n) + 1);
   }
+  if (g->col_host && ranked) {
+    g->stage_edges = stage_capacity(g->nnz);
+    MC_ALLOC(g->stage, 2 * g->stage_edges);
+    MC_ALLOC(g->chunk_offsets, g->stage_edges / kTileEdges + 1);
+    MC_CUDA_TRY(cudaStreamCreateWithFlags(&g->copy_stream, cudaStreamNonBlocking));
+    for (cudaEvent_t &e : g->stage_ev)
+      MC_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
   MC_CUDA_TRY(dev_alloc(&g->scan_temp, g->scan_temp_size, g->stream));
 #undef MC_ALLOC
   g->tc_ready = true;
+  return MC_OK;
+}
+
+// Passes A and B with the columns in host memory: the column array crosses
+// the host link once, in chunks of whole tiles copied by DMA into two
+// device buffers, while the passes run on the previous chunk.  Each chunk
+// runs A, the scan of its tile counts on top of the earlier chunks' total,
+// and B, so no pass waits for the whole array. The DAG holds dag_cap
+// entries; a chunk that would end past it raises kErrDagCapacity and writes
+// nothing (the caller reads the flag before counting).
+static int staged_dag_passes(mc_dgraph *g, const int32_t *deg) {
+  const int64_t n = g->n, nnz = g->nnz;
+  cudaStream_t s = g->stream, cs = g->copy_stream;
+  cudaEvent_t *copied = g->stage_ev, *drained = g->stage_ev + 2;
+  MC_CUDA_TRY(cudaMemsetAsync(g->tile_offsets, 0, sizeof(int64_t), s));
+  // Copies start after the work already queued on the handle's stream.
+  MC_CUDA_TRY(cudaEventRecord(drained[0], s));
+  MC_CUDA_TRY(cudaStreamWaitEvent(cs, drained[0], 0));
+  const int64_t chunks = (nnz + g->stage_edges - 1) / g->stage_edges;
+  for (int64_t c = 0; c < chunks; ++c) {
+    const int slot = (int)(c & 1);
+    const int64_t e0 = c * g->stage_edges, e1 = std::min(nnz, e0 + g->stage_edges);
+    const int64_t tb = e0 / kTileEdges, ct = (e1 - e0 + kTileEdges - 1) / kTileEdges;
+    int32_t *buf = g->stage + (int64_t)slot * g->stage_edges;
+    if (c >= 2) MC_CUDA_TRY(cudaStreamWaitEvent(cs, drained[slot], 0));
+    MC_CUDA_TRY(cudaMemcpyAsync(buf, g->col_h + e0, sizeof(int32_t) * (size_t)(e1 - e0),
+                                cudaMemcpyHostToDevice, cs));
+    MC_CUDA_TRY(cudaEventRecord(copied[slot], cs));
+    MC_CUDA_TRY(cudaStreamWaitEvent(s, copied[slot], 0));
+    const ColumnChunk cc{buf, e0, tb};
+    dag_pass_kernel<false><<<(unsigned)ct, kTileThreads, 0, s>>>(
+        g->rowptr, cc, deg, n, nnz, g->key, g->keep, g->tile_counts, nullptr, nullptr, nullptr,
+        nullptr, nullptr, nullptr, 0);
+    MC_CUDA_TRY(cudaGetLastError());
+    MC_CUDA_TRY(exclusive_scan(g->tile_counts + tb, g->chunk_offsets, ct, g->scan_temp, s));
+    chunk_offsets_kernel<<<grid_for(ct + 1, 256), 256, 0, s>>>(g->chunk_offsets, ct,
+                                                               g->tile_offsets + tb, g->dag_cap,
+                                                               g->err);
+    MC_CUDA_TRY(cudaGetLastError());
+    dag_pass_kernel<true><<<(unsigned)ct, kTileThreads, 0, s>>>(
+        g->rowptr, cc, deg, n, nnz, g->key, g->keep, nullptr, g->tile_offsets, g->dag_rowptr,
+        g->dag_col, g->rank, g->dag_rank, g->tile_offsets + tb + ct, g->dag_cap);
+    MC_CUDA_TRY(cudaGetLastError());
+    MC_CUDA_TRY(cudaEventRecord(drained[slot], s));
+    g->launches += 3 + scan_launches(ct);
+  }
   return MC_OK;
 }
 
@@ -539,27 +637,21 @@ int tc_orient(mc_dgraph *g) {
   }
   if (tiles == 0) {
     MC_CUDA_TRY(cudaMemsetAsync(g->dag_rowptr, 0, sizeof(int64_t) * (n + 1), s));
+  } else if (g->col_host) {
+    const int rc = staged_dag_passes(g, deg);
+    if (rc != MC_OK) return rc;
   } else {
     const unsigned grid = (unsigned)tiles;
-    dag_pass_kernel<false><<<grid, kTileThreads, 0, s>>>(g->rowptr, g->col, deg, n, nnz, g->key,
-                                                         g->keep, g->tile_counts, nullptr,
-                                                         nullptr, nullptr, nullptr, nullptr);
+    const ColumnChunk all{g->col, 0, 0};
+    dag_pass_kernel<false><<<grid, kTileThreads, 0, s>>>(
+        g->rowptr, all, deg, n, nnz, g->key, g->keep, g->tile_counts, nullptr, nullptr, nullptr,
+        nullptr, nullptr, nullptr, 0);
     MC_CUDA_TRY(cudaGetLastError());
     MC_CUDA_TRY(exclusive_scan(g->tile_counts, g->tile_offsets, tiles, g->scan_temp, s));
-    if (g->dag_cap < nnz) {
-      // An exact-size DAG: a graph that keeps more than nnz / 2 entries is
-      // not symmetric, and pass B would write past the arrays.
-      int64_t m_plus = 0;
-      MC_CUDA_TRY(cudaMemcpyAsync(&m_plus, g->tile_offsets + tiles, sizeof(m_plus),
-                                  cudaMemcpyDeviceToHost, s));
-      MC_CUDA_TRY(cudaStreamSynchronize(s));
-      if (m_plus > g->dag_cap) return MC_ERR_FORMAT;
-    }
-    dag_pass_kernel<true><<<grid, kTileThreads, 0, s>>>(g->rowptr, g->col, deg, n, nnz, g->key,
-                                                        g->keep, nullptr, g->tile_offsets,
-                                                        g->dag_rowptr, g->dag_col,
-                                                        g->batch.gid ? nullptr : g->rank,
-                                                        g->batch.gid ? nullptr : g->dag_rank);
+    dag_pass_kernel<true><<<grid, kTileThreads, 0, s>>>(
+        g->rowptr, all, deg, n, nnz, g->key, g->keep, nullptr, g->tile_offsets, g->dag_rowptr,
+        g->dag_col, g->batch.gid ? nullptr : g->rank, g->batch.gid ? nullptr : g->dag_rank,
+        nullptr, 0);
     MC_CUDA_TRY(cudaGetLastError());
     g->launches += 2 + scan_launches(tiles);
   }

@@ -57,6 +57,23 @@ def test_triangles_equal_device_columns(gen):
         assert want == orc.tc(g.rowptr, g.col)
 
 
+@pytest.mark.parametrize("stage", [4096, 3 * 4096, 40_000, 1 << 20])
+def test_staged_orientation_over_many_chunks(stage, monkeypatch):
+    """The column array crosses to the device in chunks of whole 4096-entry
+    tiles through two buffers; small chunks split rows between chunks and
+    reuse each buffer many times. The DAG must equal the device-column one."""
+    monkeypatch.setenv("MERCURY_STAGE_EDGES", str(stage))
+    g = Graph.rmat(14, 16, seed=8)
+    with DeviceGraph(g) as d:
+        want = d.tc_count()
+        want_dag = d.export_dag()
+    with DeviceGraph(g, host_columns=True) as h:
+        assert h.tc_count() == want
+        got_dag = h.export_dag()
+        assert np.array_equal(got_dag[0], want_dag[0]) and np.array_equal(got_dag[1], want_dag[1])
+        assert h.tc_count() == want
+
+
 @pytest.mark.parametrize("route", ["edge", "centers"])
 def test_patterns_equal_device_columns_on_both_routes(route, monkeypatch):
     monkeypatch.setenv("MERCURY_PATTERN_KERNEL", route)
@@ -96,6 +113,9 @@ def test_small_device_budget_chooses_host_columns(monkeypatch):
         assert h.tc_count() == want
         assert h.pattern_count(4) == want_p4
     assert tc_count_host(g.rowptr, g.col) == want  # the one-shot path falls back too
+    small = Graph.rmat(10, 8, seed=3)
+    assert tc_count_host(small.rowptr, small.col) == orc.tc(small.rowptr, small.col)
+    assert tc_count_host(g.rowptr, g.col) == want  # its cached host-column context again
     monkeypatch.setenv("MERCURY_DEVICE_BYTES", str(1 << 40))
     with DeviceGraph(g) as d:
         assert not d.columns_on_host
@@ -114,10 +134,15 @@ def test_asymmetric_rows_are_refused_before_the_dag_is_written():
     """With host columns the DAG holds exactly nnz / 2 entries. A directed
     path (each row lists only its successor) keeps every entry, more than
     nnz / 2: the count is refused instead of writing past the DAG."""
-    n = 1000
-    rowptr = np.concatenate([np.arange(n, dtype=np.int64), [n - 1]]).astype(np.int64)
-    col = np.arange(1, n, dtype=np.int32)
-    with DeviceGraph(rowptr, col, host_columns=True) as h:
-        with pytest.raises(McError) as ex:
-            h.tc_count()
-        assert ex.value.status == MC_ERR_FORMAT
+    for n, stage in ((1000, 0), (50_000, 4096)):  # one chunk; 13 chunks
+        if stage:
+            os.environ["MERCURY_STAGE_EDGES"] = str(stage)
+        try:
+            rowptr = np.concatenate([np.arange(n, dtype=np.int64), [n - 1]]).astype(np.int64)
+            col = np.arange(1, n, dtype=np.int32)
+            with DeviceGraph(rowptr, col, host_columns=True) as h:
+                with pytest.raises(McError) as ex:
+                    h.tc_count()
+                assert ex.value.status == MC_ERR_FORMAT
+        finally:
+            os.environ.pop("MERCURY_STAGE_EDGES", None)
