@@ -31,7 +31,7 @@ void release(mc_dgraph *g) {
                   g->leaf_tasks, g->scan_temp,  g->counters, g->err, g->pat_scratch,
                   g->mega_cnt,   g->mega_off,   g->mega_tasks, g->rank,
                   g->dag_rank,   g->rank_keys,  g->rank_counts, g->rank_offsets,
-                  g->center_scratch, g->stage, g->chunk_offsets};
+                  g->center_scratch, g->stage, g->chunk_offsets, g->core_bits};
   if (g->col_host) bufs[1] = nullptr;  // pinned host memory, freed below
   // Stream-ordered frees: no device-wide synchronisation, so other handles'
   // work keeps running while this one is released.
@@ -407,6 +407,13 @@ int mc_tc_count_shard(mc_dgraph_t *g, int shard, int num_shards, uint64_t *count
   if (const char *env = std::getenv("MERCURY_TC_BITMAP_BITS")) {
     const long v = std::atol(env);
     if (v >= 0) g->bitmap_bits_cap = (int)std::min<long>(v, 0x7fffffff);
+  }
+  // MERCURY_TC_DENSE_FACTOR (1..64): words of a core-bitmap AND allowed per
+  // list entry it replaces.
+  g->dense_factor = 2;
+  if (const char *env = std::getenv("MERCURY_TC_DENSE_FACTOR")) {
+    const int v = std::atoi(env);
+    if (v >= 1 && v <= 64) g->dense_factor = v;
   }
   MC_CUDA_TRY(cudaEventRecord(g->ev[4], s));
   rc = mc::tc_count_launch(g, g->ev[2], shard, num_shards);

@@ -22,6 +22,20 @@ constexpr int kHubSmallTableLog2 = 12;
 // Least shared memory of a hub CTA (also the bitmap capacity: 8 bits per
 // byte, so owners of degree rank below 262144 use bitmaps).
 constexpr int kHubBitmapBytes = 32768;
+// Core bitmaps: N+(v) as a bitmap over ranks [0, rank(v)) for the vertices
+// of the kCoreRanks lowest ranks (the highest degrees), so that a hub task
+// intersects such a partner by a word-wise AND with its owner's bitmap.
+constexpr int kCoreRanks = 32768;
+
+// Word offset of rank r's core bitmap: rank t holds ceil(t / 128) quads (4
+// words, 16-byte aligned) covering bits [0, t), so the offset is 4 times
+// sum over t < r of ceil(t / 128) = 64 Q (Q + 1) + (r - 1 - 128 Q)(Q + 1),
+// with Q = (r - 1) / 128.
+__host__ __device__ __forceinline__ int64_t core_offset(int64_t r) {
+  if (r <= 0) return 0;
+  const int64_t q = (r - 1) >> 7;
+  return 4 * (64 * q * (q + 1) + (r - 1 - 128 * q) * (q + 1));
+}
 }  // namespace mc
 
 namespace mc {
@@ -71,6 +85,11 @@ struct mc_dgraph {
   unsigned long long *rank_keys = nullptr;  // 2 n sort keys
   int32_t *rank_counts = nullptr;           // radix histograms
   int64_t *rank_offsets = nullptr;
+  const unsigned long long *rank_sorted = nullptr;  // rank p -> key of vertex (see orient.cu)
+  unsigned *core_bits = nullptr;  // core_offset(core_ranks) words
+  int core_ranks = 0;             // capacity: core_offset(core_ranks) words
+  int core_used = 0;              // ranks [0, core_used) have core bitmaps (<= n)
+  int dense_factor = 2;           // AND when its words <= factor x list entries
   uint16_t *keep = nullptr;       // one DAG keep mask per orientation thread
   int32_t *tile_counts = nullptr; // tiles
   int64_t *tile_offsets = nullptr;// tiles + 1

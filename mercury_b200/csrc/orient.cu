@@ -345,6 +345,28 @@ __global__ void rank_scatter_kernel(const unsigned long long *__restrict__ sorte
   if (p < n) rank[n - 1 - (int64_t)(uint32_t)sorted[p]] = (int32_t)p;
 }
 
+// Core bitmaps: warp per rank p < core_ranks; its vertex is the one whose
+// sort key sits at position p. Every entry z of N+(v) ranks below p, so it
+// sets bit z of the words from core_offset(p) (which start
+// cleared; the row's last quad pads to a multiple of 128 bits with zeros).
+// Nothing runs when an exact-size DAG was overrun: its rows were
+// then never written.
+__global__ void core_bits_kernel(const unsigned long long *__restrict__ sorted, int64_t n,
+                                 int core_ranks, const int64_t *__restrict__ dag_rowptr,
+                                 const int32_t *__restrict__ dag_rank, unsigned *core,
+                                 unsigned *err) {
+  const int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
+  const int lane = threadIdx.x & (kWarp - 1);
+  if (p >= core_ranks || (*(volatile unsigned *)err & kErrDagCapacity)) return;
+  const int64_t v = n - 1 - (int64_t)(uint32_t)sorted[p];
+  unsigned *row = core + core_offset(p);
+  for (int64_t e = dag_rowptr[v] + lane; e < dag_rowptr[v + 1]; e += kWarp) {
+    const int z = __ldg(dag_rank + e);
+    if (z >= 0 && z < p) atomicOr(row + (z >> 5), 1u << (z & 31));
+    else atomicOr(err, (unsigned)kErrRank);
+  }
+}
+
 // key[v] = {degree, 0}; deg[v] = degree alone (4 bytes per gather in pass A).
 __global__ void init_key_kernel(const int64_t *rowptr, int64_t n, int2 *key, int32_t *deg) {
   const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -503,6 +525,17 @@ int64_t stage_capacity(int64_t nnz) {
   return std::min(stage, std::max<int64_t>((nnz + kTileEdges - 1) / kTileEdges, 1) * kTileEdges);
 }
 
+// Ranks with core bitmaps: kCoreRanks, or MERCURY_TC_CORE_RANKS (0 turns
+// them off; tests move the boundary with it), at most n.
+int core_rank_count(int64_t n) {
+  int64_t k = kCoreRanks;
+  if (const char *env = std::getenv("MERCURY_TC_CORE_RANKS")) {
+    const long long v = std::atoll(env);
+    if (v >= 0) k = std::min<long long>(v, 1 << 18);
+  }
+  return (int)std::min<int64_t>(k, n);
+}
+
 int64_t tc_device_bytes(int64_t n, int64_t nnz, bool col_host) {
   const int64_t cap = std::max<int64_t>(nnz, 1);
   const int64_t tiles = std::max<int64_t>((nnz + kTileEdges - 1) / kTileEdges, 1);
@@ -513,7 +546,7 @@ int64_t tc_device_bytes(int64_t n, int64_t nnz, bool col_host) {
       col_host ? 2 * 4 * stage_capacity(nnz) + 8 * (stage_capacity(nnz) / kTileEdges + 1) : 0;
   return (n + 1) * (8 + 8 + 3 * 4 + 3 * 8 + 4 + 16) + 3 * 8 * tasks +
          2 * 4 * dag_capacity(nnz, col_host) + tiles * (2 * kTileThreads + 12) +
-         2 * 12 * (radix_entries(n) + 1) + scan + staging;
+         2 * 12 * (radix_entries(n) + 1) + scan + staging + 4 * core_offset(core_rank_count(n));
 }
 
 int tc_alloc(mc_dgraph *g) {
@@ -549,6 +582,8 @@ int tc_alloc(mc_dgraph *g) {
     MC_ALLOC(g->rank_keys, 2 * n + 2);
     MC_ALLOC(g->rank_counts, radix_entries(n) + 1);
     MC_ALLOC(g->rank_offsets, radix_entries(n) + 1);
+    g->core_ranks = core_rank_count(n);
+    if (g->core_ranks > 0) MC_ALLOC(g->core_bits, core_offset(g->core_ranks));
   }
   if (g->col_host && ranked) {
     g->stage_edges = stage_capacity(g->nnz);
@@ -615,6 +650,7 @@ int tc_orient(mc_dgraph *g) {
   const int64_t n = g->n, nnz = g->nnz;
   cudaStream_t s = g->stream;
   MC_CUDA_TRY(cudaMemsetAsync(g->counters, 0, sizeof(unsigned long long) * 7, s));
+  g->core_used = 0;
   if (n == 0) return MC_OK;
   const int64_t tiles = (nnz + kTileEdges - 1) / kTileEdges;
   // The degrees alone, for pass A's gathers, in mega_cnt (unused until the
@@ -633,6 +669,7 @@ int tc_orient(mc_dgraph *g) {
                                g->rank_offsets, g->scan_temp, s, &sorted, &g->launches));
     rank_scatter_kernel<<<grid_for(n, 256), 256, 0, s>>>(sorted, n, g->rank);
     MC_CUDA_TRY(cudaGetLastError());
+    g->rank_sorted = sorted;
     g->launches += 2;
   }
   if (tiles == 0) {
@@ -654,6 +691,16 @@ int tc_orient(mc_dgraph *g) {
         nullptr, 0);
     MC_CUDA_TRY(cudaGetLastError());
     g->launches += 2 + scan_launches(tiles);
+  }
+  // A handle reused for a smaller graph keeps its capacity: only the ranks
+  // of this graph get core bitmaps.
+  if (g->core_bits && g->rank_sorted && !g->batch.gid) {
+    g->core_used = (int)std::min<int64_t>(g->core_ranks, n);
+    MC_CUDA_TRY(cudaMemsetAsync(g->core_bits, 0, sizeof(unsigned) * core_offset(g->core_used), s));
+    core_bits_kernel<<<grid_for((int64_t)g->core_used * kWarp, 256), 256, 0, s>>>(
+        g->rank_sorted, n, g->core_used, g->dag_rowptr, g->dag_rank, g->core_bits, g->err);
+    MC_CUDA_TRY(cudaGetLastError());
+    g->launches += 1;
   }
   task_count_kernel<<<grid_for(n, 256), 256, 0, s>>>(g->key, n, g->hub_cnt, g->leaf_cnt,
                                                      g->mega_cnt, g->counters + 3, g->batch);

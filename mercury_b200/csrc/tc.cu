@@ -45,6 +45,11 @@ struct CountArgs {
   const int32_t *__restrict__ rank;
   const int32_t *__restrict__ dag_rank;  // N+ lists as ranks
   int bitmap_bits;
+  // Core bitmaps of the ranks [0, core_ranks) (null: none), laid out by
+  // core_offset().
+  const unsigned *__restrict__ core;
+  int core_ranks;
+  int dense_factor;  // dense when the AND's words <= dense_factor x list length
   int shard, num_shards;  // this call counts tasks shard, shard + num_shards, ...
   BatchView bv;           // per-graph table factor and counts of a batch
 };
@@ -160,24 +165,32 @@ constexpr int kLongList = 64;
 
 // Partners of one hub task, compacted in row order.  Thread t examines
 // neighbours 2t and 2t+1 of the chunk; one block scan of (long partners,
-// short partners, short list lengths) packed in 64 bits places every
-// partner.  Long list j (j < nl): start base[j], length off[j].  Short list
-// j: elements [off[nl+j], off[nl+j+1]) of the short stream, element f of it
-// at lists[base[nl+j] + f] (base = list start - offset).  Returns nl and the
-// short stream length.
+// short partners, dense partners, short list lengths) packed in 64 bits
+// (16 bits each: a chunk has at most 512 partners and the short lengths sum
+// to at most 512 x 63) places every partner.  Long list j (j < nl): start
+// base[j], length off[j].  Short list j: elements [off[nl+j], off[nl+j+1])
+// of the short stream, element f of it at lists[base[nl+j] + f] (base =
+// list start - offset).  Dense partner j (j < nd): its rank at
+// base[kHubChunk - 1 - j], above every long and short entry.
+//
+// A long partner y is dense when the owner keeps a bitmap (owner_bits, its
+// rank) and y has a core bitmap whose AND with it over the words below both
+// ranks takes at most dense_factor words per entry of y's list.
 struct Partners {
   int nl;     // long lists
   int total;  // elements of the short stream
+  int nd;     // dense partners
 };
 
 __device__ __forceinline__ Partners find_partners(const CountArgs &a, int x, int px, int64_t e0,
                                                   int nc, long long *s_base, int *s_off,
-                                                  unsigned long long *s_warp) {
+                                                  unsigned long long *s_warp, int owner_bits) {
   static_assert(kHubChunk == 2 * kCountThreads, "two neighbours per thread");
   constexpr int kWarps = kCountThreads / kWarp;
   const int lane = threadIdx.x & (kWarp - 1), warp = threadIdx.x / kWarp;
   int len[2] = {0, 0};
   long long st[2] = {0, 0};
+  bool dense[2] = {false, false};
 #pragma unroll
   for (int r = 0; r < 2; ++r) {
     const int i = 2 * threadIdx.x + r;
@@ -186,14 +199,21 @@ __device__ __forceinline__ Partners find_partners(const CountArgs &a, int x, int
       const int py = __ldg(&a.key[y].y);
       if (owns(x, px, y, py)) {
         len[r] = py;
-        st[r] = __ldg(a.dag_rowptr + y);
+        if (py >= kLongList && owner_bits > 0) {
+          const int ry = __ldg(a.rank + y);
+          const int words = (min(ry, owner_bits) + 31) >> 5;
+          dense[r] = ry < a.core_ranks && words <= a.dense_factor * py;
+          if (dense[r]) st[r] = ry;
+        }
+        if (!dense[r]) st[r] = __ldg(a.dag_rowptr + y);
       }
     }
   }
   unsigned long long mine = 0;
 #pragma unroll
   for (int r = 0; r < 2; ++r) {
-    if (len[r] >= kLongList) mine += 1ull << 48;
+    if (dense[r]) mine += 1ull << 16;
+    else if (len[r] >= kLongList) mine += 1ull << 48;
     else if (len[r] > 0) mine += (1ull << 32) + (unsigned)len[r];
   }
   unsigned long long incl = mine;
@@ -213,11 +233,16 @@ __device__ __forceinline__ Partners find_partners(const CountArgs &a, int x, int
   }
   const unsigned long long excl = before + incl - mine;
   const int nl = (int)(all >> 48), ns = (int)((all >> 32) & 0xffff);
+  const int nd = (int)((all >> 16) & 0xffff);
   int lslot = (int)(excl >> 48);
-  int sslot = nl + (int)((excl >> 32) & 0xffff), off = (int)(unsigned)excl;
+  int sslot = nl + (int)((excl >> 32) & 0xffff), off = (int)(excl & 0xffff);
+  int dslot = (int)((excl >> 16) & 0xffff);
 #pragma unroll
   for (int r = 0; r < 2; ++r) {
-    if (len[r] >= kLongList) {
+    if (dense[r]) {
+      s_base[kHubChunk - 1 - dslot] = st[r];
+      ++dslot;
+    } else if (len[r] >= kLongList) {
       s_base[lslot] = st[r];
       s_off[lslot] = len[r];
       ++lslot;
@@ -228,10 +253,10 @@ __device__ __forceinline__ Partners find_partners(const CountArgs &a, int x, int
       off += len[r];
     }
   }
-  const int total = (int)(unsigned)all;
+  const int total = (int)(all & 0xffff);
   if (threadIdx.x == 0) s_off[nl + ns] = total;
   __syncthreads();
-  return Partners{nl, total};
+  return Partners{nl, total, nd};
 }
 
 // One warp streams one list lists[st, st + len) with lane-per-element loads
@@ -291,21 +316,57 @@ __device__ __forceinline__ unsigned stream_short(const int32_t *__restrict__ lis
   return hits;
 }
 
-// All partner lists of the task: the long ones claimed a list at a time by
-// the warps, then the short stream.  Returns this thread's hits.
+// |N+(owner) & N+(y)| for a dense partner y of rank ry: the AND of the
+// owner's bitmap (shared memory, cleared to whole quads past its rank) and
+// y's core bitmap over the quads below both ranks, lane-per-quad (16-byte
+// loads: 512 bytes per instruction, no bank conflict), 2 loads in flight.
+__device__ __forceinline__ unsigned and_count(const unsigned *bits, int owner_bits,
+                                              const unsigned *__restrict__ core, int ry,
+                                              int lane) {
+  const uint4 *q = reinterpret_cast<const uint4 *>(core + core_offset(ry));
+  const uint4 *o = reinterpret_cast<const uint4 *>(bits);
+  const int quads = (min(ry, owner_bits) + 127) >> 7;
+  unsigned h = 0;
+  for (int base = 0; base < quads; base += 2 * kWarp) {
+    uint4 v[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int k = base + u * kWarp + lane;
+      v[u] = k < quads ? __ldg(q + k) : make_uint4(0, 0, 0, 0);
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int k = base + u * kWarp + lane;
+      const uint4 w = o[k < quads ? k : 0];
+      h += __popc(w.x & v[u].x) + __popc(w.y & v[u].y) + __popc(w.z & v[u].z) +
+           __popc(w.w & v[u].w);
+    }
+  }
+  return h;
+}
+
+// All partner lists of the task: the long ones and the dense partners
+// claimed one at a time by the warps, then the short stream.  Returns this
+// thread's hits.
 template <class Probe>
 __device__ __forceinline__ unsigned long long stream_partners(const int32_t *__restrict__ lists,
                                                               const long long *s_base,
                                                               const int *s_off, Partners pt,
                                                               int *s_next, int warp, int lane,
-                                                              const Probe &probe) {
+                                                              const Probe &probe,
+                                                              const unsigned *bits = nullptr,
+                                                              int owner_bits = 0,
+                                                              const unsigned *core = nullptr) {
   unsigned long long hits = 0;
   for (;;) {
     int j = 0;
     if (lane == 0) j = atomicAdd(s_next, 1);
     j = __shfl_sync(kFull, j, 0);
-    if (j >= pt.nl) break;
-    hits += stream_one(lists, s_base[j], s_off[j], lane, probe);
+    if (j >= pt.nl + pt.nd) break;
+    if (j < pt.nl)
+      hits += stream_one(lists, s_base[j], s_off[j], lane, probe);
+    else
+      hits += and_count(bits, owner_bits, core, (int)s_base[kHubChunk - 1 - (j - pt.nl)], lane);
   }
   if (pt.total > 0)
     hits += stream_short(lists, s_base + pt.nl, s_off + pt.nl, pt.total, warp, lane, probe);
@@ -387,7 +448,9 @@ __global__ void __launch_bounds__(kCountThreads, 5) tc_hub_kernel(CountArgs a) {
     } else if (use_table) {
       for (int i = threadIdx.x; i < (1 << lg) / 4; i += blockDim.x) t4[i] = make_int4(-1, -1, -1, -1);
     }
-    const Partners pt = find_partners(a, x, d, e0, nc, s_base, s_off, s_warp);
+    // Dense partners need the owner's bitmap and the core bitmaps.
+    const int owner_bits = bitmap && a.core ? R : 0;
+    const Partners pt = find_partners(a, x, d, e0, nc, s_base, s_off, s_warp, owner_bits);
     // N+(x) into shared memory.
     if (bitmap) {
       unsigned *bits = reinterpret_cast<unsigned *>(table);
@@ -407,7 +470,8 @@ __global__ void __launch_bounds__(kCountThreads, 5) tc_hub_kernel(CountArgs a) {
     unsigned long long th = 0;
     if (bitmap)
       th = stream_partners(a.dag_rank, s_base, s_off, pt, &s_next, warp, lane,
-                           BitmapProbe{reinterpret_cast<const unsigned *>(table), (unsigned)R});
+                           BitmapProbe{reinterpret_cast<const unsigned *>(table), (unsigned)R},
+                           reinterpret_cast<const unsigned *>(table), R, a.core);
     else if (use_table)
       th = stream_partners(a.dag_col, s_base, s_off, pt, &s_next, warp, lane,
                            CuckooProbe{table, shift});
@@ -598,6 +662,9 @@ int tc_count_launch(mc_dgraph *g, cudaEvent_t after_hub, int shard, int num_shar
   const bool ranked = g->rank != nullptr && g->batch.gid == nullptr;
   a.rank = ranked ? g->rank : nullptr;
   a.dag_rank = ranked ? g->dag_rank : nullptr;
+  a.core = ranked && g->core_used > 0 ? g->core_bits : nullptr;
+  a.core_ranks = a.core ? g->core_used : 0;
+  a.dense_factor = g->dense_factor;
   MC_CUDA_TRY(cudaFuncSetAttribute(tc_hub_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)big_smem));
   a.table_log2_max = small_lg;

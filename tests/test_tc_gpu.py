@@ -122,6 +122,36 @@ def test_hub_bitmap_and_table_paths_agree(monkeypatch, make, cap):
         assert d.tc_count() == want
 
 
+@pytest.mark.parametrize("core", ["0", "1", "64", "1000", "32768", "262144"])
+@pytest.mark.parametrize("make", [lambda: Graph.rmat(16, 16, seed=31),
+                                  lambda: Graph.chung_lu(80000, 2.1, 24.0, 8000.0, seed=32),
+                                  lambda: fixture("dense400"),
+                                  lambda: fixture("k5")])
+def test_dense_partners_by_core_bitmap_and(monkeypatch, make, core):
+    """Long partners among the core ranks are intersected by a word-wise AND
+    of the owner's bitmap with the partner's core bitmap; moving the core
+    boundary (0: probes only) never changes the count."""
+    g = make()
+    want = orc.tc(g.rowptr, g.col)
+    monkeypatch.setenv("MERCURY_TC_CORE_RANKS", core)
+    with DeviceGraph(g) as d:
+        assert d.tc_count() == want
+        assert d.tc_count() == want
+        assert sum(d.tc_count_shard(s, 3) for s in range(3)) == want
+
+
+@pytest.mark.parametrize("bits", ["0", "700", "5000"])
+def test_dense_partners_with_mixed_owner_kinds(monkeypatch, bits):
+    """Owners above the bitmap cap use tables and never take the AND path;
+    the owners below it do; both kinds in one count give the oracle's."""
+    g = Graph.rmat(15, 24, seed=33)
+    want = orc.tc(g.rowptr, g.col)
+    monkeypatch.setenv("MERCURY_TC_BITMAP_BITS", bits)
+    monkeypatch.setenv("MERCURY_TC_CORE_RANKS", "4096")
+    with DeviceGraph(g) as d:
+        assert d.tc_count() == want
+
+
 def test_empty_and_edgeless_graphs():
     with DeviceGraph(np.zeros(1, dtype=np.int64), np.zeros(0, dtype=np.int32)) as d:
         assert d.tc_count() == 0
