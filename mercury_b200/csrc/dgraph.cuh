@@ -74,6 +74,9 @@ struct mc_dgraph {
   // ---- triangle-count scratch, allocated on the first mc_tc_count -------
   bool tc_ready = false;
   int2 *key = nullptr;            // n      {symmetric degree, DAG out-degree}
+  // n: {d+, rank (INT_MAX without ranks), DAG row start low, high}: what a
+  // hub task needs of a neighbour, in one 16-byte load.
+  int4 *pinfo = nullptr;
   int64_t *dag_rowptr = nullptr;  // n + 1
   int32_t *dag_col = nullptr;     // dag_cap (m+ used)
   int64_t dag_cap = 0;            // nnz; nnz / 2 + 1 with host columns

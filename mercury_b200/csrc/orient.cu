@@ -21,6 +21,7 @@
 //   B  DAG entries and row offsets written from the keep masks
 // Each vertex's (degree, d+) pair is one 8-byte word (key[]).
 #include <algorithm>
+#include <climits>
 #include <cstdio>
 #include <cstdlib>
 
@@ -367,6 +368,17 @@ __global__ void core_bits_kernel(const unsigned long long *__restrict__ sorted, 
   }
 }
 
+// pinfo[v] = {d+(v), rank(v) (INT_MAX without ranks), dag_rowptr[v]}.
+__global__ void partner_info_kernel(const int2 *__restrict__ key, const int32_t *__restrict__ rank,
+                                    const int64_t *__restrict__ dag_rowptr, int64_t n,
+                                    int4 *__restrict__ pinfo) {
+  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n) return;
+  const long long st = dag_rowptr[v];
+  pinfo[v] = make_int4(key[v].y, rank ? rank[v] : INT_MAX, (int)(unsigned)(st & 0xffffffffll),
+                       (int)(st >> 32));
+}
+
 // key[v] = {degree, 0}; deg[v] = degree alone (4 bytes per gather in pass A).
 __global__ void init_key_kernel(const int64_t *rowptr, int64_t n, int2 *key, int32_t *deg) {
   const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -544,7 +556,7 @@ int64_t tc_device_bytes(int64_t n, int64_t nnz, bool col_host) {
                                          radix_temp_bytes(n));
   const int64_t staging =
       col_host ? 2 * 4 * stage_capacity(nnz) + 8 * (stage_capacity(nnz) / kTileEdges + 1) : 0;
-  return (n + 1) * (8 + 8 + 3 * 4 + 3 * 8 + 4 + 16) + 3 * 8 * tasks +
+  return (n + 1) * (8 + 16 + 8 + 3 * 4 + 3 * 8 + 4 + 16) + 3 * 8 * tasks +
          2 * 4 * dag_capacity(nnz, col_host) + tiles * (2 * kTileThreads + 12) +
          2 * 12 * (radix_entries(n) + 1) + scan + staging + 4 * core_offset(core_rank_count(n));
 }
@@ -562,6 +574,7 @@ int tc_alloc(mc_dgraph *g) {
 #define MC_ALLOC(ptr, count) \
   MC_CUDA_TRY(dev_alloc((void **)&(ptr), sizeof(*(ptr)) * (size_t)(count), g->stream))
   MC_ALLOC(g->key, n + 1);
+  MC_ALLOC(g->pinfo, n + 1);
   MC_ALLOC(g->dag_rowptr, n + 1);
   MC_ALLOC(g->dag_col, g->dag_cap);
   MC_ALLOC(g->keep, tiles * kTileThreads);
@@ -702,6 +715,10 @@ int tc_orient(mc_dgraph *g) {
     MC_CUDA_TRY(cudaGetLastError());
     g->launches += 1;
   }
+  partner_info_kernel<<<grid_for(n, 256), 256, 0, s>>>(
+      g->key, g->batch.gid ? nullptr : g->rank, g->dag_rowptr, n, g->pinfo);
+  MC_CUDA_TRY(cudaGetLastError());
+  g->launches += 1;
   task_count_kernel<<<grid_for(n, 256), 256, 0, s>>>(g->key, n, g->hub_cnt, g->leaf_cnt,
                                                      g->mega_cnt, g->counters + 3, g->batch);
   MC_CUDA_TRY(cudaGetLastError());

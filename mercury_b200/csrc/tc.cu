@@ -31,6 +31,7 @@ struct CountArgs {
   const int64_t *__restrict__ rowptr;      // symmetric CSR
   const int32_t *__restrict__ col;
   const int2 *__restrict__ key;            // {deg, d+}
+  const int4 *__restrict__ pinfo;          // {d+, rank, DAG row start (2 words)}
   const int64_t *__restrict__ dag_rowptr;  // N+ lists
   const int32_t *__restrict__ dag_col;
   const uint64_t *__restrict__ tasks;
@@ -196,16 +197,17 @@ __device__ __forceinline__ Partners find_partners(const CountArgs &a, int x, int
     const int i = 2 * threadIdx.x + r;
     if (i < nc) {
       const int y = __ldg(a.col + e0 + i);
-      const int py = __ldg(&a.key[y].y);
+      const int4 pi = __ldg(a.pinfo + y);
+      const int py = pi.x;
       if (owns(x, px, y, py)) {
         len[r] = py;
         if (py >= kLongList && owner_bits > 0) {
-          const int ry = __ldg(a.rank + y);
+          const int ry = pi.y;
           const int words = (min(ry, owner_bits) + 31) >> 5;
           dense[r] = ry < a.core_ranks && words <= a.dense_factor * py;
           if (dense[r]) st[r] = ry;
         }
-        if (!dense[r]) st[r] = __ldg(a.dag_rowptr + y);
+        if (!dense[r]) st[r] = ((long long)pi.w << 32) | (unsigned)pi.z;
       }
     }
   }
@@ -259,26 +261,33 @@ __device__ __forceinline__ Partners find_partners(const CountArgs &a, int x, int
   return Partners{nl, total, nd};
 }
 
-// One warp streams one list lists[st, st + len) with lane-per-element loads
-// (128 bytes per instruction): every load of a 128-element batch is issued
-// before the first probe.  Entries past the end probe as kNoKey, which costs
-// less than a branch per 32-entry group (batch depth 4 measured best of
-// 2, 3, 4, 6, 8 at RMAT scale 22).
-template <class Probe>
-__device__ __forceinline__ unsigned stream_one(const int32_t *__restrict__ lists, long long st,
-                                               int len, int lane, const Probe &probe) {
+// One warp streams N lists lists[st[i], st[i] + len[i]) together with
+// lane-per-element loads (128 bytes per instruction): every load of a
+// 128-element batch of every list is issued before the first probe, so a
+// warp keeps 4 N loads in flight per lane.  Entries past a list's end probe
+// as kNoKey, which costs less than a branch per 32-entry group.  Batch depth
+// 4 with N = 2 measured best (depths 2..8 with N = 1, N = 3 slower, and
+// 16-byte loads slower still, at RMAT scale 22).
+template <int N, class Probe>
+__device__ __forceinline__ unsigned stream_n(const int32_t *__restrict__ lists, const long long *st,
+                                             const int *len, int lane, const Probe &probe) {
   constexpr int kB = 4;
-  const int32_t *p = lists + st;
+  int mx = 0;
+#pragma unroll
+  for (int i = 0; i < N; ++i) mx = max(mx, len[i]);
   unsigned h = 0;
-  for (int base = 0; base < len; base += kB * kWarp) {
-    int w[kB];
+  for (int base = 0; base < mx; base += kB * kWarp) {
+    int w[N][kB];
 #pragma unroll
     for (int u = 0; u < kB; ++u) {
       const int k = base + u * kWarp + lane;
-      w[u] = k < len ? __ldg(p + k) : kNoKey;
+#pragma unroll
+      for (int i = 0; i < N; ++i) w[i][u] = k < len[i] ? __ldg(lists + st[i] + k) : kNoKey;
     }
 #pragma unroll
-    for (int u = 0; u < kB; ++u) h += probe(w[u]);
+    for (int u = 0; u < kB; ++u)
+#pragma unroll
+      for (int i = 0; i < N; ++i) h += probe(w[i][u]);
   }
   return h;
 }
@@ -316,38 +325,50 @@ __device__ __forceinline__ unsigned stream_short(const int32_t *__restrict__ lis
   return hits;
 }
 
-// |N+(owner) & N+(y)| for a dense partner y of rank ry: the AND of the
-// owner's bitmap (shared memory, cleared to whole quads past its rank) and
-// y's core bitmap over the quads below both ranks, lane-per-quad (16-byte
-// loads: 512 bytes per instruction, no bank conflict), 2 loads in flight.
-__device__ __forceinline__ unsigned and_count(const unsigned *bits, int owner_bits,
-                                              const unsigned *__restrict__ core, int ry,
-                                              int lane) {
-  const uint4 *q = reinterpret_cast<const uint4 *>(core + core_offset(ry));
+// |N+(owner) & N+(y)| summed over N dense partners y of ranks ry[i] (-1:
+// none): the AND of the owner's bitmap (shared memory, cleared to whole
+// quads past its rank) and each y's core bitmap over the quads below both
+// ranks, lane-per-quad (16-byte loads: 512 bytes per instruction, no bank
+// conflict), 2 N loads in flight per lane (N = 4 measured best of 1, 2, 4).
+template <int N>
+__device__ __forceinline__ unsigned and_count_n(const unsigned *bits, int owner_bits,
+                                                const unsigned *__restrict__ core, const int *ry,
+                                                int lane) {
   const uint4 *o = reinterpret_cast<const uint4 *>(bits);
-  const int quads = (min(ry, owner_bits) + 127) >> 7;
+  const uint4 *q[N];
+  int nq[N];
+  int mx = 0;
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    q[i] = reinterpret_cast<const uint4 *>(core + core_offset(max(ry[i], 0)));
+    nq[i] = ry[i] >= 0 ? (min(ry[i], owner_bits) + 127) >> 7 : 0;
+    mx = max(mx, nq[i]);
+  }
   unsigned h = 0;
-  for (int base = 0; base < quads; base += 2 * kWarp) {
-    uint4 v[2];
+  for (int base = 0; base < mx; base += 2 * kWarp) {
+    uint4 v[N][2];
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
       const int k = base + u * kWarp + lane;
-      v[u] = k < quads ? __ldg(q + k) : make_uint4(0, 0, 0, 0);
+#pragma unroll
+      for (int i = 0; i < N; ++i) v[i][u] = k < nq[i] ? __ldg(q[i] + k) : make_uint4(0, 0, 0, 0);
     }
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
       const int k = base + u * kWarp + lane;
-      const uint4 w = o[k < quads ? k : 0];
-      h += __popc(w.x & v[u].x) + __popc(w.y & v[u].y) + __popc(w.z & v[u].z) +
-           __popc(w.w & v[u].w);
+      const uint4 w = o[k < mx ? k : 0];
+#pragma unroll
+      for (int i = 0; i < N; ++i)
+        h += __popc(w.x & v[i][u].x) + __popc(w.y & v[i][u].y) + __popc(w.z & v[i][u].z) +
+             __popc(w.w & v[i][u].w);
     }
   }
   return h;
 }
 
-// All partner lists of the task: the long ones and the dense partners
-// claimed one at a time by the warps, then the short stream.  Returns this
-// thread's hits.
+// All partner lists of the task: the long ones (two per claim) and the
+// dense partners (four per claim) claimed by the warps, then the short
+// stream.  Returns this thread's hits.
 template <class Probe>
 __device__ __forceinline__ unsigned long long stream_partners(const int32_t *__restrict__ lists,
                                                               const long long *s_base,
@@ -358,15 +379,32 @@ __device__ __forceinline__ unsigned long long stream_partners(const int32_t *__r
                                                               int owner_bits = 0,
                                                               const unsigned *core = nullptr) {
   unsigned long long hits = 0;
+  constexpr int kNL = 2, kND = 4;
+  const int lp = (pt.nl + kNL - 1) / kNL, dp = (pt.nd + kND - 1) / kND;
   for (;;) {
     int j = 0;
     if (lane == 0) j = atomicAdd(s_next, 1);
     j = __shfl_sync(kFull, j, 0);
-    if (j >= pt.nl + pt.nd) break;
-    if (j < pt.nl)
-      hits += stream_one(lists, s_base[j], s_off[j], lane, probe);
-    else
-      hits += and_count(bits, owner_bits, core, (int)s_base[kHubChunk - 1 - (j - pt.nl)], lane);
+    if (j >= lp + dp) break;
+    if (j < lp) {
+      long long st[kNL];
+      int len[kNL];
+#pragma unroll
+      for (int i = 0; i < kNL; ++i) {
+        const int a = kNL * j + i;
+        st[i] = a < pt.nl ? s_base[a] : 0;
+        len[i] = a < pt.nl ? s_off[a] : 0;
+      }
+      hits += stream_n<kNL>(lists, st, len, lane, probe);
+    } else {
+      int ry[kND];
+#pragma unroll
+      for (int i = 0; i < kND; ++i) {
+        const int a = kND * (j - lp) + i;
+        ry[i] = a < pt.nd ? (int)s_base[kHubChunk - 1 - a] : -1;
+      }
+      hits += and_count_n<kND>(bits, owner_bits, core, ry, lane);
+    }
   }
   if (pt.total > 0)
     hits += stream_short(lists, s_base + pt.nl, s_off + pt.nl, pt.total, warp, lane, probe);
@@ -419,15 +457,19 @@ __global__ void __launch_bounds__(kCountThreads, 5) tc_hub_kernel(CountArgs a) {
   const int lane = threadIdx.x & (kWarp - 1), warp = threadIdx.x / kWarp;
   const int64_t ntasks = shard_tasks(a);
   unsigned long long hits = 0;
+  // Thread 0 claims each task one task ahead, so the queue atomic's latency
+  // overlaps the current task.
+  unsigned long long t_next = 0;
+  if (threadIdx.x == 0) s_task = atomicAdd(a.queue, 1ull);
   for (;;) {
     if (threadIdx.x == 0) {
-      s_task = atomicAdd(a.queue, 1ull);
       s_fail = 0;
       s_next = 0;
     }
     __syncthreads();
     const unsigned long long t = s_task;
     if ((int64_t)t >= ntasks) break;
+    if (threadIdx.x == 0) t_next = atomicAdd(a.queue, 1ull);
     const uint64_t task = shard_task(a, t);
     const int x = (int)(task >> 32);
     const int chunk = (int)(task & 0xffffffffu);
@@ -448,20 +490,38 @@ __global__ void __launch_bounds__(kCountThreads, 5) tc_hub_kernel(CountArgs a) {
     } else if (use_table) {
       for (int i = threadIdx.x; i < (1 << lg) / 4; i += blockDim.x) t4[i] = make_int4(-1, -1, -1, -1);
     }
+    // The owner's first kOwnAhead x 256 out-list entries are loaded now and
+    // stored after the partner scan (whose barriers also order them after
+    // the clear), so their loads overlap the scan's.
+    constexpr int kOwnAhead = 4;
+    int own[kOwnAhead];
+    const int32_t *own_list = bitmap ? a.dag_rank + a0 : a.dag_col + a0;
+#pragma unroll
+    for (int r = 0; r < kOwnAhead; ++r) {
+      const int i = threadIdx.x + r * kCountThreads;
+      own[r] = (bitmap || use_table) && i < d ? __ldg(own_list + i) : -1;
+    }
     // Dense partners need the owner's bitmap and the core bitmaps.
     const int owner_bits = bitmap && a.core ? R : 0;
     const Partners pt = find_partners(a, x, d, e0, nc, s_base, s_off, s_warp, owner_bits);
     // N+(x) into shared memory.
     if (bitmap) {
       unsigned *bits = reinterpret_cast<unsigned *>(table);
-      for (int i = threadIdx.x; i < d; i += blockDim.x) {
-        const unsigned r = (unsigned)__ldg(a.dag_rank + a0 + i);
+      auto set = [&](unsigned r) {
         if (r < (unsigned)R) atomicOr(bits + (r >> 5), 1u << (r & 31));
         else atomicOr(a.err, kErrRank);  // never written outside the bitmap
-      }
+      };
+#pragma unroll
+      for (int r = 0; r < kOwnAhead; ++r)
+        if (own[r] >= 0) set((unsigned)own[r]);
+      for (int i = threadIdx.x + kOwnAhead * kCountThreads; i < d; i += blockDim.x)
+        set((unsigned)__ldg(a.dag_rank + a0 + i));
     } else if (use_table) {
       bool ok = true;
-      for (int i = threadIdx.x; i < d; i += blockDim.x)
+#pragma unroll
+      for (int r = 0; r < kOwnAhead; ++r)
+        if (own[r] >= 0) ok &= cuckoo_insert(table, shift, own[r]);
+      for (int i = threadIdx.x + kOwnAhead * kCountThreads; i < d; i += blockDim.x)
         ok &= cuckoo_insert(table, shift, __ldg(a.dag_col + a0 + i));
       if (!ok) s_fail = 1;
     }
@@ -480,6 +540,7 @@ __global__ void __launch_bounds__(kCountThreads, 5) tc_hub_kernel(CountArgs a) {
                            ListProbe{a.dag_col + a0, d});
     hits += th;
     flush_task(a, x, th, lane);
+    if (threadIdx.x == 0) s_task = t_next;  // every thread read s_task two barriers ago
     __syncthreads();  // shared memory is rewritten by the next task
   }
   hits = warp_sum_u64(hits);
@@ -561,18 +622,18 @@ __global__ void __launch_bounds__(kCountThreads) tc_leaf_kernel(CountArgs a) {
   LeafTask cur = leaf_fetch(a, ntasks, next_ticket(), lane);
   while (cur.valid) {
     // Partners of the current chunk: d+ of each neighbour, then the list start.
-    int py[2];
+    int4 pi[2];
 #pragma unroll
-    for (int r = 0; r < 2; ++r) py[r] = cur.y[r] >= 0 ? __ldg(&a.key[cur.y[r]].y) : 0;
+    for (int r = 0; r < 2; ++r) pi[r] = cur.y[r] >= 0 ? __ldg(a.pinfo + cur.y[r]) : make_int4(0, 0, 0, 0);
     // The next task (claimed while those loads are in flight).
     const unsigned long long tn = next_ticket();
     int64_t pst[2] = {0, 0};
     int plen[2] = {0, 0};
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
-      if (cur.y[r] >= 0 && owns(cur.x, cur.d, cur.y[r], py[r])) {
-        pst[r] = __ldg(a.dag_rowptr + cur.y[r]);
-        plen[r] = py[r];
+      if (cur.y[r] >= 0 && owns(cur.x, cur.d, cur.y[r], pi[r].x)) {
+        pst[r] = ((long long)pi[r].w << 32) | (unsigned)pi[r].z;
+        plen[r] = pi[r].x;
       }
     }
     // The next task's owner row, out-list and neighbours.
@@ -640,6 +701,7 @@ int tc_count_launch(mc_dgraph *g, cudaEvent_t after_hub, int shard, int num_shar
   a.rowptr = g->rowptr;
   a.col = g->col;
   a.key = g->key;
+  a.pinfo = g->pinfo;
   a.dag_rowptr = g->dag_rowptr;
   a.dag_col = g->dag_col;
   a.result = g->counters + 0;
