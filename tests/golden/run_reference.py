@@ -19,7 +19,9 @@ CPU, the limits that kernel's fixed buffers assume
 (gpu_kernels/tc_challenge.cuh:4-192, tc_challenge.cu:93-101): DAG
 out-degree of every large-task vertex <= 4096 (shared-memory table) and at
 most 64 out-neighbours per hash bin (uid % 1019) -- a graph that breaks them
-is skipped, not run.
+is skipped, not run.  Graphs with a DAG out-degree of 1019 or more are
+skipped too: the reference's hash kernel faulted on such graphs on a B200
+(see reference_tc_limits_ok).
 """
 from __future__ import annotations
 
@@ -62,6 +64,15 @@ def reference_tc_limits_ok(rowptr, col):
     dplus = np.diff(drp)
     if dplus.max(initial=0) > 4096:
         return False, f"max d+ {int(dplus.max())} > 4096"
+    # The hash kernel packs each bin's offset from shared_bucket[0..1019) and
+    # then, with no barrier between the two loops, overwrites shared_bucket
+    # from index 0 with the table (gpu_kernels/tc_challenge.cuh:76-94); a
+    # warp still packing can read a vertex id as an offset.  On a B200 it
+    # raised an illegal memory access (error 700 at tc_challenge.cu:103) on
+    # RMAT scale 22 (max d+ 1032, third of three runs) and scale 24 (max d+
+    # 1746, first run), so graphs whose owners reach d+ 1019 are not run.
+    if dplus.max(initial=0) >= 1019:
+        return False, f"max d+ {int(dplus.max())} >= 1019: the reference kernel faulted at such sizes"
     src = np.repeat(np.arange(n, dtype=np.int64), dplus)
     big = dplus[src] > 128  # only vertices reaching the hash kernel matter
     if big.any():
