@@ -76,10 +76,60 @@ __device__ __forceinline__ bool bsearch(const int32_t *list, int len, int key) {
   return false;
 }
 
+// Per-warp hash set in shared memory: one table of kSetSlots ints (open
+// addressing, linear probing) holding at most kSetMax distinct keys (load
+// <= 1/2), each tagged 0 or 1: a key k is stored as k (tag 0) or -(k + 2)
+// (tag 1), and -1 marks an empty slot, so two disjoint sets share the
+// table.  Sets larger than that take the binary-search forms below.
+constexpr int kSetSlots = 1024;
+constexpr int kSetMax = kSetSlots / 2;
+constexpr int kSetShift = 32 - 10;
+static_assert((1 << (32 - kSetShift)) == kSetSlots, "set hash width");
+
+struct WarpSet {
+  int *tab;
+  __device__ __forceinline__ static unsigned slot(int key) {
+    return ((unsigned)key * 2654435769u) >> kSetShift;
+  }
+  __device__ void clear(int lane) const {
+    int4 *t4 = reinterpret_cast<int4 *>(tab);
+    for (int i = lane; i < kSetSlots / 4; i += kWarp) t4[i] = make_int4(-1, -1, -1, -1);
+    __syncwarp();
+  }
+  // Inserts list[0, n) with the given tag (keys distinct from every key
+  // already present; at most kSetMax keys in all).
+  __device__ void insert(const int32_t *list, int n, int tag, int lane) const {
+    for (int i = lane; i < n; i += kWarp) {
+      const int key = list[i];
+      const int code = tag ? -(key + 2) : key;
+      unsigned sl = slot(key);
+      for (int probe = 0; probe < kSetSlots; ++probe) {
+        if (atomicCAS(tab + sl, -1, code) == -1) break;
+        sl = (sl + 1) & (kSetSlots - 1);
+      }
+    }
+    __syncwarp();
+  }
+  // 0: absent, 1: present with tag 0, 2: present with tag 1.
+  __device__ __forceinline__ int lookup(int key) const {
+    const int alt = -(key + 2);
+    unsigned sl = slot(key);
+    for (int probe = 0; probe < kSetSlots; ++probe) {
+      const int v = tab[sl];
+      if (v == key) return 1;
+      if (v == alt) return 2;
+      if (v == -1) return 0;
+      sl = (sl + 1) & (kSetSlots - 1);
+    }
+    return 0;
+  }
+};
+
 struct Warp {
   const int64_t *__restrict__ rp;
   const int32_t *__restrict__ ci;
   int lane;
+  int *H = nullptr;  // this warp's kSetSlots-int set table (null: none)
   __device__ __forceinline__ int deg(int v) const { return (int)(__ldg(rp + v + 1) - __ldg(rp + v)); }
   __device__ __forceinline__ const int32_t *N(int v) const { return ci + __ldg(rp + v); }
   // x in N(k), searched in k's list.
@@ -138,6 +188,28 @@ struct Warp {
 struct Acc {
   unsigned long long c1 = 0, c2 = 0;
 };
+
+__device__ __forceinline__ int ceil_log2_int(int v) { return v <= 1 ? 1 : 32 - __clz(v - 1); }
+
+// |N(x) & S| by the whole warp (every lane gets the total), S the set's
+// tag-0 keys and also given as its list of nS entries: lanes stream
+// N(x) probing the set (ceil(d / 32) steps), or search S's entries in N(x)
+// (ceil(nS / 32) binary searches), whichever takes fewer warp steps.
+__device__ __forceinline__ int warp_common(const Warp &w, int x, const WarpSet &S,
+                                           const int32_t *list, int nS) {
+  const int32_t *p = w.N(x);
+  const int d = w.deg(x);
+  int c = 0;
+  if ((d + kWarp - 1) / kWarp <= ((nS + kWarp - 1) / kWarp) * ceil_log2_int(d)) {
+    for (int k = w.lane; k < d; k += kWarp) c += S.lookup(__ldg(p + k)) == 1;
+  } else {
+    for (int k = w.lane; k < nS; k += kWarp) c += bsearch(p, d, list[k]);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
+  return c;
+}
+
 
 // freq[j] = #{i > j : a[j] not in N(a[i])}   (P3 :280-292, P7 :386-398)
 __device__ void pair_freq(const Warp &w, const int32_t *a, int na, int32_t *freq) {
@@ -249,6 +321,57 @@ __device__ void edge_pattern(const Warp &w, int v0, int v1, int32_t *L, int64_t 
     const int nA = w.inter(n0, d0, v1, -1, L0);
     const int nB = w.diff(n0, d0, v1, -1, L1);
     const int nC = w.diff(n1, d1, v0, -1, L2);
+    if (w.H && nA + nC <= kSetMax && nB <= kSetMax) {
+      // The same per-edge terms through the hash set.  For b in B the
+      // reference's f = #{a in A : b not in N(a)} = nA - |N(b) & A| and
+      // t = #{c in C : c not in N(b)} = nC - |N(b) & C| (the graph is
+      // symmetric): one lane per b walks N(b) once for both, A and C
+      // sharing the table with tags 0 and 1 (they are disjoint), or
+      // searches A and C in N(b) when that is shorter.
+      const WarpSet s0{w.H};
+      if (nA > 0) {  // with A empty every f is 0
+        s0.clear(w.lane);
+        s0.insert(L0, nA, 0, w.lane);
+        s0.insert(L2, nC, 1, w.lane);
+        for (int j = w.lane; j < nB; j += kWarp) {
+          const int b = L1[j];
+          const int32_t *p = w.N(b);
+          const int db = w.deg(b);
+          int ca = 0, cc = 0;
+          if (db <= (nA + nC) * ceil_log2_int(db)) {
+            for (int k = 0; k < db; ++k) {
+              const int r = s0.lookup(__ldg(p + k));
+              ca += r == 1;
+              cc += r == 2;
+            }
+          } else {
+            for (int k = 0; k < nA; ++k) ca += bsearch(p, db, L0[k]);
+            for (int k = 0; k < nC; ++k) cc += bsearch(p, db, L2[k]);
+          }
+          const int f = nA - ca;
+          if (f) acc.c1 += wrap_mul(nC - cc, f);
+        }
+        __syncwarp();
+      }
+      // Correction: for v2 in A, D = C & N(v2), E = B - N(v2), and
+      // #{e in E : e not in N(c)} = nE - |N(c) & E| for c in D (the whole
+      // warp per c: D is short).
+      for (int i = 0; i < nA; ++i) {
+        const int v2 = L0[i];
+        const int nD = w.inter(L2, nC, v2, -1, L3);
+        if (nD == 0) continue;
+        const int nE = w.diff(L1, nB, v2, -1, L4);
+        s0.clear(w.lane);
+        s0.insert(L4, nE, 0, w.lane);
+        for (int j = 0; j < nD; ++j) {
+          const int common = warp_common(w, L3[j], s0, L4, nE);
+          if (w.lane == 0) acc.c2 += (unsigned long long)(nE - common);
+        }
+        __syncwarp();
+      }
+      __syncwarp();
+      return;
+    }
     // freq over B of the A vertices not adjacent to it
     for (int j = w.lane; j < nB; j += kWarp) {
       const int x = L1[j];
@@ -345,10 +468,11 @@ __device__ void vertex_star(const Warp &w, int v0, int32_t *L, Acc &acc) {
 // from the queue one at a time.
 template <int P, bool kStar>
 __global__ void __launch_bounds__(kPatThreads) pattern_kernel(PatArgs a) {
+  __shared__ __align__(16) int s_sets[kPatThreads / kWarp][kSetSlots];
   const int lane = threadIdx.x & (kWarp - 1);
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
   int32_t *L = a.scratch + gw * kLists * a.cap;
-  const Warp w{a.rp, a.ci, lane};
+  const Warp w{a.rp, a.ci, lane, s_sets[threadIdx.x / kWarp]};
   const int64_t all = kStar ? a.n : (a.task_off ? a.task_off[a.n] : a.nnz);
   const int64_t ntasks = all > a.shard ? (all - a.shard + a.num_shards - 1) / a.num_shards : 0;
   Acc acc;
@@ -442,8 +566,6 @@ __device__ __forceinline__ unsigned full_word(int k, int d) {
   const int b = d - 32 * k;
   return b >= 32 ? ~0u : (b <= 0 ? 0u : ((1u << b) - 1u));
 }
-
-__device__ __forceinline__ int ceil_log2_int(int v) { return v <= 1 ? 1 : 32 - __clz(v - 1); }
 
 // Position of y in the sorted n0[0, d0), or -1.
 __device__ __forceinline__ int find_pos(const int32_t *n0, int d0, int y) {
@@ -942,10 +1064,11 @@ __device__ __forceinline__ void batch_edge(const Warp &w, int v0, int v1, int32_
 // tasks (one per vertex of every P1 graph), then one task per directed edge
 // of every pattern graph; each task's counters go to its own graph.
 __global__ void __launch_bounds__(kPatThreads) batch_pattern_kernel(BatchPatternArgs b) {
+  __shared__ __align__(16) int s_sets[kPatThreads / kWarp][kSetSlots];
   const int lane = threadIdx.x & (kWarp - 1);
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
   int32_t *L = b.scratch + gw * kLists * b.cap;
-  const Warp w{b.rp, b.ci, lane};
+  const Warp w{b.rp, b.ci, lane, s_sets[threadIdx.x / kWarp]};
   const int64_t n_star = b.star_off[b.num_graphs], n_edge = b.edge_off[b.num_graphs];
   for (;;) {
     unsigned long long t = 0;
