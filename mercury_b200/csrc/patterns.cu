@@ -57,6 +57,9 @@ struct PatArgs {
   // Shard `shard` of `num_shards` takes queue positions t -> task
   // t * num_shards + shard (partial counts of all shards sum to the count).
   int shard = 0, num_shards = 1;
+  // 0: the binary-search forms only (MERCURY_PATTERN_SETS=0; tests compare
+  // both forms with it).
+  int use_sets = 1;
 };
 
 __device__ __forceinline__ unsigned long long wrap_mul(int a, int b) {
@@ -130,6 +133,7 @@ struct Warp {
   const int32_t *__restrict__ ci;
   int lane;
   int *H = nullptr;  // this warp's kSetSlots-int set table (null: none)
+  unsigned *M = nullptr;  // this warp's 32 words of row masks
   __device__ __forceinline__ int deg(int v) const { return (int)(__ldg(rp + v + 1) - __ldg(rp + v)); }
   __device__ __forceinline__ const int32_t *N(int v) const { return ci + __ldg(rp + v); }
   // x in N(k), searched in k's list.
@@ -188,6 +192,17 @@ struct Warp {
 struct Acc {
   unsigned long long c1 = 0, c2 = 0;
 };
+
+// Index of y in the ascending list[0, n) (y present).
+__device__ __forceinline__ int pos_of(const int32_t *list, int n, int y) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (list[mid] < y) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
 
 __device__ __forceinline__ int ceil_log2_int(int v) { return v <= 1 ? 1 : 32 - __clz(v - 1); }
 
@@ -424,6 +439,72 @@ __device__ void edge_pattern(const Warp &w, int v0, int v1, int32_t *L, int64_t 
   } else if (P == 8) {  // P8_subgraph_matching (:461-572)
     const int nA = w.inter(n0, d0, v1, -1, L0);
     const int nB = w.diff(n1, d1, v0, -1, L1);
+    if (w.H && w.M && nA + nB <= kSetMax && nA <= kWarp) {
+      // For a = A[j] the reference's freq = #{v in B : a not in N(v)} =
+      // nB - |N(a) & B| and c = #{x in A : x < a, x in N(a)} (symmetric
+      // graph): lane j walks N(a) once against B (tag 0) and A (tag 1,
+      // disjoint from B), or searches B and A in N(a) when that is shorter.
+      // The same pass records which B entries N(a) holds (bit j of
+      // mask_C[p] for B[p]) and M[j] = {k > j : A[k] in N(a)}; then the
+      // correction, for v4 = B[p] with C = A & N(v4) (mask_C[p]) and D =
+      // A - N(v4), is #{(v2, key) : v2 in C, key in D, key > v2, key in
+      // N(v2)} = sum over i in C of popc(M[i] & ~mask_C[p]).
+      const WarpSet s0{w.H};
+      s0.clear(w.lane);
+      s0.insert(L1, nB, 0, w.lane);
+      s0.insert(L0, nA, 1, w.lane);
+      unsigned *maskc = reinterpret_cast<unsigned *>(L2);
+      for (int p = w.lane; p < nB; p += kWarp) maskc[p] = 0u;
+      __syncwarp();
+      unsigned mrow = 0;
+      if (w.lane < nA) {
+        const int j = w.lane;
+        const int x = L0[j];
+        const int32_t *p = w.N(x);
+        const int dx = w.deg(x);
+        int hb = 0, ca = 0;
+        if (dx <= (nB + nA) * ceil_log2_int(dx)) {
+          for (int k = 0; k < dx; ++k) {
+            const int y = __ldg(p + k);
+            const int r = s0.lookup(y);
+            if (r == 1) {
+              ++hb;
+              atomicOr(maskc + pos_of(L1, nB, y), 1u << j);
+            } else if (r == 2) {
+              if (y < x) ++ca;
+              else mrow |= 1u << pos_of(L0, nA, y);
+            }
+          }
+        } else {
+          for (int k = 0; k < nB; ++k)
+            if (bsearch(p, dx, L1[k])) {
+              ++hb;
+              atomicOr(maskc + k, 1u << j);
+            }
+          for (int k = 0; k < nA; ++k)
+            if (k != j && bsearch(p, dx, L0[k])) {
+              if (k < j) ++ca;
+              else mrow |= 1u << k;
+            }
+        }
+        acc.c1 += wrap_mul(ca, nB - hb);
+      }
+      w.M[w.lane] = mrow;
+      __syncwarp();
+      for (int p = w.lane; p < nB; p += kWarp) {
+        const unsigned mc = __ldcg(maskc + p);  // set by atomics: read at L2
+        unsigned rest = mc;
+        int t = 0;
+        while (rest) {
+          const int i = __ffs(rest) - 1;
+          rest &= rest - 1u;
+          t += __popc(w.M[i] & ~mc);
+        }
+        acc.c2 += (unsigned long long)t;
+      }
+      __syncwarp();
+      return;
+    }
     cross_freq(w, L0, nA, L1, nB, L4);
     for (int i = 0; i < nA; ++i) {
       const int c = w.count(L0, nA, L0[i], L0[i], true);
@@ -469,10 +550,12 @@ __device__ void vertex_star(const Warp &w, int v0, int32_t *L, Acc &acc) {
 template <int P, bool kStar>
 __global__ void __launch_bounds__(kPatThreads) pattern_kernel(PatArgs a) {
   __shared__ __align__(16) int s_sets[kPatThreads / kWarp][kSetSlots];
+  __shared__ unsigned s_rows[kPatThreads / kWarp][kWarp];
   const int lane = threadIdx.x & (kWarp - 1);
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
   int32_t *L = a.scratch + gw * kLists * a.cap;
-  const Warp w{a.rp, a.ci, lane, s_sets[threadIdx.x / kWarp]};
+  const Warp w{a.rp, a.ci, lane, a.use_sets ? s_sets[threadIdx.x / kWarp] : nullptr,
+               a.use_sets ? s_rows[threadIdx.x / kWarp] : nullptr};
   const int64_t all = kStar ? a.n : (a.task_off ? a.task_off[a.n] : a.nnz);
   const int64_t ntasks = all > a.shard ? (all - a.shard + a.num_shards - 1) / a.num_shards : 0;
   Acc acc;
@@ -1065,10 +1148,11 @@ __device__ __forceinline__ void batch_edge(const Warp &w, int v0, int v1, int32_
 // of every pattern graph; each task's counters go to its own graph.
 __global__ void __launch_bounds__(kPatThreads) batch_pattern_kernel(BatchPatternArgs b) {
   __shared__ __align__(16) int s_sets[kPatThreads / kWarp][kSetSlots];
+  __shared__ unsigned s_rows[kPatThreads / kWarp][kWarp];
   const int lane = threadIdx.x & (kWarp - 1);
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
   int32_t *L = b.scratch + gw * kLists * b.cap;
-  const Warp w{b.rp, b.ci, lane, s_sets[threadIdx.x / kWarp]};
+  const Warp w{b.rp, b.ci, lane, s_sets[threadIdx.x / kWarp], s_rows[threadIdx.x / kWarp]};
   const int64_t n_star = b.star_off[b.num_graphs], n_edge = b.edge_off[b.num_graphs];
   for (;;) {
     unsigned long long t = 0;
@@ -1245,6 +1329,7 @@ int pattern_count(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12, mc_ti
             g->counters + 0, g->counters + 2};
   a.shard = shard;
   a.num_shards = num_shards;
+  if (const char *env = std::getenv("MERCURY_PATTERN_SETS")) a.use_sets = std::atoi(env) != 0;
   MC_CUDA_TRY(cudaEventRecord(g->ev[0], s));
   int rc = MC_OK;
   if (g->n > 0 && g->nnz > 0) {

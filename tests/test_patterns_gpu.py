@@ -39,6 +39,45 @@ def test_patterns_random_dense_vs_oracle(seed):
             assert d.pattern_count(k) == orc.pattern(rp, col, k), k
 
 
+_DENSE = {}
+
+
+def dense_case(n, p, seed):
+    """Dense seeded graph and its oracle counts (computed once per module)."""
+    if (n, p, seed) not in _DENSE:
+        rp, col = csr_from_edges(n, random_graph(n, p, seed))
+        _DENSE[(n, p, seed)] = (rp, col, [orc.pattern(rp, col, k) for k in range(1, 9)])
+    return _DENSE[(n, p, seed)]
+
+
+@pytest.mark.parametrize("n,p,seed", [(120, 0.5, 11), (200, 0.6, 12)])
+@pytest.mark.parametrize("sets", ["1", "0"])
+def test_patterns_dense_hash_and_search_forms_vs_oracle(monkeypatch, n, p, seed, sets):
+    """Dense graphs: common neighbourhoods above 32 (the P8 bitmask limit)
+    and degrees up to 138. The shared-memory set forms (sets=1) and the
+    binary-search forms (MERCURY_PATTERN_SETS=0) both give the oracle's
+    counts."""
+    monkeypatch.setenv("MERCURY_PATTERN_SETS", sets)
+    monkeypatch.setenv("MERCURY_PATTERN_KERNEL", "edge")
+    rp, col, want = dense_case(n, p, seed)
+    with DeviceGraph(rp, col) as d:
+        assert [d.pattern_count(k) for k in range(1, 9)] == want
+
+
+@pytest.mark.parametrize("make", [lambda: Graph.chung_lu(30000, 2.1, 12.0, 900.0, seed=7),
+                                  lambda: Graph.rmat(13, 16, seed=5)])
+def test_hash_set_forms_equal_search_forms(monkeypatch, make):
+    """Hubs of degree up to 900 put some edges past the 512-key table; both
+    forms agree on every pattern of the warp-per-edge route."""
+    g = make()
+    monkeypatch.setenv("MERCURY_PATTERN_KERNEL", "edge")
+    with DeviceGraph(g) as d:
+        fast = [d.pattern_count(k) for k in range(1, 9)]
+        monkeypatch.setenv("MERCURY_PATTERN_SETS", "0")
+        slow = [d.pattern_count(k) for k in range(1, 9)]
+    assert fast == slow
+
+
 def test_patterns_chung_lu_vs_oracle():
     g = Graph.chung_lu(4000, 2.1, 10.0, 200.0, seed=9)
     rp, col = np.array(g.rowptr), np.array(g.col)
