@@ -318,6 +318,20 @@ __device__ void edge_pattern(const Warp &w, int v0, int v1, int32_t *L, int64_t 
     const int nB = w.diff(n1, d1, v0, -1, L1);
     const int32_t *outer = nA < nB ? L0 : L1, *inner = nA < nB ? L1 : L0;
     const int no = nA < nB ? nA : nB, ni = nA < nB ? nB : nA;
+    if (w.H && ni <= kSetMax) {
+      // Per v2 in outer, the whole warp: ni - |N(v2) & inner|, streaming
+      // N(v2) against `inner` in the shared-memory set, or searching inner's
+      // entries in N(v2) when that takes fewer warp steps.
+      const WarpSet s0{w.H};
+      s0.clear(w.lane);
+      s0.insert(inner, ni, 0, w.lane);
+      for (int i = 0; i < no; ++i) {
+        const int common = warp_common(w, outer[i], s0, inner, ni);
+        if (w.lane == 0) acc.c1 += (unsigned long long)(ni - common);
+      }
+      __syncwarp();
+      return;
+    }
     for (int i = 0; i < no; ++i) {
       const int v2 = outer[i];
       const int dv2 = w.deg(v2);
