@@ -437,6 +437,19 @@ __device__ void edge_pattern(const Warp &w, int v0, int v1, int32_t *L, int64_t 
       const int nE = w.diff(L1, nB, v2, -1, L3);
       const int32_t *outer = nD < nE ? L2 : L3, *inner = nD < nE ? L3 : L2;
       const int no = nD < nE ? nD : nE, ni = nD < nE ? nE : nD;
+      if (w.H && ni <= kSetMax && no > 0) {
+        // #{x in inner : x not in N(v3)} = ni - |N(v3) & inner| by the
+        // whole warp, `inner` in the shared-memory set.
+        const WarpSet s0{w.H};
+        s0.clear(w.lane);
+        s0.insert(inner, ni, 0, w.lane);
+        for (int ii = 0; ii < no; ++ii) {
+          const int common = warp_common(w, outer[ii], s0, inner, ni);
+          if (w.lane == 0) acc.c1 += (unsigned long long)(ni - common);
+        }
+        __syncwarp();
+        continue;
+      }
       for (int ii = 0; ii < no; ++ii) {
         const int v3 = outer[ii];
         for (int j = w.lane; j < ni; j += kWarp) acc.c1 += !w.in(v3, inner[j]);
