@@ -362,23 +362,37 @@ __device__ void edge_pattern(const Warp &w, int v0, int v1, int32_t *L, int64_t 
         s0.clear(w.lane);
         s0.insert(L0, nA, 0, w.lane);
         s0.insert(L2, nC, 1, w.lane);
-        for (int j = w.lane; j < nB; j += kWarp) {
-          const int b = L1[j];
-          const int32_t *p = w.N(b);
-          const int db = w.deg(b);
+        // Groups of kGroup lanes per b (kWarp / kGroup b's at a time): short
+        // and hub neighbourhoods alike keep the group's lanes busy.
+        constexpr int kGroup = 8;
+        const int grp = w.lane / kGroup, sub = w.lane % kGroup;
+        const int nb_round = (nB + kWarp / kGroup - 1) / (kWarp / kGroup) * (kWarp / kGroup);
+        for (int j0 = 0; j0 < nb_round; j0 += kWarp / kGroup) {
+          const int j = j0 + grp;
           int ca = 0, cc = 0;
-          if (db <= (nA + nC) * ceil_log2_int(db)) {
-            for (int k = 0; k < db; ++k) {
-              const int r = s0.lookup(__ldg(p + k));
-              ca += r == 1;
-              cc += r == 2;
+          if (j < nB) {
+            const int b = L1[j];
+            const int32_t *p = w.N(b);
+            const int db = w.deg(b);
+            if ((db + kGroup - 1) / kGroup <=
+                ((nA + nC + kGroup - 1) / kGroup) * ceil_log2_int(db)) {
+              for (int k = sub; k < db; k += kGroup) {
+                const int r = s0.lookup(__ldg(p + k));
+                ca += r == 1;
+                cc += r == 2;
+              }
+            } else {
+              for (int k = sub; k < nA; k += kGroup) ca += bsearch(p, db, L0[k]);
+              for (int k = sub; k < nC; k += kGroup) cc += bsearch(p, db, L2[k]);
             }
-          } else {
-            for (int k = 0; k < nA; ++k) ca += bsearch(p, db, L0[k]);
-            for (int k = 0; k < nC; ++k) cc += bsearch(p, db, L2[k]);
+          }
+#pragma unroll
+          for (int o = kGroup / 2; o > 0; o >>= 1) {
+            ca += __shfl_xor_sync(kFull, ca, o);
+            cc += __shfl_xor_sync(kFull, cc, o);
           }
           const int f = nA - ca;
-          if (f) acc.c1 += wrap_mul(nC - cc, f);
+          if (j < nB && sub == 0 && f) acc.c1 += wrap_mul(nC - cc, f);
         }
         __syncwarp();
       }
