@@ -9,7 +9,10 @@
 // same per-edge terms (each pattern takes the faster; see
 // pattern_uses_centers):
 //  * warp per directed edge: the frontier lists of the pattern materialised
-//    in a per-warp slice of global scratch, membership by binary search;
+//    in a per-warp slice of global scratch, membership by binary search or,
+//    for the dominant terms of P4, P5, P6 and P8, by a per-warp hash set in
+//    shared memory (counts restated as |N(x) & S| through the symmetry of
+//    the graph; same integers, same 32-bit products);
 //  * center bitmaps: a group of warps per center v0 holds the adjacency among
 //    N(v0) as bit rows in shared memory and reads each term off popcounts
 //    (centers of degree above kCenterMaxDeg stay on the first route).
