@@ -22,6 +22,9 @@ enum DeviceError : unsigned {
   kErrRank = 1u << 7,         // an out-list entry not ranked below its owner
   kErrDagCapacity = 1u << 8,  // more DAG entries than an exact-size DAG holds
 };
+// Bits of the CSR contract checks.
+constexpr unsigned kErrContract = kErrIdRange | kErrUnsorted | kErrSelfLoop | kErrRowptr |
+                                  kErrAsymmetric;
 
 #define MC_CUDA_TRY(expr)                                   \
   do {                                                      \

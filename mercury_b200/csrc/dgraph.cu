@@ -368,17 +368,23 @@ int mc_tc_count(mc_dgraph_t *g, uint64_t *count, mc_timing_t *timing) {
   return mc_tc_count_shard(g, 0, 1, count, timing);
 }
 
-int mc_tc_count_shard(mc_dgraph_t *g, int shard, int num_shards, uint64_t *count,
-                      mc_timing_t *timing) {
-  mc::NvtxRange range("mc_tc_count");
+}  // extern "C"
+
+namespace mc {
+namespace {
+// The triangle count of a handle; upload (host memory, or null) streams the
+// column array into the handle during orientation (see tc_orient).
+int tc_count_impl(mc_dgraph_t *g, int shard, int num_shards, uint64_t *count,
+                  mc_timing_t *timing, const int32_t *upload) {
+  NvtxRange range("mc_tc_count");
   if (!g || !count || num_shards < 1 || shard < 0 || shard >= num_shards) return MC_ERR_ARG;
   MC_CUDA_TRY(cudaSetDevice(g->device));
-  int rc = mc::tc_alloc(g);
+  int rc = tc_alloc(g);
   if (rc != MC_OK) return rc;
   cudaStream_t s = g->stream;
   const int64_t launches_before = g->launches;
   MC_CUDA_TRY(cudaEventRecord(g->ev[0], s));
-  rc = mc::tc_orient(g);
+  rc = tc_orient(g, upload);
   if (rc != MC_OK) return rc;
   MC_CUDA_TRY(cudaEventRecord(g->ev[1], s));
   // The hub table size follows the largest DAG out-degree (load <= 1/4).
@@ -386,9 +392,10 @@ int mc_tc_count_shard(mc_dgraph_t *g, int shard, int num_shards, uint64_t *count
                               cudaMemcpyDeviceToHost, s));
   MC_CUDA_TRY(cudaMemcpyAsync(g->h_err, g->err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
   MC_CUDA_TRY(cudaStreamSynchronize(s));
-  // An exact-size DAG (host columns) that the rows overran: the input is not
-  // symmetric, and the DAG was left unwritten.
-  if (*g->h_err & mc::kErrDagCapacity) return MC_ERR_FORMAT;
+  // An exact-size DAG (host columns) that the rows overran (the input is not
+  // symmetric), or a streamed chunk that failed its contract checks: the DAG
+  // was left unwritten.
+  if (*g->h_err & (kErrDagCapacity | kErrContract)) return MC_ERR_FORMAT;
   const long long maxd = (long long)g->h_counters[3];
   // MERCURY_TC_TABLE_LOG2_MAX (8..15) lowers the shared-memory table cap;
   // owners whose list no longer fits are then probed by binary search in
@@ -435,6 +442,16 @@ int mc_tc_count_shard(mc_dgraph_t *g, int shard, int num_shards, uint64_t *count
     timing->launches = g->launches - launches_before;
   }
   return MC_OK;
+}
+
+}  // namespace
+}  // namespace mc
+
+extern "C" {
+
+int mc_tc_count_shard(mc_dgraph_t *g, int shard, int num_shards, uint64_t *count,
+                      mc_timing_t *timing) {
+  return mc::tc_count_impl(g, shard, num_shards, count, timing, nullptr);
 }
 
 int mc_tc_stats(const mc_dgraph_t *g, mc_tc_stats_t *stats) {
@@ -509,16 +526,23 @@ int mc_tc_count_host(const int64_t *rowptr, const int32_t *col, int64_t n, int64
   MC_CUDA_TRY(cudaEventRecord(e0, g->stream));
   MC_CUDA_TRY(cudaMemcpyAsync(g->rowptr, rowptr, sizeof(int64_t) * (size_t)(n + 1),
                               cudaMemcpyHostToDevice, g->stream));
-  if (nnz > 0 && g->col_host)
-    mc::copy_to_pinned(g->col_h, col, nnz);  // while the offsets upload
-  else if (nnz > 0)
-    MC_CUDA_TRY(cudaMemcpyAsync(g->col, col, sizeof(int32_t) * (size_t)nnz, cudaMemcpyHostToDevice,
-                                g->stream));
+  if (nnz > 0 && g->col_host) mc::copy_to_pinned(g->col_h, col, nnz);  // while the offsets upload
   MC_CUDA_TRY(cudaEventRecord(e1, g->stream));
   g->launches = 0;
-  int rc = mc::validate_graph(g, 0);
-  const int64_t validate_launches = g->launches;
-  if (rc == MC_OK) rc = mc_tc_count(g, count, timing);
+  int rc;
+  int64_t validate_launches = 0;
+  if (g->col_host) {
+    rc = mc::validate_graph(g, 0);
+    validate_launches = g->launches;
+    if (rc == MC_OK) rc = mc_tc_count(g, count, timing);
+  } else {
+    // Device columns: the row offsets are checked first; the column array
+    // then crosses in chunks during orientation, each chunk checked before
+    // the passes that read it, so the copy overlaps the checks and passes.
+    rc = mc::validate_rowptr(g);
+    validate_launches = g->launches;
+    if (rc == MC_OK) rc = mc::tc_count_impl(g, 0, 1, count, timing, nnz > 0 ? col : nullptr);
+  }
   if (rc == MC_OK && timing) {
     timing->h2d_ms = mc::elapsed(e0, e1);
     timing->orient_ms += mc::elapsed(e1, g->ev[0]);  // validation on upload

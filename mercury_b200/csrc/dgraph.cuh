@@ -107,7 +107,8 @@ struct mc_dgraph {
   int64_t stage_edges = 0;
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t stage_ev[4] = {};
-  int64_t *chunk_offsets = nullptr;
+  int64_t chunk_edges = 0;  // entries per chunk of a streamed upload (fixed at allocation)
+  int64_t *chunk_offsets = nullptr;  // chunk_edges / kTileEdges + 1
   void *scan_temp = nullptr;
   size_t scan_temp_size = 0;
   // 0: result, 1: hub queue, 2: leaf queue, 3: max d+, 4-5: partner
@@ -131,7 +132,12 @@ int tc_alloc(mc_dgraph *g);
 // Device bytes tc_alloc takes for a single graph of n vertices and nnz
 // entries (the DAG at half the entries when the columns are on the host).
 int64_t tc_device_bytes(int64_t n, int64_t nnz, bool col_host);
-int tc_orient(mc_dgraph *g);
+// upload (host memory, nnz entries): the column array is copied into the
+// handle in chunks during the passes, each chunk checked against the CSR
+// contract first (the row offsets must have been checked: validate_rowptr).
+int tc_orient(mc_dgraph *g, const int32_t *upload = nullptr);
+// Contract checks of the row offsets alone; sets max_degree.
+int validate_rowptr(mc_dgraph *g);
 int tc_partner_stats(mc_dgraph *g, unsigned long long *partner_edges, unsigned long long *work);
 // Contract checks of a caller-owned device CSR with caller-provided device
 // words for the error flag and the maximum degree (nothing is allocated).

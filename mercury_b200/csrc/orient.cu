@@ -177,7 +177,8 @@ struct ColumnChunk {
 // compacted into out_col (and, when rank is given, their ranks into
 // out_rank) and out_rowptr[r] = kept entries before rowptr[r].  With
 // chunk_end given, pass B writes nothing when *chunk_end (the DAG entries
-// up to the end of this chunk) exceeds cap.
+// up to the end of this chunk) exceeds cap; with stop given, neither pass
+// does anything once a contract bit is set there.
 template <bool kWrite>
 __global__ void __launch_bounds__(kTileThreads)
     dag_pass_kernel(const int64_t *__restrict__ rowptr, ColumnChunk cc,
@@ -185,9 +186,13 @@ __global__ void __launch_bounds__(kTileThreads)
                     uint16_t *keep_masks, int32_t *counts_out,
                     const int64_t *__restrict__ offs_in, int64_t *out_rowptr, int32_t *out_col,
                     const int32_t *__restrict__ rank, int32_t *out_rank,
-                    const int64_t *chunk_end, int64_t cap) {
+                    const int64_t *chunk_end, int64_t cap, const unsigned *stop) {
   __shared__ int64_t seg[kSegMax];
-  if (kWrite && chunk_end && *chunk_end > cap) return;  // the same for the whole CTA
+  // Both checks read one word, the same for the whole CTA.  `stop`: the
+  // contract checks of a chunk validated just before found a bad entry, so
+  // no id is gathered or written.
+  if (stop && (*(volatile const unsigned *)stop & kErrContract)) return;
+  if (kWrite && chunk_end && *chunk_end > cap) return;
   const int64_t tile = cc.tile_base + blockIdx.x;
   const int64_t t0 = tile * kTileEdges;
   const int64_t t1 = min(t0 + kTileEdges, nnz);
@@ -265,9 +270,10 @@ __global__ void chunk_offsets_kernel(const int64_t *__restrict__ local, int64_t 
 // ascending rows, no self-loops, and (optionally) symmetry.
 __global__ void __launch_bounds__(kTileThreads)
     validate_entries_kernel(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ col,
-                            int64_t n, int64_t nnz, int check_sym, unsigned *err) {
+                            int64_t n, int64_t nnz, int check_sym, unsigned *err,
+                            int64_t tile_base) {
   __shared__ int64_t seg[kSegMax];
-  const int64_t t0 = (int64_t)blockIdx.x * kTileEdges;
+  const int64_t t0 = (tile_base + blockIdx.x) * kTileEdges;
   const int64_t t1 = min(t0 + kTileEdges, nnz);
   const TileRows tr = load_tile_rows(rowptr, n, t0, t1, seg);
   const int64_t s = t0 + (int64_t)threadIdx.x * kEdgesPerThread;
@@ -358,7 +364,7 @@ __global__ void core_bits_kernel(const unsigned long long *__restrict__ sorted, 
                                  unsigned *err) {
   const int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
   const int lane = threadIdx.x & (kWarp - 1);
-  if (p >= core_ranks || (*(volatile unsigned *)err & kErrDagCapacity)) return;
+  if (p >= core_ranks || (*(volatile unsigned *)err & (kErrDagCapacity | kErrContract))) return;
   const int64_t v = n - 1 - (int64_t)(uint32_t)sorted[p];
   unsigned *row = core + core_offset(p);
   for (int64_t e = dag_rowptr[v] + lane; e < dag_rowptr[v + 1]; e += kWarp) {
@@ -485,12 +491,28 @@ int validate_graph(mc_dgraph *g, unsigned flags) {
   g->launches += 1 + (tiles > 0 ? 1 : 0);
   if (tiles > 0) {
     validate_entries_kernel<<<(unsigned)tiles, kTileThreads, 0, g->stream>>>(
-        g->rowptr, g->col, g->n, g->nnz, (flags & MC_VALIDATE_SYMMETRY) ? 1 : 0, g->err);
+        g->rowptr, g->col, g->n, g->nnz, (flags & MC_VALIDATE_SYMMETRY) ? 1 : 0, g->err, 0);
     MC_CUDA_TRY(cudaGetLastError());
   }
   MC_CUDA_TRY(cudaMemcpyAsync(g->h_err, g->err, sizeof(unsigned), cudaMemcpyDeviceToHost, g->stream));
   MC_CUDA_TRY(cudaStreamSynchronize(g->stream));
   return *g->h_err ? MC_ERR_FORMAT : MC_OK;
+}
+
+int validate_rowptr(mc_dgraph *g) {
+  MC_CUDA_TRY(cudaMemsetAsync(g->err, 0, sizeof(unsigned), g->stream));
+  MC_CUDA_TRY(cudaMemsetAsync(g->counters + 7, 0, sizeof(unsigned long long), g->stream));
+  validate_rowptr_kernel<<<grid_for(g->n + 1, 256), 256, 0, g->stream>>>(
+      g->rowptr, g->n, g->nnz, g->err, g->counters + 7);
+  MC_CUDA_TRY(cudaGetLastError());
+  g->launches += 1;
+  MC_CUDA_TRY(cudaMemcpyAsync(g->h_err, g->err, sizeof(unsigned), cudaMemcpyDeviceToHost, g->stream));
+  MC_CUDA_TRY(cudaMemcpyAsync(g->h_counters + 7, g->counters + 7, sizeof(unsigned long long),
+                              cudaMemcpyDeviceToHost, g->stream));
+  MC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  if (*g->h_err) return MC_ERR_FORMAT;
+  g->max_degree = (int64_t)g->h_counters[7];
+  return MC_OK;
 }
 
 int validate_csr_words(const int64_t *rowptr, const int32_t *col, int64_t n, int64_t nnz,
@@ -508,7 +530,8 @@ int validate_csr_words(const int64_t *rowptr, const int32_t *col, int64_t n, int
   if (h_err) return MC_ERR_FORMAT;  // the entry walk needs monotone offsets
   const int64_t tiles = (nnz + kTileEdges - 1) / kTileEdges;
   if (tiles > 0) {
-    validate_entries_kernel<<<(unsigned)tiles, kTileThreads, 0, s>>>(rowptr, col, n, nnz, 0, d_err);
+    validate_entries_kernel<<<(unsigned)tiles, kTileThreads, 0, s>>>(rowptr, col, n, nnz, 0, d_err,
+                                                                   0);
     MC_CUDA_TRY(cudaGetLastError());
     MC_CUDA_TRY(cudaMemcpyAsync(&h_err, d_err, sizeof(h_err), cudaMemcpyDeviceToHost, s));
     MC_CUDA_TRY(cudaStreamSynchronize(s));
@@ -598,13 +621,18 @@ int tc_alloc(mc_dgraph *g) {
     g->core_ranks = core_rank_count(n);
     if (g->core_ranks > 0) MC_ALLOC(g->core_bits, core_offset(g->core_ranks));
   }
-  if (g->col_host && ranked) {
-    g->stage_edges = stage_capacity(g->nnz);
-    MC_ALLOC(g->stage, 2 * g->stage_edges);
-    MC_ALLOC(g->chunk_offsets, g->stage_edges / kTileEdges + 1);
+  // Chunked column passes (host columns, or a streamed upload of a single
+  // graph): the copy stream, its events and one chunk's tile offsets.
+  if (ranked) {
+    g->chunk_edges = stage_capacity(g->nnz);
+    MC_ALLOC(g->chunk_offsets, g->chunk_edges / kTileEdges + 1);
     MC_CUDA_TRY(cudaStreamCreateWithFlags(&g->copy_stream, cudaStreamNonBlocking));
     for (cudaEvent_t &e : g->stage_ev)
       MC_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  if (g->col_host && ranked) {
+    g->stage_edges = g->chunk_edges;
+    MC_ALLOC(g->stage, 2 * g->stage_edges);
   }
   MC_CUDA_TRY(dev_alloc(&g->scan_temp, g->scan_temp_size, g->stream));
 #undef MC_ALLOC
@@ -612,36 +640,50 @@ int tc_alloc(mc_dgraph *g) {
   return MC_OK;
 }
 
-// Passes A and B with the columns in host memory: the column array crosses
-// the host link once, in chunks of whole tiles copied by DMA into two
-// device buffers, while the passes run on the previous chunk.  Each chunk
-// runs A, the scan of its tile counts on top of the earlier chunks' total,
-// and B, so no pass waits for the whole array. The DAG holds dag_cap
-// entries; a chunk that would end past it raises kErrDagCapacity and writes
-// nothing (the caller reads the flag before counting).
-static int staged_dag_passes(mc_dgraph *g, const int32_t *deg) {
+// Passes A and B over a column array that crosses from host memory in
+// chunks of whole tiles, copied by DMA on a copy stream while the passes run
+// on the previous chunk.  Each chunk runs A, the scan of its tile counts on
+// top of the earlier chunks' total, and B, so no pass waits for the whole
+// array.  Two forms:
+//  * host columns (in_place false): chunks go to two staging buffers; the
+//    columns were validated when the handle was made;
+//  * streamed upload (in_place true): chunks land in the handle's own device
+//    column array, and each chunk's contract checks run before its passes,
+//    which do nothing once a check has failed (no gather of an unchecked id).
+// The DAG holds dag_cap entries; a chunk that would end past it raises
+// kErrDagCapacity and writes nothing.  The caller reads the flags before
+// counting.
+static int staged_dag_passes(mc_dgraph *g, const int32_t *deg, const int32_t *src, bool in_place) {
   const int64_t n = g->n, nnz = g->nnz;
   cudaStream_t s = g->stream, cs = g->copy_stream;
   cudaEvent_t *copied = g->stage_ev, *drained = g->stage_ev + 2;
+  const int64_t chunk = in_place ? g->chunk_edges : g->stage_edges;
+  const unsigned *stop = in_place ? g->err : nullptr;
   MC_CUDA_TRY(cudaMemsetAsync(g->tile_offsets, 0, sizeof(int64_t), s));
   // Copies start after the work already queued on the handle's stream.
   MC_CUDA_TRY(cudaEventRecord(drained[0], s));
   MC_CUDA_TRY(cudaStreamWaitEvent(cs, drained[0], 0));
-  const int64_t chunks = (nnz + g->stage_edges - 1) / g->stage_edges;
+  const int64_t chunks = (nnz + chunk - 1) / chunk;
   for (int64_t c = 0; c < chunks; ++c) {
     const int slot = (int)(c & 1);
-    const int64_t e0 = c * g->stage_edges, e1 = std::min(nnz, e0 + g->stage_edges);
+    const int64_t e0 = c * chunk, e1 = std::min(nnz, e0 + chunk);
     const int64_t tb = e0 / kTileEdges, ct = (e1 - e0 + kTileEdges - 1) / kTileEdges;
-    int32_t *buf = g->stage + (int64_t)slot * g->stage_edges;
-    if (c >= 2) MC_CUDA_TRY(cudaStreamWaitEvent(cs, drained[slot], 0));
-    MC_CUDA_TRY(cudaMemcpyAsync(buf, g->col_h + e0, sizeof(int32_t) * (size_t)(e1 - e0),
+    int32_t *buf = in_place ? g->col + e0 : g->stage + (int64_t)slot * g->stage_edges;
+    if (!in_place && c >= 2) MC_CUDA_TRY(cudaStreamWaitEvent(cs, drained[slot], 0));
+    MC_CUDA_TRY(cudaMemcpyAsync(buf, src + e0, sizeof(int32_t) * (size_t)(e1 - e0),
                                 cudaMemcpyHostToDevice, cs));
     MC_CUDA_TRY(cudaEventRecord(copied[slot], cs));
     MC_CUDA_TRY(cudaStreamWaitEvent(s, copied[slot], 0));
-    const ColumnChunk cc{buf, e0, tb};
+    if (in_place) {
+      validate_entries_kernel<<<(unsigned)ct, kTileThreads, 0, s>>>(g->rowptr, g->col, n, nnz, 0,
+                                                                    g->err, tb);
+      MC_CUDA_TRY(cudaGetLastError());
+      g->launches += 1;
+    }
+    const ColumnChunk cc = in_place ? ColumnChunk{g->col, 0, tb} : ColumnChunk{buf, e0, tb};
     dag_pass_kernel<false><<<(unsigned)ct, kTileThreads, 0, s>>>(
         g->rowptr, cc, deg, n, nnz, g->key, g->keep, g->tile_counts, nullptr, nullptr, nullptr,
-        nullptr, nullptr, nullptr, 0);
+        nullptr, nullptr, nullptr, 0, stop);
     MC_CUDA_TRY(cudaGetLastError());
     MC_CUDA_TRY(exclusive_scan(g->tile_counts + tb, g->chunk_offsets, ct, g->scan_temp, s));
     chunk_offsets_kernel<<<grid_for(ct + 1, 256), 256, 0, s>>>(g->chunk_offsets, ct,
@@ -650,7 +692,7 @@ static int staged_dag_passes(mc_dgraph *g, const int32_t *deg) {
     MC_CUDA_TRY(cudaGetLastError());
     dag_pass_kernel<true><<<(unsigned)ct, kTileThreads, 0, s>>>(
         g->rowptr, cc, deg, n, nnz, g->key, g->keep, nullptr, g->tile_offsets, g->dag_rowptr,
-        g->dag_col, g->rank, g->dag_rank, g->tile_offsets + tb + ct, g->dag_cap);
+        g->dag_col, g->rank, g->dag_rank, g->tile_offsets + tb + ct, g->dag_cap, stop);
     MC_CUDA_TRY(cudaGetLastError());
     MC_CUDA_TRY(cudaEventRecord(drained[slot], s));
     g->launches += 3 + scan_launches(ct);
@@ -658,7 +700,7 @@ static int staged_dag_passes(mc_dgraph *g, const int32_t *deg) {
   return MC_OK;
 }
 
-int tc_orient(mc_dgraph *g) {
+int tc_orient(mc_dgraph *g, const int32_t *upload) {
   NvtxRange range("tc_orient");
   const int64_t n = g->n, nnz = g->nnz;
   cudaStream_t s = g->stream;
@@ -687,21 +729,24 @@ int tc_orient(mc_dgraph *g) {
   }
   if (tiles == 0) {
     MC_CUDA_TRY(cudaMemsetAsync(g->dag_rowptr, 0, sizeof(int64_t) * (n + 1), s));
+  } else if (upload) {
+    const int rc = staged_dag_passes(g, deg, upload, true);
+    if (rc != MC_OK) return rc;
   } else if (g->col_host) {
-    const int rc = staged_dag_passes(g, deg);
+    const int rc = staged_dag_passes(g, deg, g->col_h, false);
     if (rc != MC_OK) return rc;
   } else {
     const unsigned grid = (unsigned)tiles;
     const ColumnChunk all{g->col, 0, 0};
     dag_pass_kernel<false><<<grid, kTileThreads, 0, s>>>(
         g->rowptr, all, deg, n, nnz, g->key, g->keep, g->tile_counts, nullptr, nullptr, nullptr,
-        nullptr, nullptr, nullptr, 0);
+        nullptr, nullptr, nullptr, 0, nullptr);
     MC_CUDA_TRY(cudaGetLastError());
     MC_CUDA_TRY(exclusive_scan(g->tile_counts, g->tile_offsets, tiles, g->scan_temp, s));
     dag_pass_kernel<true><<<grid, kTileThreads, 0, s>>>(
         g->rowptr, all, deg, n, nnz, g->key, g->keep, nullptr, g->tile_offsets, g->dag_rowptr,
         g->dag_col, g->batch.gid ? nullptr : g->rank, g->batch.gid ? nullptr : g->dag_rank,
-        nullptr, 0);
+        nullptr, 0, nullptr);
     MC_CUDA_TRY(cudaGetLastError());
     g->launches += 2 + scan_launches(tiles);
   }

@@ -85,6 +85,56 @@ def test_one_shot_host_entry_equals_handle_path():
     assert tc_count_host(h.rowptr, h.col) == orc.tc(h.rowptr, h.col)
 
 
+def in_fresh_thread(body):
+    """Runs body in a new thread: the one-shot call keeps a per-thread device
+    context, so a new thread makes a new one (with the current settings)."""
+    import threading
+    errors = []
+
+    def run():
+        try:
+            body()
+        except BaseException as e:  # re-raised in the test's thread
+            errors.append(e)
+
+    t = threading.Thread(target=run)
+    t.start()
+    t.join()
+    if errors:
+        raise errors[0]
+
+
+def test_one_shot_streams_the_columns_in_checked_chunks(monkeypatch):
+    """The one-shot call copies the column array in chunks (4096 entries
+    here: about 100 of them) while the contract checks and orientation
+    passes run on the chunks already copied. A bad id in the last chunk or
+    an unsorted row in the middle is refused, and the next call counts
+    again."""
+    monkeypatch.setenv("MERCURY_STAGE_EDGES", "4096")
+    g = Graph.rmat(14, 16, seed=5)
+    rp, col = np.asarray(g.rowptr), np.asarray(g.col)
+    want = orc.tc(rp, col)
+    bad_id = col.copy()
+    bad_id[-1] = g.n + 5
+    unsorted = col.copy()
+    mid = int(np.searchsorted(rp, len(col) // 2))
+    while rp[mid + 1] - rp[mid] < 2:
+        mid += 1
+    a = rp[mid]
+    unsorted[a], unsorted[a + 1] = unsorted[a + 1], unsorted[a]
+
+    def body():
+        assert tc_count_host(rp, col) == want
+        assert tc_count_host(rp, col) == want
+        for bad in (bad_id, unsorted):
+            with pytest.raises(McError) as ex:
+                tc_count_host(rp, bad)
+            assert ex.value.status == _ffi.MC_ERR_FORMAT
+            assert tc_count_host(rp, col) == want
+
+    in_fresh_thread(body)
+
+
 @pytest.mark.parametrize("shards", [2, 3, 8])
 def test_shard_partials_sum_to_the_count(shards):
     g = Graph.rmat(14, 16, seed=8)
