@@ -730,9 +730,12 @@ int tc_orient(mc_dgraph *g, const int32_t *upload) {
   if (tiles == 0) {
     MC_CUDA_TRY(cudaMemsetAsync(g->dag_rowptr, 0, sizeof(int64_t) * (n + 1), s));
   } else if (upload) {
+    // A streamed upload needs the chunk machinery of a single-graph handle.
+    if (!g->copy_stream || !g->chunk_offsets || g->chunk_edges <= 0) return MC_ERR_ARG;
     const int rc = staged_dag_passes(g, deg, upload, true);
     if (rc != MC_OK) return rc;
   } else if (g->col_host) {
+    if (!g->copy_stream || !g->stage || g->stage_edges <= 0) return MC_ERR_ARG;
     const int rc = staged_dag_passes(g, deg, g->col_h, false);
     if (rc != MC_OK) return rc;
   } else {
