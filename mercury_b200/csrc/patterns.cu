@@ -474,6 +474,49 @@ __device__ void edge_pattern(const Warp &w, int v0, int v1, int32_t *L, int64_t 
     }
   } else if (P == 7) {  // P7_subgraph_matching (:352-459)
     const int nA = w.inter(n0, d0, v1, -1, L0);
+    if (w.M && nA <= kWarp) {
+      // Every set of P7 lies inside A (ascending, at most 32 entries): lane
+      // i holds M[i] = {k : A[k] in N(A[i])}, and by the graph's symmetry
+      // freq[i] = #{k > i : A[i] not in N(A[k])} = popc(~M[i] above i),
+      // c = #{x in A : x < A[i], x not in N(A[i])} = popc(~M[i] below i),
+      // and the correction for v2 = A[i] (D = ~M[i] below i, C = M[i]) is
+      // the sum over t in C of popc(D above t & ~M[t]).  With |A| <= 2 every
+      // term is 0.
+      if (nA < 3) {
+        __syncwarp();
+        return;
+      }
+      unsigned row = 0;
+      if (w.lane < nA) {
+        const int32_t *p = w.N(L0[w.lane]);
+        const int dx = w.deg(L0[w.lane]);
+        for (int k = 0; k < nA; ++k)
+          if (k != w.lane && bsearch(p, dx, L0[k])) row |= 1u << k;
+      }
+      w.M[w.lane] = row;
+      __syncwarp();
+      if (w.lane < nA) {
+        const int i = w.lane;
+        const unsigned valid = nA == kWarp ? kFull : ((1u << nA) - 1u);
+        const unsigned below = (1u << i) - 1u;
+        const unsigned above = valid & ~below & ~(1u << i);
+        const int freq = __popc(~row & above);
+        const int c = __popc(~row & below);
+        acc.c1 += wrap_mul(c, freq);
+        const unsigned dmask = ~row & below;
+        unsigned cm = row;
+        int c2 = 0;
+        while (cm) {
+          const int t = __ffs(cm) - 1;
+          cm &= cm - 1u;
+          const unsigned above_t = t == kWarp - 1 ? 0u : ~((2u << t) - 1u);
+          c2 += __popc(dmask & above_t & ~w.M[t]);
+        }
+        acc.c2 += (unsigned long long)c2;
+      }
+      __syncwarp();
+      return;
+    }
     pair_freq(w, L0, nA, L4);
     for (int i = 0; i < nA; ++i) {
       const int c = w.count(L0, nA, L0[i], L0[i], false);
