@@ -12,7 +12,8 @@
 //    in a per-warp slice of global scratch, membership by binary search or,
 //    for the dominant terms of P4, P5, P6 and P8, by a per-warp hash set in
 //    shared memory (counts restated as |N(x) & S| through the symmetry of
-//    the graph; same integers, same 32-bit products);
+//    the graph; same integers, same 32-bit products), and for P7 and P8's
+//    correction by 32-bit adjacency rows within A when |A| <= 32;
 //  * center bitmaps: a group of warps per center v0 holds the adjacency among
 //    N(v0) as bit rows in shared memory and reads each term off popcounts
 //    (centers of degree above kCenterMaxDeg stay on the first route).
