@@ -62,6 +62,8 @@ def parse_args():
     p.add_argument("--pat-n", type=int, default=100000)
     p.add_argument("--pat-mean", type=float, default=10.0)
     p.add_argument("--pat-cap", type=float, default=200.0)
+    p.add_argument("--pat-budget-ms", type=float, default=0.0,
+                   help="patterns mode: device-time budget per pattern (0: none)")
     p.add_argument("--serve-rates", default="100,1000,5000,20000")
     p.add_argument("--serve-seconds", type=float, default=2.0)
     p.add_argument("--serve-pool", type=int, default=512)
@@ -87,7 +89,7 @@ def workload_config(a):
 
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled every 200 ms in the background."""
+    """nvidia-smi clocks/throttle reasons sampled every 50 ms in the background."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -105,7 +107,7 @@ class ClockSampler:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=self.fh, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
@@ -160,19 +162,41 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def traffic_from_profile():
-    """DRAM bytes per launch of tc_hub_kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "tc_hub_kernel_rmat22.txt")
-    if not os.path.exists(path):
+HUB_DRAM_PROFILE = os.path.join(ROOT, "profiles", "tc_hub_kernel_rmat22_dram.txt")
+
+
+def hub_profile(a):
+    """Counters of one tc_hub_kernel launch captured by ncu on exactly this
+    workload (RMAT scale 22, edge factor 16, seed 1): DRAM bytes read +
+    written, warp instructions issued and the launch's duration, as the
+    committed summary records them ("key = value" lines).  None for any other
+    workload: traffic is not carried over from one graph to another."""
+    if (a.scale, a.edge_factor, a.seed) != (22, 16, 1) or getattr(a, "host_columns", False):
         return None
-    with open(path) as f:
+    if not os.path.exists(HUB_DRAM_PROFILE):
+        return None
+    rec = {}
+    with open(HUB_DRAM_PROFILE) as f:
         for line in f:
-            if line.startswith("dram_bytes_per_launch"):
+            if "=" in line and not line.startswith("#"):
+                k, v = line.split("=", 1)
                 try:
-                    return float(line.split("=")[1].split()[0])
+                    rec[k.strip()] = float(v.split()[0])
                 except (IndexError, ValueError):
-                    return None
-    return None
+                    pass
+    need = ("dram_bytes_per_launch", "warp_inst_per_launch", "ncu_duration_ms")
+    return rec if all(k in rec for k in need) else None
+
+
+def committed_reference_count(a):
+    """Triangle count the reference's own tc_challenge printed for this RMAT
+    graph (tests/golden/reference_counts.json), or None if it has no record."""
+    if (a.edge_factor, a.seed) != (16, 1):
+        return None
+    path = os.path.join(ROOT, "tests", "golden", "reference_counts.json")
+    with open(path) as f:
+        rec = json.load(f).get("rmat_tc", {}).get(f"rmat{a.scale}")
+    return None if rec is None else int(rec["triangles"])
 
 
 def algorithmic_bytes(n, drp, dcol):
@@ -200,6 +224,52 @@ def algorithmic_bytes(n, drp, dcol):
             "merge_volume": float((ds + dd).sum())}
 
 
+SM_COUNT = 148
+ISSUE_SLOTS_PER_SM_CYCLE = 4  # one warp instruction per scheduler per cycle
+
+
+def hub_roofline(a, hub_ms, ab, peak, peak_kind, clk):
+    """Roofline of tc_hub_kernel, the dominant kernel of the step.
+
+    The kernel is bound by memory latency and instruction issue, not by HBM
+    bandwidth: the edge-iterator merge volume (12 B + 4 B x (d+u + d+v) per
+    DAG edge) is not a floor for it, because each owner's list is read once
+    into shared memory and dense partners are read as bitmap quads, so that
+    volume over the launch time exceeds the HBM peak.  The line therefore
+    reports what the hardware did: DRAM bytes per launch (ncu, this workload)
+    over the launch time measured here, against the measured HBM peak; and
+    the warp instructions per launch over the issue slots of the launch time
+    at the sampled SM clock.  The merge volume stays beside them as
+    information."""
+    prof = hub_profile(a)
+    sec = hub_ms / 1e3
+    roof = {"bound": "hbm", "kernel": "tc_hub_kernel", "unit": "GB/s", "peak": peak,
+            "peak_source": f"{peak_kind} hbm_gbs", "launch_ms": hub_ms,
+            "algorithmic_bytes_per_launch": ab["b_hub"],
+            "algorithmic_gbs": ab["b_hub"] / sec / 1e9,
+            "algorithmic_note": "edge-iterator merge volume, 12 B + 4 B x (d+u + d+v) per DAG "
+                                "edge owned by a hub task + 8 B per owner row: information "
+                                "only, not a floor for this kernel"}
+    if prof is None:
+        roof.update({"achieved": None, "frac": None, "traffic": None,
+                     "traffic_source": "no ncu record of this workload"})
+        return roof
+    traffic = prof["dram_bytes_per_launch"]
+    achieved = traffic / sec / 1e9
+    roof.update({"achieved": achieved, "frac": achieved / peak, "traffic": traffic,
+                 "traffic_source": os.path.relpath(HUB_DRAM_PROFILE, ROOT),
+                 "achieved_is": "measured DRAM bytes (read + write) per launch / CUDA-event "
+                                "launch time of this run"})
+    mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz")
+    if mhz:
+        slots = SM_COUNT * ISSUE_SLOTS_PER_SM_CYCLE * mhz * 1e6 * sec
+        roof["issue"] = {"warp_inst_per_launch": prof["warp_inst_per_launch"],
+                         "issue_slots": slots,
+                         "frac": prof["warp_inst_per_launch"] / slots,
+                         "sm_mhz": mhz}
+    return roof
+
+
 # ---------------------------------------------------------------- CPU side
 def cpu_baseline(g, drp=None, dcol=None, target_s=12.0):
     """Oracle on the host cores: orientation of the whole graph plus a count
@@ -221,7 +291,7 @@ def cpu_baseline(g, drp=None, dcol=None, target_s=12.0):
     # scale the modulus so one sample takes about target_s seconds
     k = max(1, int(k * dt / target_s)) if dt < target_s else k
     t0 = time.perf_counter()
-    _, e = orc.tc_sample(drp, dcol, k)
+    sampled, e = orc.tc_sample(drp, dcol, k)
     t_sample = time.perf_counter() - t0
     t_count = t_sample * (m_dag / max(e, 1))
     m = len(col) // 2
@@ -232,17 +302,20 @@ def cpu_baseline(g, drp=None, dcol=None, target_s=12.0):
                   f"a hash-sampled 1/{k} of the sources ({e} of {m_dag} DAG edges, "
                   f"{t_sample:.2f} s), count time extrapolated by edges",
         "orient_s": t_orient, "count_s_extrapolated": t_count,
+        # the oracle's count of the whole graph when the sample is all of it
+        "triangles": sampled if e == m_dag else None,
     }
 
 
 def run_reference(a, rank, world):
+    """The reference path's CPU restatement on the host cores, on this
+    benchmark's workload.  The graph comes from the oracle's own generator
+    restatement, so this arm maps nothing of the product library."""
     if rank != 0:
         return 0
-    from mercury_b200 import Graph
     from oracle import oracle as orc
-    g = Graph.rmat(a.scale, a.edge_factor, seed=a.seed)
-    rp, col = np.asarray(g.rowptr), np.asarray(g.col)
-    m = len(col) // 2
+    rp, col = orc.rmat(a.scale, a.edge_factor, seed=a.seed)
+    n, m = len(rp) - 1, len(col) // 2
     # Size the per-step sample so W+K steps take a few minutes in total.
     steps_total = a.steps + a.warmup
     per_step_s = max(1.0, min(8.0, 150.0 / max(steps_total, 1)))
@@ -268,18 +341,23 @@ def run_reference(a, rank, world):
         t2 = time.perf_counter()
         if i >= a.warmup:
             times.append((t1 - t0) + (t2 - t1) * (len(dcol) / max(e, 1)))
-    step_s = statistics.mean(times)
+    step_s = min(times)  # best of the timed steps
     value = m / step_s
     line = {
         "metric": "TC edges/s", "value": value, "unit": "edges/s", "n_gpus": world,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": step_s * 1e3,
+        "mean_ms_per_step": statistics.mean(times) * 1e3,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "int32",
-        "data": "synthetic", "config": workload_config(a), "impl": "reference",
+        "data": "synthetic",
+        "config": {**workload_config(a), "n": n, "m": m,
+                   "parallelism": f"task-shard x{world}" if world > 1 else "1 GPU"},
+        "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "edges/s", "cores": orc.num_threads(),
                          "kind": "port",
                          "sample": f"per step: oracle orientation of the whole graph + merge "
                                    f"count over a hash-sampled 1/{k} of the sources, count "
-                                   f"time extrapolated by DAG edges"},
+                                   f"time extrapolated by DAG edges; value from the best of "
+                                   f"{len(times)} timed steps"},
         "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -385,12 +463,24 @@ def run_ours(a, rank, world, local_rank):
             assert tc_count_host(rp_np, col_np, tm) == count
         e2e_s = (time.perf_counter() - t0) / a.e2e_steps
         launches_e2e = int(tm.launches)
+        # The drop-in's own inputs: the loader's arrays in ordinary (pageable)
+        # host memory, which the driver copies through its staging buffers.
+        rp_pg, col_pg = np.array(g.rowptr), np.array(g.col)
+        assert tc_count_host(rp_pg, col_pg, tm) == count
+        t0 = time.perf_counter()
+        for _ in range(a.e2e_steps):
+            assert tc_count_host(rp_pg, col_pg, tm) == count
+        pg_s = (time.perf_counter() - t0) / a.e2e_steps
         e2e = {"value": m / e2e_s, "unit": "edges/s", "ms_per_step": e2e_s * 1e3,
                "h2d_bytes_per_step": int(rp_np.nbytes + col_np.nbytes),
                "d2h_bytes_per_step": 8 + 8 * 8 + 4,
                "timed_with": "host wall clock around each synchronous call",
-               "launches_per_step": launches_e2e}
-        del rp_pin, col_pin
+               "host_memory": "pinned",
+               "launches_per_step": launches_e2e,
+               "pageable": {"value": m / pg_s, "unit": "edges/s", "ms_per_step": pg_s * 1e3,
+                            "host_memory": "pageable (what TCSolver passes from the loader's "
+                                           "arrays)"}}
+        del rp_pin, col_pin, rp_pg, col_pg
 
     if rank != 0:
         if world > 1:
@@ -405,8 +495,18 @@ def run_ours(a, rank, world, local_rank):
     peak, peak_kind = load_peaks()
     hub_avg = statistics.mean(hub_ms)
     cnt_avg = statistics.mean(count_ms)
-    achieved = ab["b_hub"] / (hub_avg / 1e3) / 1e9
-    traffic = traffic_from_profile()
+    clk = clocks.summary()
+    # Parity at full size: the reference program's committed count for this
+    # graph and, when the CPU sample covers the whole graph, the oracle's.
+    ref_count = committed_reference_count(a)
+    if ref_count is not None:
+        assert count == ref_count, f"count {count} != reference program's {ref_count}"
+    cpu = None
+    if world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline(g, target_s=a.cpu_seconds)
+        if cpu.get("triangles") is not None:
+            assert count == cpu["triangles"], f"count {count} != oracle {cpu['triangles']}"
+    roof = hub_roofline(a, hub_avg, ab, peak, peak_kind, clk)
     line = {
         "metric": "TC edges/s", "value": value, "unit": "edges/s", "n_gpus": world,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_per_step,
@@ -417,23 +517,19 @@ def run_ours(a, rank, world, local_rank):
         "phases_ms": {"orient": statistics.mean(orient_ms), "count": cnt_avg, "hub_kernel": hub_avg,
                       "leaf_kernel": statistics.mean([t for t in (np.array(count_ms) - np.array(hub_ms))])},
         "count_phase_edges_per_s": m / (cnt_avg / 1e3),
-        "roofline": {"bound": "hbm", "kernel": "tc_hub_kernel", "achieved": achieved,
-                     "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_source": f"{peak_kind} hbm_gbs",
-                     "traffic": traffic,
-                     "algorithmic_bytes_per_launch": ab["b_hub"],
-                     "per_unit": "per DAG edge owned by a hub task: 12 B + 4 B x (d+u + d+v); "
-                                 "8 B per owner row"},
+        "roofline": roof,
+        "parity": {"reference_program_count": ref_count,
+                   "oracle_count": None if cpu is None else cpu.get("triangles")},
         "roofline_count_phase": {"b_tc": ab["b_tc"], "achieved_gbs": ab["b_tc"] / (cnt_avg / 1e3) / 1e9,
                                  "b_min_stream_shorter": ab["b_min"],
                                  "achieved_min_gbs": ab["b_min"] / (cnt_avg / 1e3) / 1e9},
         "tc_stats": stats,
         "gpu_launches": launches,
-        "clocks": clocks.summary(),
+        "clocks": clk,
         "e2e": e2e,
     }
-    if world == 1 and not a.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(g, target_s=a.cpu_seconds)
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
     dg.close()
     if world > 1:
@@ -603,11 +699,27 @@ def run_serve(a, local_rank):
     return 0
 
 
+def load_pattern_golden(a):
+    """Committed counts for this pattern workload (tests/golden/pattern_counts.json)."""
+    path = os.path.join(ROOT, "tests", "golden", "pattern_counts.json")
+    if not os.path.exists(path):
+        return {}
+    with open(path) as f:
+        rec = json.load(f)
+    key = f"chung_lu_n{a.pat_n}_mean{a.pat_mean:g}_cap{a.pat_cap:g}_seed1"
+    return rec.get(key, {}).get("counts", {})
+
+
 def run_patterns(a, rank, world, local_rank):
     """P1..P8 on one seeded Chung-Lu graph: count and device time per
     pattern (matches/s = count / kernel time; directed-edge tasks/s beside).
-    Under torchrun each rank holds the graph and counts its shard; the
-    partial counts are summed (mod 2^64) and the time is the max over ranks."""
+    With --pat-budget-ms, each pattern's first count runs under that budget
+    of device time (mc_pattern_count_budget: sliced launches, stopped between
+    slices); patterns that do not finish are named with the fraction of their
+    tasks done.  Counts are checked against tests/golden/pattern_counts.json
+    where it holds them.  Under torchrun each rank holds the graph and counts
+    its shard; the partial counts are summed (mod 2^64) and the time is the
+    max over ranks."""
     import torch
     from mercury_b200 import DeviceGraph, Graph
     torch.cuda.set_device(local_rank)
@@ -616,7 +728,8 @@ def run_patterns(a, rank, world, local_rank):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     g = Graph.chung_lu(a.pat_n, 2.1, a.pat_mean, a.pat_cap, seed=1)
-    per = []
+    golden = load_pattern_golden(a)
+    per, unfinished = [], []
     with DeviceGraph(g) as d:
         def count(k):
             if world == 1:
@@ -624,27 +737,46 @@ def run_patterns(a, rank, world, local_rank):
             part = d.pattern_count_shard(k, *shard_of(rank, world))
             return combine_ranks(part, d.last_timing.count_ms, "cuda")
         for k in range(1, 9):
-            first, _ = count(k)
-            ts = []
-            for _ in range(max(a.steps, 1)):
-                c, ms = count(k)
-                assert c == first
-                ts.append(ms)
+            if a.pat_budget_ms > 0 and world == 1:
+                first, frac = d.pattern_count_budget(k, a.pat_budget_ms)
+                if first is None:
+                    unfinished.append({"pattern": f"P{k}", "budget_ms": a.pat_budget_ms,
+                                       "tasks_done_fraction": frac})
+                    continue
+                ms = d.last_timing.count_ms
+                ts = [ms]
+                for _ in range(max(a.steps, 1) - 1):
+                    c, ms = count(k)
+                    assert c == first
+                    ts.append(ms)
+            else:
+                first, _ = count(k)
+                ts = []
+                for _ in range(max(a.steps, 1)):
+                    c, ms = count(k)
+                    assert c == first
+                    ts.append(ms)
+            if f"P{k}" in golden:
+                assert first == golden[f"P{k}"], f"P{k} {first} != committed {golden[f'P{k}']}"
             ms = statistics.mean(ts)
             per.append({"pattern": f"P{k}", "count": first, "ms": ms,
+                        "checked_against_committed": f"P{k}" in golden,
                         "matches_per_s": first / (ms / 1e3) if ms > 0 else None,
                         "edge_tasks_per_s": g.nnz / (ms / 1e3) if ms > 0 else None})
+            print(json.dumps({"progress": per[-1]}), file=sys.stderr, flush=True)
     if world > 1:
         dist.destroy_process_group()
         if rank != 0:
             return 0
-    line = {"metric": "P1-P8 matches/s", "value": statistics.mean(p["matches_per_s"] for p in per),
+    done = [p["matches_per_s"] for p in per if p["matches_per_s"]]
+    line = {"metric": "P1-P8 matches/s", "value": statistics.mean(done) if done else None,
             "unit": "matches/s", "n_gpus": world, "higher_is_better": True, "vs_baseline": None,
             "dtype": "int32", "data": "synthetic",
             "config": {"workload": f"Chung-Lu n={a.pat_n} gamma 2.1 mean {a.pat_mean} cap "
                                    f"{a.pat_cap} seed 1", "n": g.n, "m": g.nnz // 2,
-                       "max_degree": g.max_degree},
-            "patterns": per}
+                       "max_degree": g.max_degree,
+                       "budget_ms_per_pattern": a.pat_budget_ms if a.pat_budget_ms > 0 else None},
+            "patterns": per, "unfinished": unfinished}
     print(json.dumps(line), flush=True)
     return 0
 

@@ -59,10 +59,12 @@ inline bool is_blank(char c) { return c == ' ' || c == '\t' || c == '\r'; }
 inline bool parse_field(const char *&p, const char *end, int64_t &v) {
   while (p < end && is_blank(*p)) ++p;
   if (p >= end || *p < '0' || *p > '9') return false;
+  constexpr int64_t kMax = int64_t(1) << 62;
   int64_t x = 0;
   while (p < end && *p >= '0' && *p <= '9') {
-    x = x * 10 + (*p - '0');
-    if (x > (int64_t(1) << 62)) return false;
+    const int64_t d = *p - '0';
+    if (x > (kMax - d) / 10) return false;  // x * 10 + d would exceed 2^62
+    x = x * 10 + d;
     ++p;
   }
   if (p < end && !is_blank(*p) && *p != '\n') return false;

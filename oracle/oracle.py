@@ -47,6 +47,12 @@ def lib() -> C.CDLL:
         L.orc_pattern.restype = C.c_uint64
         L.orc_csr_build.argtypes = [C.c_int64, C.c_int64, P, P, P, P]
         L.orc_csr_build.restype = C.c_int64
+        L.orc_rmat_draws.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                     C.c_uint64, P, P]
+        L.orc_rmat_draws.restype = C.c_int64
+        L.orc_chung_lu_draws.argtypes = [C.c_int64, C.c_double, C.c_double, C.c_double,
+                                         C.c_uint64, P, P]
+        L.orc_chung_lu_draws.restype = C.c_int64
         _lib = L
     return _lib
 
@@ -149,3 +155,30 @@ def csr_build(src, dst, n: int):
     if nnz < 0:
         raise ValueError("id outside [0, n)")
     return rowptr, col[:nnz]
+
+
+def rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19,
+         seed: int = 1):
+    """Symmetric CSR (rowptr, col) of the seeded RMAT graph, built on the CPU
+    (gen_oracle.cpp + csr_oracle.cpp) without the product library."""
+    pairs = lib().orc_rmat_draws(scale, edge_factor, a, b, c, seed, None, None)
+    if pairs < 0:
+        raise ValueError("RMAT arguments outside the generator's range")
+    src = np.empty(pairs, dtype=np.int32)
+    dst = np.empty(pairs, dtype=np.int32)
+    lib().orc_rmat_draws(scale, edge_factor, a, b, c, seed, src.ctypes.data, dst.ctypes.data)
+    return csr_build(src, dst, 1 << scale)
+
+
+def chung_lu(n: int, gamma: float = 2.1, mean_degree: float = 20.0, max_weight: float = 50000.0,
+             seed: int = 1):
+    """Symmetric CSR (rowptr, col) of the seeded Chung-Lu graph, built on the
+    CPU without the product library."""
+    pairs = lib().orc_chung_lu_draws(n, gamma, mean_degree, max_weight, seed, None, None)
+    if pairs < 0:
+        raise ValueError("Chung-Lu arguments outside the generator's range")
+    src = np.empty(pairs, dtype=np.int32)
+    dst = np.empty(pairs, dtype=np.int32)
+    lib().orc_chung_lu_draws(n, gamma, mean_degree, max_weight, seed, src.ctypes.data,
+                             dst.ctypes.data)
+    return csr_build(src, dst, n)

@@ -3,7 +3,9 @@
 # own build system.  Outputs only go to _ref/ (git-ignored; it travels to the
 # GPU machine with the rest of the tree).  Used to pin parity against the
 # reference itself and to time it on the same GPU.
-REF ?= /root/reference
+# REF: the reference checkout (pass REF=...; default: "reference" beside the
+# repository root).
+REF ?= $(abspath ../../reference)
 OUT := _ref
 NVCC ?= nvcc
 CXX := g++

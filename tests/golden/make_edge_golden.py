@@ -28,7 +28,11 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "edges")
-TSV2MTX = "/root/reference/datasets/tsv2mtx.py"
+# The reference checkout: $MERCURY_REFERENCE_DIR, else "reference" beside the
+# repository.
+REFERENCE = os.environ.get("MERCURY_REFERENCE_DIR") or os.path.join(
+    os.path.dirname(os.path.dirname(os.path.dirname(HERE))), "reference")
+TSV2MTX = os.path.join(REFERENCE, "datasets", "tsv2mtx.py")
 
 
 def csr_digest(rowptr: np.ndarray, col: np.ndarray) -> str:

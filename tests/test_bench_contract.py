@@ -6,7 +6,9 @@ pinned for this path: per DAG edge u->v, 12 B plus 4 B x (d+u + d+v), plus
 the larger d+, ties to the larger id) has d+ above the leaf limit. These
 tests restate that formula with plain loops on small DAGs from the oracle's
 orientation and check the bench's vectorised form against it, and check the
-other inputs of the bench line (peaks, committed traffic, workload config).
+other inputs of the bench line (peaks, the ncu record of the hub kernel,
+the reference program's counts, the workload config), and that the CPU
+reference arm maps nothing of the product library.
 """
 import json
 import os
@@ -67,12 +69,70 @@ def test_peaks_come_from_the_measured_file_when_present():
         assert (peak, kind) == (6650.0, "fallback")
 
 
-def test_traffic_is_read_from_the_committed_hub_profile():
-    t = bench.traffic_from_profile()
-    assert t is not None and t > 0
-    with open(os.path.join(ROOT, "profiles", "tc_hub_kernel_rmat22.txt")) as f:
-        line = [ln for ln in f if ln.startswith("dram_bytes_per_launch")][0]
-    assert t == float(line.split("=")[1].split()[0])
+def _args(**kw):
+    d = dict(scale=22, edge_factor=16, seed=1, host_columns=False)
+    d.update(kw)
+    return SimpleNamespace(**d)
+
+
+def test_hub_counters_are_used_only_for_the_workload_they_were_captured_on(tmp_path, monkeypatch):
+    prof = tmp_path / "hub.txt"
+    prof.write_text("# ncu ...\ndram_bytes_per_launch = 2.5e10\nwarp_inst_per_launch = 8e9\n"
+                    "ncu_duration_ms = 11.0\n")
+    monkeypatch.setattr(bench, "HUB_DRAM_PROFILE", str(prof))
+    rec = bench.hub_profile(_args())
+    assert rec["dram_bytes_per_launch"] == 2.5e10 and rec["warp_inst_per_launch"] == 8e9
+    for other in (_args(scale=24), _args(scale=18), _args(edge_factor=8), _args(seed=2),
+                  _args(host_columns=True)):
+        assert bench.hub_profile(other) is None
+
+
+def test_hub_roofline_reports_measured_traffic_and_issue(tmp_path, monkeypatch):
+    prof = tmp_path / "hub.txt"
+    prof.write_text("dram_bytes_per_launch = 2.0e10\nwarp_inst_per_launch = 9.0e9\n"
+                    "ncu_duration_ms = 10.5\n")
+    monkeypatch.setattr(bench, "HUB_DRAM_PROFILE", str(prof))
+    ab = {"b_hub": 1.7e11}
+    roof = bench.hub_roofline(_args(), 10.0, ab, 6500.0, "measured", {"sm_mhz": 1965.0})
+    assert roof["traffic"] == 2.0e10
+    assert roof["achieved"] == pytest.approx(2.0e10 / 0.010 / 1e9)
+    assert roof["frac"] == pytest.approx(roof["achieved"] / 6500.0) and roof["frac"] <= 1.2
+    slots = 148 * 4 * 1965e6 * 0.010
+    assert roof["issue"]["frac"] == pytest.approx(9.0e9 / slots)
+    # The merge volume is kept as information only.
+    assert roof["algorithmic_gbs"] == pytest.approx(1.7e11 / 0.010 / 1e9)
+    # Without a record for the workload there is no traffic and no fraction.
+    roof = bench.hub_roofline(_args(scale=20), 10.0, ab, 6500.0, "measured", {"sm_mhz": 1965.0})
+    assert roof["traffic"] is None and roof["frac"] is None
+
+
+def test_committed_hub_record_parses_when_present():
+    if not os.path.exists(bench.HUB_DRAM_PROFILE):
+        pytest.skip("no committed ncu record of the hub kernel yet")
+    rec = bench.hub_profile(_args())
+    assert rec is not None and rec["dram_bytes_per_launch"] > 0
+
+
+def test_reference_count_record_matches_rmat_configs():
+    assert bench.committed_reference_count(_args()) == 2109663139
+    assert bench.committed_reference_count(_args(scale=16)) == 15715146
+    assert bench.committed_reference_count(_args(scale=23)) is None
+    assert bench.committed_reference_count(_args(seed=2)) is None
+
+
+def test_reference_arm_maps_no_product_library():
+    import subprocess
+    code = ("import sys; sys.argv = ['bench.py', '--impl', 'reference', '--scale', '10', "
+            "'--steps', '1', '--warmup', '1']; sys.path.insert(0, %r); import bench; "
+            "bench.main(); print('MAPPED', open('/proc/self/maps').read().count('libmercury_b200'))"
+            % ROOT)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300,
+                       cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = r.stdout.strip().splitlines()
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference" and line["config"]["m"] > 0
+    assert lines[-1] == "MAPPED 0"
 
 
 def test_workload_config_names_the_placement():

@@ -137,6 +137,10 @@ def test_empty_lists(tmp_path):
     ("1.5 2\n", MC_ERR_FORMAT),        # not an integer
     ("x y\n", MC_ERR_FORMAT),
     ("1 4294967297\n", MC_ERR_UNSUPPORTED),  # beyond int32 ids
+    ("1 4611686018427387904\n", MC_ERR_UNSUPPORTED),  # 2^62: a number, beyond int32 ids
+    ("1 4611686018427387905\n", MC_ERR_FORMAT),       # above 2^62: not read as a number
+    ("1 9999999999999999999\n", MC_ERR_FORMAT),       # 19 digits: x * 10 would pass 2^63
+    ("1 99999999999999999999\n", MC_ERR_FORMAT),      # 20 digits
 ])
 def test_bad_lines_are_refused(tmp_path, body, status):
     with pytest.raises(McError) as ex:

@@ -83,3 +83,19 @@ def test_division_sizes_cover_the_contributing_edges():
     assert d["small_edges"] + d["large_edges"] <= drp[-1]
     assert d["large_edges"] > 0
     assert d == GOLD["dense400"]["division"]
+
+
+@pytest.mark.parametrize("scale,ef,seed", [(8, 8, 3), (12, 16, 1), (14, 32, 7)])
+def test_rmat_restatement_equals_library_generator(scale, ef, seed):
+    from mercury_b200 import Graph
+    rp, col = orc.rmat(scale, ef, seed=seed)
+    g = Graph.rmat(scale, ef, seed=seed)
+    assert np.array_equal(rp, g.rowptr) and np.array_equal(col, g.col)
+
+
+@pytest.mark.parametrize("n,mean,cap,seed", [(5000, 10.0, 200.0, 1), (30000, 20.0, 5000.0, 2)])
+def test_chung_lu_restatement_equals_library_generator(n, mean, cap, seed):
+    from mercury_b200 import Graph
+    rp, col = orc.chung_lu(n, 2.1, mean, cap, seed=seed)
+    g = Graph.chung_lu(n, 2.1, mean, cap, seed=seed)
+    assert np.array_equal(rp, g.rowptr) and np.array_equal(col, g.col)
