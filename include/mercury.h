@@ -261,6 +261,20 @@ int mc_pattern_count_shard(mc_dgraph_t *g, int pattern, int shard,
                            int num_shards, uint64_t *partial,
                            mc_timing_t *timing);
 
+/* mc_pattern_count with a time budget.  The count runs as a sequence of
+ * launches over slices of its tasks, each sized from the previous one's
+ * measured time to last about MERCURY_PATTERN_SLICE_MS (default 250 ms);
+ * once the slices have used more than budget_ms of device time the count
+ * stops between two slices and returns MC_ERR_TIMEOUT (count not written).
+ * progress (optional) receives the fraction of the tasks done.  Graphs with
+ * a maximum degree above 4,096 are counted in slices by mc_pattern_count too
+ * (no budget): a hub edge alone can take seconds.  The reference has no
+ * budget; its kernels run to the end (subgraph_matching/sm_multigpu.cu:
+ * 150-200). */
+int mc_pattern_count_budget(mc_dgraph_t *g, int pattern, double budget_ms,
+                            uint64_t *count, double *progress,
+                            mc_timing_t *timing);
+
 /* Pattern count P<pattern> (1..8) of a symmetric CSR the caller already
  * holds in device memory (d_rowptr: int64[n+1], d_col: int32[nnz]), for
  * callers that cannot allocate device memory: a host application that owns
@@ -274,13 +288,19 @@ int mc_pattern_count_shard(mc_dgraph_t *g, int pattern, int shard,
  * graphs whose maximum degree leaves room for fewer than 8 warps
  * (max_degree > 174762) are refused with MC_ERR_UNSUPPORTED; larger
  * degrees run fewer warps.  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress) with that device current; make that
- * first call before any stream capture.  All calls share the array and its
- * last contents (the counters are cleared at the start of every call):
- * calls whose work overlaps on the GPU -- from two host threads, or on two
- * streams -- race and must be serialised by the caller.  `stream` is a
- * cudaStream_t (NULL: the default stream); the call returns after the count
- * is on the host.  The graph is checked like mc_dgraph_create (MC_ERR_FORMAT).
+ * device address (cudaGetSymbolAddress) with that device current, and looks
+ * it up again when the device's context has changed since (after a
+ * cudaDeviceReset, which reloads the module holding the array); make the
+ * first call on a device, and the first after a reset, before any stream
+ * capture.  All calls share the array and its last contents (the counters
+ * are cleared at the start of every call): calls whose work overlaps on the
+ * GPU -- from two host threads, or on two streams -- race and must be
+ * serialised by the caller.  `stream` is a cudaStream_t (NULL: the default
+ * stream); the call returns after the count is on the host.  Vertex ids in
+ * [0, n), ascending rows, no self-loops and monotone offsets are checked on
+ * the device (MC_ERR_FORMAT); symmetry is NOT checked here, and the count of
+ * a CSR that is not symmetric is meaningless (mc_graph_validate checks it on
+ * the host).
  * No counterpart in the reference, which allocates its frontier with
  * cudaMalloc (subgraph_matching/sm_multigpu.cu:117-122). */
 int mc_pattern_count_static(const int64_t *d_rowptr, const int32_t *d_col,
@@ -313,7 +333,10 @@ void mc_batch_free(mc_batch_t *b);
 /* ---- serving ---------------------------------------------------------------
  * A request loop with continuous batching (no reference counterpart).
  * Worker threads (each with its own stream) take every queued request that
- * fits the HBM budget -- up to max_batch per batch, in arrival order --
+ * fits the HBM budget -- up to max_batch per batch, in arrival order, and
+ * closing a batch once its estimated work (n + nnz per triangle job, the sum
+ * of squared degrees per pattern job) would pass 2^23 entry visits
+ * (MERCURY_SERVE_BATCH_WORK), so a request above that runs alone --
  * assemble the batch on the device, count it with the batch kernels and
  * deliver each graph's count; requests that arrive while batches run are
  * admitted as memory is returned, and batches of different workers overlap

@@ -118,6 +118,8 @@ SIGNATURES = {
     "mc_tc_count_host": (C.c_int, [_P, _P, _I64, _I64, _PU64, C.POINTER(Timing)]),
     "mc_pattern_count": (C.c_int, [_P, C.c_int, _PU64, C.POINTER(Timing)]),
     "mc_pattern_count_shard": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _PU64, C.POINTER(Timing)]),
+    "mc_pattern_count_budget": (C.c_int, [_P, C.c_int, C.c_double, _PU64,
+                                          C.POINTER(C.c_double), C.POINTER(Timing)]),
     "mc_pattern_count_static": (C.c_int, [_P, _P, _I64, _I64, C.c_int, _PU64, _P]),
     "mc_batch_create": (C.c_int, [_P, _P, _I64, _I64, _P, C.c_int, _P, _P, _PP]),
     "mc_batch_autotune": (C.c_int, [_P, _P]),

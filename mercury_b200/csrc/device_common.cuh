@@ -21,6 +21,7 @@ enum DeviceError : unsigned {
   kErrCapacity = 1u << 6,     // a scratch list exceeded its capacity
   kErrRank = 1u << 7,         // an out-list entry not ranked below its owner
   kErrDagCapacity = 1u << 8,  // more DAG entries than an exact-size DAG holds
+  kErrWaitTimeout = 1u << 9,  // a bounded wait for an asynchronous copy gave up
 };
 // Bits of the CSR contract checks.
 constexpr unsigned kErrContract = kErrIdRange | kErrUnsorted | kErrSelfLoop | kErrRowptr |

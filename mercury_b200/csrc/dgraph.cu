@@ -31,7 +31,8 @@ void release(mc_dgraph *g) {
                   g->leaf_tasks, g->scan_temp,  g->counters, g->err, g->pat_scratch,
                   g->mega_cnt,   g->mega_off,   g->mega_tasks, g->rank,
                   g->dag_rank,   g->rank_keys,  g->rank_counts, g->rank_offsets,
-                  g->center_scratch, g->stage, g->chunk_offsets, g->core_bits, g->pinfo};
+                  g->center_scratch, g->stage, g->chunk_offsets, g->core_bits, g->pinfo,
+                  g->hop_scratch, g->hub_bits};
   if (g->col_host) bufs[1] = nullptr;  // pinned host memory, freed below
   // Stream-ordered frees: no device-wide synchronisation, so other handles'
   // work keeps running while this one is released.

@@ -70,6 +70,10 @@ struct mc_dgraph {
   size_t pat_scratch_bytes = 0;
   void *center_scratch = nullptr;  // center classes of the bitmap kernels
   size_t center_scratch_bytes = 0;
+  void *hop_scratch = nullptr;     // two-hop rows of the centers (outer patterns)
+  size_t hop_scratch_bytes = 0;
+  void *hub_bits = nullptr;        // per-CTA id bitmaps of the large P1 centers
+  size_t hub_bits_bytes = 0;
 
   // ---- triangle-count scratch, allocated on the first mc_tc_count -------
   bool tc_ready = false;
@@ -149,8 +153,12 @@ int tc_count_launch(mc_dgraph *g, cudaEvent_t after_hub, int shard, int num_shar
 // patterns.cu: result of P<pattern>; c12 (optional) receives counters 1 and 2.
 // Shard `shard` of `num_shards` (0 of 1: the whole count); partial results
 // of all shards sum to the count modulo 2^64.
+// budget_ms > 0: slice the launches and stop with MC_ERR_TIMEOUT once the
+// sliced launches have used more device time than that; progress (optional)
+// receives the fraction of the sliced tasks done.
 int pattern_count(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12, mc_timing_t *timing,
-                  int shard = 0, int num_shards = 1);
+                  int shard = 0, int num_shards = 1, double budget_ms = -1.0,
+                  double *progress = nullptr);
 
 // Pattern tasks of a batch (see batch.cu): pattern graphs 0..num_graphs-1.
 struct BatchPatternArgs {

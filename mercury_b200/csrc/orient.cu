@@ -599,7 +599,8 @@ int tc_alloc(mc_dgraph *g) {
   MC_ALLOC(g->key, n + 1);
   MC_ALLOC(g->pinfo, n + 1);
   MC_ALLOC(g->dag_rowptr, n + 1);
-  MC_ALLOC(g->dag_col, g->dag_cap);
+  // 4 entries of padding: the staged hub kernel copies whole 16-byte groups.
+  MC_ALLOC(g->dag_col, g->dag_cap + 4);
   MC_ALLOC(g->keep, tiles * kTileThreads);
   MC_ALLOC(g->tile_counts, tiles);
   MC_ALLOC(g->tile_offsets, tiles + 1);
@@ -614,7 +615,7 @@ int tc_alloc(mc_dgraph *g) {
   MC_ALLOC(g->mega_tasks, g->task_capacity);
   if (ranked) {
     MC_ALLOC(g->rank, n + 1);
-    MC_ALLOC(g->dag_rank, g->dag_cap);
+    MC_ALLOC(g->dag_rank, g->dag_cap + 4);
     MC_ALLOC(g->rank_keys, 2 * n + 2);
     MC_ALLOC(g->rank_counts, radix_entries(n) + 1);
     MC_ALLOC(g->rank_offsets, radix_entries(n) + 1);

@@ -29,9 +29,12 @@
 // sign-extended).
 #include <algorithm>
 #include <climits>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+
+#include <cuda.h>
 
 #include "dgraph.cuh"
 #include "device_common.cuh"
@@ -64,6 +67,12 @@ struct PatArgs {
   // 0: the binary-search forms only (MERCURY_PATTERN_SETS=0; tests compare
   // both forms with it).
   int use_sets = 1;
+  // Slice [task_begin, task_end) of this shard's queue positions (task_end
+  // < 0: to the end); the queue counter starts at 0 for every slice.
+  int64_t task_begin = 0, task_end = -1;
+  // Budgeted count: stop at *deadline (globaltimer ns), raising *stop_flag.
+  const unsigned long long *deadline = nullptr;
+  unsigned long long *stop_flag = nullptr;
 };
 
 __device__ __forceinline__ unsigned long long wrap_mul(int a, int b) {
@@ -132,12 +141,35 @@ struct WarpSet {
   }
 };
 
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 struct Warp {
   const int64_t *__restrict__ rp;
   const int32_t *__restrict__ ci;
   int lane;
   int *H = nullptr;  // this warp's kSetSlots-int set table (null: none)
   unsigned *M = nullptr;  // this warp's 32 words of row masks
+  // A budgeted count: past *deadline (globaltimer ns) the warp stops and
+  // raises *stop_flag (the count is then incomplete and refused).
+  const unsigned long long *deadline = nullptr;
+  unsigned long long *stop_flag = nullptr;
+  // Warp-uniform: lane 0's clock decides (call from every lane).
+  __device__ __forceinline__ bool out_of_time() const {
+    if (!deadline) return false;
+    unsigned long long t = lane == 0 ? global_ns() : 0ull;
+    t = __shfl_sync(kFull, t, 0);
+    const bool late = t > *deadline;
+    if (late && lane == 0) atomicOr(stop_flag, 1ull);
+    return late;
+  }
+  // One lane's own check, for loops whose trip counts differ across lanes.
+  __device__ __forceinline__ bool lane_out_of_time() const {
+    return deadline && global_ns() > *deadline;
+  }
   __device__ __forceinline__ int deg(int v) const { return (int)(__ldg(rp + v + 1) - __ldg(rp + v)); }
   __device__ __forceinline__ const int32_t *N(int v) const { return ci + __ldg(rp + v); }
   // x in N(k), searched in k's list.
@@ -235,7 +267,10 @@ __device__ void pair_freq(const Warp &w, const int32_t *a, int na, int32_t *freq
   for (int j = w.lane; j < na; j += kWarp) {
     const int x = a[j];
     int f = 0;
-    for (int i = j + 1; i < na; ++i) f += !w.in(a[i], x);
+    for (int i = j + 1; i < na; ++i) {
+      if ((i & 1023) == 0 && w.lane_out_of_time()) break;
+      f += !w.in(a[i], x);
+    }
     freq[j] = f;
   }
   __syncwarp();
@@ -247,7 +282,10 @@ __device__ void cross_freq(const Warp &w, const int32_t *a, int na, const int32_
   for (int j = w.lane; j < na; j += kWarp) {
     const int x = a[j];
     int f = 0;
-    for (int i = 0; i < nl; ++i) f += !w.in(list[i], x);
+    for (int i = 0; i < nl; ++i) {
+      if ((i & 1023) == 1023 && w.lane_out_of_time()) break;
+      f += !w.in(list[i], x);
+    }
     freq[j] = f;
   }
   __syncwarp();
@@ -258,6 +296,7 @@ __device__ void cross_freq(const Warp &w, const int32_t *a, int na, const int32_
 __device__ void bounded_correction(const Warp &w, const int32_t *A, int nA, int32_t *D,
                                    int32_t *C, Acc &acc) {
   for (int i = 0; i < nA; ++i) {
+    if ((i & 15) == 15 && w.out_of_time()) return;
     const int v2 = A[i];
     const int nD = w.diff(A, nA, v2, v2, D);
     const int nC = w.inter(A, nA, v2, -1, C);
@@ -282,6 +321,7 @@ __device__ void edge_pattern(const Warp &w, int v0, int v1, int32_t *L, int64_t 
     const int nA = w.diff(n0, d0, v1, v1, L0);   // dif, bounded by v1
     const int nB = w.inter(n0, d0, v1, v1, L1);  // int, bounded by v1
     for (int i = 0; i < nB; ++i) {
+      if ((i & 15) == 15 && w.out_of_time()) return;
       const int v2 = L1[i];
       for (int j = w.lane; j < nA; j += kWarp) {
         const int key = L0[j];
@@ -293,10 +333,12 @@ __device__ void edge_pattern(const Warp &w, int v0, int v1, int32_t *L, int64_t 
     const int nB = w.diff(n1, d1, v0, -1, L1);
     cross_freq(w, L0, nA, L1, nB, L4);
     for (int i = 0; i < nA; ++i) {
+      if ((i & 15) == 15 && w.out_of_time()) return;
       const int c = w.count(L0, nA, L0[i], L0[i], false);
       if (w.lane == 0) acc.c1 += wrap_mul(c, L4[i]);
     }
     for (int i = 0; i < nB; ++i) {
+      if ((i & 15) == 15 && w.out_of_time()) return;
       const int v4 = L1[i];
       const int nD = w.diff(L0, nA, v4, -1, L2);
       const int nC = w.inter(L0, nA, v4, -1, L3);
@@ -312,6 +354,7 @@ __device__ void edge_pattern(const Warp &w, int v0, int v1, int32_t *L, int64_t 
     const int nA = w.diff(n0, d0, v1, -1, L0);
     pair_freq(w, L0, nA, L4);
     for (int i = 0; i < nA; ++i) {
+      if ((i & 15) == 15 && w.out_of_time()) return;
       const int c = w.count(L0, nA, L0[i], L0[i], false);
       if (w.lane == 0) acc.c1 += wrap_mul(c, L4[i]);
     }
@@ -330,6 +373,7 @@ __device__ void edge_pattern(const Warp &w, int v0, int v1, int32_t *L, int64_t 
       s0.clear(w.lane);
       s0.insert(inner, ni, 0, w.lane);
       for (int i = 0; i < no; ++i) {
+        if ((i & 15) == 15 && w.out_of_time()) return;
         const int common = warp_common(w, outer[i], s0, inner, ni);
         if (w.lane == 0) acc.c1 += (unsigned long long)(ni - common);
       }
@@ -337,6 +381,7 @@ __device__ void edge_pattern(const Warp &w, int v0, int v1, int32_t *L, int64_t 
       return;
     }
     for (int i = 0; i < no; ++i) {
+      if ((i & 15) == 15 && w.out_of_time()) return;
       const int v2 = outer[i];
       const int dv2 = w.deg(v2);
       if (dv2 < ni) {
@@ -372,6 +417,7 @@ __device__ void edge_pattern(const Warp &w, int v0, int v1, int32_t *L, int64_t 
         const int grp = w.lane / kGroup, sub = w.lane % kGroup;
         const int nb_round = (nB + kWarp / kGroup - 1) / (kWarp / kGroup) * (kWarp / kGroup);
         for (int j0 = 0; j0 < nb_round; j0 += kWarp / kGroup) {
+          if ((j0 & 255) == 252 && w.out_of_time()) return;
           const int j = j0 + grp;
           int ca = 0, cc = 0;
           if (j < nB) {
@@ -404,6 +450,7 @@ __device__ void edge_pattern(const Warp &w, int v0, int v1, int32_t *L, int64_t 
       // #{e in E : e not in N(c)} = nE - |N(c) & E| for c in D (the whole
       // warp per c: D is short).
       for (int i = 0; i < nA; ++i) {
+        if ((i & 15) == 15 && w.out_of_time()) return;
         const int v2 = L0[i];
         const int nD = w.inter(L2, nC, v2, -1, L3);
         if (nD == 0) continue;
@@ -428,6 +475,7 @@ __device__ void edge_pattern(const Warp &w, int v0, int v1, int32_t *L, int64_t 
     }
     __syncwarp();
     for (int i = 0; i < nB; ++i) {
+      if ((i & 15) == 15 && w.out_of_time()) return;
       const int f = L5[i];
       if (f == 0) continue;
       const int b = L1[i];
@@ -438,6 +486,7 @@ __device__ void edge_pattern(const Warp &w, int v0, int v1, int32_t *L, int64_t 
       if (w.lane == 0) acc.c1 += wrap_mul(t, f);
     }
     for (int i = 0; i < nA; ++i) {
+      if ((i & 15) == 15 && w.out_of_time()) return;
       const int v2 = L0[i];
       const int nD = w.inter(L2, nC, v2, -1, L3);  // C & N(v2)
       const int nE = w.diff(L1, nB, v2, -1, L4);   // B - N(v2)
@@ -450,6 +499,7 @@ __device__ void edge_pattern(const Warp &w, int v0, int v1, int32_t *L, int64_t 
     const int nA = w.inter(n0, d0, v1, -1, L0);
     const int nB = w.diff(n1, d1, v0, -1, L1);
     for (int i = 0; i < nA; ++i) {
+      if ((i & 15) == 15 && w.out_of_time()) return;
       const int v2 = L0[i];
       const int nD = w.diff(L0, nA, v2, -1, L2);
       const int nE = w.diff(L1, nB, v2, -1, L3);
@@ -520,6 +570,7 @@ __device__ void edge_pattern(const Warp &w, int v0, int v1, int32_t *L, int64_t 
     }
     pair_freq(w, L0, nA, L4);
     for (int i = 0; i < nA; ++i) {
+      if ((i & 15) == 15 && w.out_of_time()) return;
       const int c = w.count(L0, nA, L0[i], L0[i], false);
       if (w.lane == 0) acc.c1 += wrap_mul(c, L4[i]);
     }
@@ -595,10 +646,12 @@ __device__ void edge_pattern(const Warp &w, int v0, int v1, int32_t *L, int64_t 
     }
     cross_freq(w, L0, nA, L1, nB, L4);
     for (int i = 0; i < nA; ++i) {
+      if ((i & 15) == 15 && w.out_of_time()) return;
       const int c = w.count(L0, nA, L0[i], L0[i], true);
       if (w.lane == 0) acc.c1 += wrap_mul(c, L4[i]);
     }
     for (int i = 0; i < nB; ++i) {
+      if ((i & 15) == 15 && w.out_of_time()) return;
       const int v4 = L1[i];
       const int nD = w.diff(L0, nA, v4, -1, L2);
       const int nC = w.inter(L0, nA, v4, -1, L3);
@@ -622,11 +675,15 @@ __device__ void vertex_star(const Warp &w, int v0, int32_t *L, Acc &acc) {
   for (int i = w.lane; i < d; i += kWarp) {
     const int x = nb[i];
     int f = 0;
-    for (int j = i + 1; j < d; ++j) f += !w.in(nb[j], x);  // x < nb[j] iff j > i
+    for (int j = i + 1; j < d; ++j) {
+      if ((j & 1023) == 0 && w.lane_out_of_time()) break;
+      f += !w.in(nb[j], x);  // x < nb[j] iff j > i
+    }
     freq[i] = f;
   }
   __syncwarp();
   for (int i = 0; i < d; ++i) {
+    if ((i & 15) == 15 && w.out_of_time()) return;
     const int c = w.count(nb, d, nb[i], nb[i], false);
     if (w.lane == 0) acc.c1 += wrap_mul(c, freq[i]);
   }
@@ -643,15 +700,19 @@ __global__ void __launch_bounds__(kPatThreads) pattern_kernel(PatArgs a) {
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
   int32_t *L = a.scratch + gw * kLists * a.cap;
   const Warp w{a.rp, a.ci, lane, a.use_sets ? s_sets[threadIdx.x / kWarp] : nullptr,
-               a.use_sets ? s_rows[threadIdx.x / kWarp] : nullptr};
+               a.use_sets ? s_rows[threadIdx.x / kWarp] : nullptr, a.deadline, a.stop_flag};
   const int64_t all = kStar ? a.n : (a.task_off ? a.task_off[a.n] : a.nnz);
   const int64_t ntasks = all > a.shard ? (all - a.shard + a.num_shards - 1) / a.num_shards : 0;
+  const int64_t t_end = a.task_end >= 0 && a.task_end < ntasks ? a.task_end : ntasks;
+  const int64_t span = t_end - a.task_begin;
   Acc acc;
   for (;;) {
+    if (w.out_of_time()) break;
     unsigned long long t = 0;
     if (lane == 0) t = atomicAdd(a.queue, 1ull);
     t = __shfl_sync(kFull, t, 0);
-    if ((int64_t)t >= ntasks) break;
+    if ((int64_t)t >= span) break;
+    t += (unsigned long long)a.task_begin;
     t = t * (unsigned long long)a.num_shards + (unsigned long long)a.shard;
     if (kStar) {
       if (w.deg((int)t) > a.skip_deg) vertex_star(w, (int)t, L, acc);
@@ -721,6 +782,53 @@ struct CenterArgs {
   const int32_t *__restrict__ count;    // how many
   unsigned long long *queue;
   unsigned long long *counters;         // [0] = c1, [1] = c2
+  // Slice [c_begin, c_end) of the class's centers (c_end < 0: to the end);
+  // the queue counter starts at 0 for every slice.
+  int64_t c_begin = 0, c_end = -1;
+  // Outer patterns: hop_words words of global scratch per group (block b's
+  // group g at (b * groups + g) * hop_words) for the center's two-hop rows;
+  // null: rows are built per edge.
+  unsigned *hop = nullptr;
+  int64_t hop_words = 0;
+  // Budgeted count: stop at *deadline (globaltimer ns), raising *stop_flag.
+  const unsigned long long *deadline = nullptr;
+  unsigned long long *stop_flag = nullptr;
+};
+
+// Warp-uniform deadline check (lane 0's clock decides; call from every lane).
+__device__ __forceinline__ bool warp_late(const unsigned long long *deadline,
+                                          unsigned long long *flag, int lane) {
+  if (!deadline) return false;
+  unsigned long long t = lane == 0 ? global_ns() : 0ull;
+  t = __shfl_sync(kFull, t, 0);
+  const bool late = t > *deadline;
+  if (late && lane == 0) atomicOr(flag, 1ull);
+  return late;
+}
+
+// Two-hop rows of a center v0: for every vertex y outside N0 + {v0} with a
+// neighbour in N0, R(y) = N(y) & N0 as W words over N0's positions, built
+// once per center by walking the lists of N0's members (sum over x in N0 of
+// d(x) entries) instead of once per edge (v0, v1) for each y in N(v1) (sum
+// over y in N(v1) of d(y) entries per edge).  keys/vals: an open-addressing
+// map y -> row (2^lg slots, load <= 1/2).
+struct HopRows {
+  const int *keys;
+  const int *vals;
+  const unsigned *rows;
+  int lg;
+  int words;
+  __device__ __forceinline__ const unsigned *row_of(int y) const {
+    const unsigned mask = (1u << lg) - 1u;
+    unsigned h = ((unsigned)y * 2654435769u) >> (32 - lg);
+    for (int step = 0; step <= (int)mask; ++step) {
+      const int k = keys[h];
+      if (k == y) return rows + (int64_t)vals[h] * words;
+      if (k < 0) break;
+      h = (h + 1u) & mask;
+    }
+    return nullptr;  // not reached for a y with a neighbour in N0
+  }
 };
 
 // Word k of the mask of positions below q (q in [0, 32W)).
@@ -901,12 +1009,16 @@ __device__ __forceinline__ void center_outer_edges(const int64_t *__restrict__ r
                                                    const int32_t *__restrict__ ci,
                                                    const unsigned *M, const PosIndex &idx,
                                                    int v0, int wg, int G, int lane,
-                                                   unsigned *Rw, int *cnt, int *slots, Acc &acc) {
+                                                   unsigned *Rw, int *cnt, int *slots,
+                                                   const HopRows *hop,
+                                                   const unsigned long long *deadline,
+                                                   unsigned long long *stop_flag, Acc &acc) {
   const int32_t *n0 = idx.n0;
   const int d0 = idx.d0;
   unsigned *Rl = Rw + lane * W;
   const unsigned upto = lane == kWarp - 1 ? kFull : ((2u << lane) - 1u);
   for (int p = wg; p < d0; p += G) {
+    if (warp_late(deadline, stop_flag, lane)) break;
     const int v1 = n0[p];
     if (P == 4 && !(v1 < v0)) continue;
     const unsigned *mp = M + p * W;
@@ -943,9 +1055,18 @@ __device__ __forceinline__ void center_outer_edges(const int64_t *__restrict__ r
       if (use) slots[__popc(um & ((1u << lane) - 1u))] = y;
       const int nu = __popc(um);
       __syncwarp();
+      const bool mine = lane < nu;
+      if (hop) {
+        // R(y) from the center's two-hop rows: each lane copies its own.
+        if (mine) {
+          const unsigned *r = hop->row_of(slots[lane]);
+#pragma unroll
+          for (int k = 0; k < W; ++k) Rl[k] = r ? r[k] : 0u;
+        }
+        __syncwarp();
+      } else {
 #pragma unroll
       for (int k = 0; k < W; ++k) Rl[k] = 0;
-      const bool mine = lane < nu;
       int64_t ys = 0;
       int dy = 0;
       if (mine) {
@@ -972,6 +1093,7 @@ __device__ __forceinline__ void center_outer_edges(const int64_t *__restrict__ r
         started += __popc(starts);
       }
       __syncwarp();
+      }  // per-edge rows
       if (mine) {
       if (P == 4) {
         int c = 0;
@@ -1057,6 +1179,90 @@ __device__ __forceinline__ void center_outer_edges(const int64_t *__restrict__ r
   }
 }
 
+__device__ __forceinline__ void group_sync(int G) {
+  if (G == 1) __syncwarp();
+  else __syncthreads();
+}
+
+// Builds the two-hop rows of center v0 in this group's scratch.  Returns
+// false (every thread of the group alike) when they do not fit; the edges
+// then build their rows per edge.
+template <int W, int G>
+__device__ bool build_hop_rows(const CenterArgs &a, const PosIndex &idx, int v0, int grp, int gl,
+                               int wg, int lane, unsigned long long *s_walk, int *s_keys,
+                               int *s_rows, HopRows *out) {
+  constexpr int kGroups = kPatThreads / kWarp / G;
+  const int32_t *n0 = idx.n0;
+  const int d0 = idx.d0;
+  if (gl == 0) {
+    *s_walk = 0;
+    *s_keys = 0;
+    *s_rows = 0;
+  }
+  group_sync(G);
+  unsigned long long walk = 0;
+  for (int i = gl; i < d0; i += G * kWarp) {
+    const int x = n0[i];
+    walk += (unsigned long long)(__ldg(a.rp + x + 1) - __ldg(a.rp + x));
+  }
+  walk = warp_sum_u64(walk);
+  if (lane == 0 && walk) atomicAdd(s_walk, walk);
+  group_sync(G);
+  const unsigned long long B = *s_walk;
+  int lg = 6;
+  while ((1ull << lg) < 2 * B) ++lg;
+  const int64_t cap = int64_t(1) << lg;
+  if (lg > 30 || 2 * cap > a.hop_words) return false;  // the same on every thread
+  unsigned *base = a.hop + ((int64_t)blockIdx.x * kGroups + grp) * a.hop_words;
+  int *keys = reinterpret_cast<int *>(base);
+  int *vals = keys + cap;
+  unsigned *rows = reinterpret_cast<unsigned *>(vals + cap);
+  const unsigned mask = (unsigned)cap - 1u;
+  for (int64_t j = gl; j < cap; j += G * kWarp) keys[j] = -1;
+  group_sync(G);
+  // Keys: every y outside N0 + {v0} adjacent to a member of N0 (at most B
+  // distinct, so the map's load stays <= 1/2 and every probe ends).
+  for (int i = wg; i < d0; i += G) {
+    const int x = n0[i];
+    const int64_t b = __ldg(a.rp + x), e = __ldg(a.rp + x + 1);
+    for (int64_t t = b + lane; t < e; t += kWarp) {
+      const int y = __ldg(a.ci + t);
+      if (y == v0 || idx.find(y) >= 0) continue;
+      unsigned h = ((unsigned)y * 2654435769u) >> (32 - lg);
+      for (int64_t step = 0; step < cap; ++step) {
+        const int old = atomicCAS(keys + h, -1, y);
+        if (old == -1) {
+          atomicAdd(s_keys, 1);
+          break;
+        }
+        if (old == y) break;
+        h = (h + 1u) & mask;
+      }
+    }
+  }
+  group_sync(G);
+  const int64_t nkeys = *s_keys;
+  if (2 * cap + nkeys * W > a.hop_words) return false;  // the same on every thread
+  for (int64_t j = gl; j < cap; j += G * kWarp)
+    if (keys[j] >= 0) vals[j] = atomicAdd(s_rows, 1);
+  for (int64_t j = gl; j < nkeys * W; j += G * kWarp) rows[j] = 0u;
+  group_sync(G);
+  const HopRows hr{keys, vals, rows, lg, W};
+  for (int i = wg; i < d0; i += G) {
+    const int x = n0[i];
+    const int64_t b = __ldg(a.rp + x), e = __ldg(a.rp + x + 1);
+    for (int64_t t = b + lane; t < e; t += kWarp) {
+      const int y = __ldg(a.ci + t);
+      if (y == v0 || idx.find(y) >= 0) continue;
+      const unsigned *r = hr.row_of(y);
+      if (r) atomicOr(const_cast<unsigned *>(r) + (i >> 5), 1u << (i & 31));
+    }
+  }
+  group_sync(G);
+  *out = hr;
+  return true;
+}
+
 // Persistent groups of G warps take centers of this class from the queue.
 template <int P, int W>
 __global__ void __launch_bounds__(kPatThreads) center_kernel(CenterArgs a) {
@@ -1075,12 +1281,20 @@ __global__ void __launch_bounds__(kPatThreads) center_kernel(CenterArgs a) {
   // Position hash of N0 (outer patterns, W >= 4), after all warps' scratch.
   int *hkeys = reinterpret_cast<int *>(n0 + 32 * W) +
                (center_outer(P) ? center_group(W) * (64 * W + 32) : 0);
-  const int total = *a.count;
+  const int64_t count = *a.count;
+  const int64_t limit = a.c_end >= 0 && a.c_end < count ? a.c_end : count;
+  __shared__ unsigned long long s_hop_walk[kGroups];
+  __shared__ int s_hop_keys[kGroups], s_hop_rows[kGroups];
   Acc acc;
   for (;;) {
     if (gl == 0) {
-      const unsigned long long t = atomicAdd(a.queue, 1ull);
-      s_center[grp] = (int64_t)t < total ? a.centers[t] : -1;
+      if (a.deadline && global_ns() > *a.deadline) {
+        atomicOr(a.stop_flag, 1ull);
+        s_center[grp] = -1;
+      } else {
+        const int64_t t = a.c_begin + (int64_t)atomicAdd(a.queue, 1ull);
+        s_center[grp] = t < limit ? a.centers[t] : -1;
+      }
     }
     if (G == 1) __syncwarp(); else __syncthreads();
     const int v0 = s_center[grp];
@@ -1124,9 +1338,15 @@ __global__ void __launch_bounds__(kPatThreads) center_kernel(CenterArgs a) {
         acc.c1 += wrap_mul(c, f);
       }
     }
-    if constexpr (center_outer(P))
-      center_outer_edges<P, W>(a.rp, a.ci, M, idx, v0, wg, G, lane, Rw, cnt, slots, acc);
-    else
+    if constexpr (center_outer(P)) {
+      const HopRows *hop = nullptr;
+      HopRows hr{};
+      if (a.hop && build_hop_rows<W, G>(a, idx, v0, grp, gl, wg, lane, s_hop_walk + grp,
+                                        s_hop_keys + grp, s_hop_rows + grp, &hr))
+        hop = &hr;
+      center_outer_edges<P, W>(a.rp, a.ci, M, idx, v0, wg, G, lane, Rw, cnt, slots, hop,
+                               a.deadline, a.stop_flag, acc);
+    } else
       center_edges<P, W>(M, d0, wg, G, lane, acc);
     if (G == 1) __syncwarp(); else __syncthreads();  // M and n0 are rewritten next
   }
@@ -1135,6 +1355,171 @@ __global__ void __launch_bounds__(kPatThreads) center_kernel(CenterArgs a) {
     if (c1) atomicAdd(a.counters + 0, c1);
     if (c2) atomicAdd(a.counters + 1, c2);
   }
+}
+
+// ---- P1 on the centers above kCenterMaxDeg ----------------------------------
+// One CTA per (center v0, chunk of kHubEdgeChunk of its edges), persistent
+// over an atomic queue.  The CTA marks N0 = N(v0) in its own bitmap over the
+// vertex ids (global memory, n bits, cleared again after the task), so that
+// "x in N0" is one bit read.  Chunk 0 also adds v0's star term.  With
+// positions in N0 equal to id order (N0 is sorted):
+//   star  (P1_frequency_count, pattern_kernels.cuh:68-133): for x = N0[i],
+//         lo / hi = neighbours of x in N0 below / above x;
+//         c1 += wrap32((i - lo) * ((d0 - 1 - i) - hi))
+//   edge (v0, v1 = N0[p]) (P1_count_correction, :6-66): B = N1 & N0 below v1
+//         (ascending), and for v2 = B[t]
+//         c2 += #{k in N0 : v2 < k < v1, k notin N1, k notin N(v2)}
+//             = (p - pos(v2) - 1) - (|B| - 1 - t)
+//               - #{k in N(v2) : v2 < k < v1, k in N0, k notin N1}
+// These are the sizes of the reference's sets A = N0 - N1 and B = N0 & N1
+// (both below v1) and its pair test, counted through the symmetry of the
+// graph; the per-vertex products are the same 32-bit products.
+constexpr int kHubEdgeChunk = 256;
+
+struct HubP1Args {
+  const int64_t *__restrict__ rp;
+  const int32_t *__restrict__ ci;
+  int64_t n;
+  const int64_t *chunk_off;  // exclusive scan of the chunks per vertex (n + 1)
+  unsigned *bits;            // per CTA: ceil(n / 32) words, all zero between tasks
+  int32_t *scratch;          // per warp: cap ints (the list B)
+  int64_t cap;
+  unsigned long long *queue;
+  unsigned long long *counters;  // [0] c1, [1] c2
+  int shard, num_shards;
+  const unsigned long long *deadline = nullptr;
+  unsigned long long *stop_flag = nullptr;
+  int64_t task_begin = 0, task_end = -1;  // slice of the queue positions
+};
+
+__device__ __forceinline__ int warp_sum_int(int v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
+__device__ __forceinline__ bool bit_set(const unsigned *bits, int v) {
+  return (bits[v >> 5] >> (v & 31)) & 1u;
+}
+
+// Position of y in the ascending list[0, n) (y present).
+__device__ __forceinline__ int lower_pos(const int32_t *__restrict__ list, int n, int y) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(list + mid) < y) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(kPatThreads) hub_p1_kernel(HubP1Args a) {
+  constexpr int kWarps = kPatThreads / kWarp;
+  __shared__ long long s_task;
+  const int lane = threadIdx.x & (kWarp - 1), warp = threadIdx.x / kWarp;
+  unsigned *bits = a.bits + (int64_t)blockIdx.x * ((a.n + 31) >> 5);
+  int32_t *B = a.scratch + ((int64_t)blockIdx.x * kWarps + warp) * a.cap;
+  const int64_t all = __ldg(a.chunk_off + a.n);
+  const int64_t ntasks = all > a.shard ? (all - a.shard + a.num_shards - 1) / a.num_shards : 0;
+  const int64_t t_end = a.task_end >= 0 && a.task_end < ntasks ? a.task_end : ntasks;
+  const int64_t span = t_end - a.task_begin;
+  Acc acc;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      long long t = (long long)atomicAdd(a.queue, 1ull);
+      if (a.deadline && global_ns() > *a.deadline) {
+        atomicOr(a.stop_flag, 1ull);
+        t = span;
+      }
+      s_task = t;
+    }
+    __syncthreads();
+    const int64_t q = s_task;
+    if (q >= span) break;
+    const int64_t t = (a.task_begin + q) * a.num_shards + a.shard;
+    const int v0 = (int)upper_row(a.chunk_off, 0, a.n - 1, t);
+    const int chunk = (int)(t - __ldg(a.chunk_off + v0));
+    const int64_t b0 = __ldg(a.rp + v0);
+    const int d0 = (int)(__ldg(a.rp + v0 + 1) - b0);
+    const int32_t *n0 = a.ci + b0;
+    for (int i = threadIdx.x; i < d0; i += kPatThreads) {
+      const int y = __ldg(n0 + i);
+      atomicOr(bits + (y >> 5), 1u << (y & 31));
+    }
+    __syncthreads();
+    if (chunk == 0) {  // the star term of v0
+      for (int i = warp; i < d0; i += kWarps) {
+        const int x = __ldg(n0 + i);
+        const int64_t bx = __ldg(a.rp + x), ex = __ldg(a.rp + x + 1);
+        int lo = 0, hi = 0;
+        for (int64_t k = bx + lane; k < ex; k += kWarp) {
+          const int y = __ldg(a.ci + k);
+          if (bit_set(bits, y)) {
+            if (y < x) ++lo;
+            else ++hi;
+          }
+        }
+        lo = warp_sum_int(lo);
+        hi = warp_sum_int(hi);
+        if (lane == 0) acc.c1 += wrap_mul(i - lo, (d0 - 1 - i) - hi);
+      }
+    }
+    const int p_end = min(d0, (chunk + 1) * kHubEdgeChunk);
+    for (int p = chunk * kHubEdgeChunk + warp; p < p_end; p += kWarps) {
+      const int v1 = __ldg(n0 + p);
+      const int64_t b1 = __ldg(a.rp + v1);
+      const int d1 = (int)(__ldg(a.rp + v1 + 1) - b1);
+      const int32_t *n1 = a.ci + b1;
+      // B = N1 & N0 below v1, in order (ballot compaction).
+      int nb = 0;
+      for (int base = 0; base < d1; base += kWarp) {
+        const int k = base + lane;
+        const int y = k < d1 ? __ldg(n1 + k) : INT_MAX;
+        const bool keep = y < v1 && bit_set(bits, y);
+        const unsigned m = __ballot_sync(kFull, keep);
+        if (keep) B[nb + __popc(m & ((1u << lane) - 1u))] = y;
+        nb += __popc(m);
+        if (__any_sync(kFull, y >= v1)) break;
+      }
+      __syncwarp();
+      unsigned long long c2 = 0;
+      for (int tb = lane; tb < nb; tb += kWarp) {
+        const int v2 = B[tb];
+        long long term = (long long)(p - lower_pos(n0, d0, v2) - 1) - (nb - 1 - tb);
+        const int64_t b2 = __ldg(a.rp + v2), e2 = __ldg(a.rp + v2 + 1);
+        // N(v2) from its first entry above v2, up to v1.
+        int64_t lo = b2, hi = e2;
+        while (lo < hi) {
+          const int64_t mid = (lo + hi) >> 1;
+          if (__ldg(a.ci + mid) <= v2) lo = mid + 1;
+          else hi = mid;
+        }
+        for (int64_t k = lo; k < e2; ++k) {
+          const int y = __ldg(a.ci + k);
+          if (y >= v1) break;
+          if (bit_set(bits, y) && !bsearch(n1, d1, y)) --term;
+        }
+        c2 += (unsigned long long)term;
+      }
+      acc.c2 += c2;
+      __syncwarp();  // B is rewritten by the warp's next edge
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < d0; i += kPatThreads) bits[__ldg(n0 + i) >> 5] = 0u;
+    __syncthreads();
+  }
+  const unsigned long long c1 = warp_sum_u64(acc.c1), c2 = warp_sum_u64(acc.c2);
+  if (lane == 0) {
+    if (c1) atomicAdd(a.counters + 0, c1);
+    if (c2) atomicAdd(a.counters + 1, c2);
+  }
+}
+
+// chunks[v] = ceil(big_deg[v] / kHubEdgeChunk).
+__global__ void hub_chunks_kernel(const int32_t *__restrict__ big_deg, int64_t n,
+                                  int32_t *__restrict__ chunks) {
+  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < n) chunks[v] = (big_deg[v] + kHubEdgeChunk - 1) / kHubEdgeChunk;
 }
 
 // Splits the vertices into the six center classes (1 <= degree <= 1024;
@@ -1166,8 +1551,71 @@ __global__ void center_classes_kernel(const int64_t *__restrict__ rp, int64_t n,
   if (cls >= 0) lists[(int64_t)cls * n + base[cls] + slot] = (int32_t)v;
 }
 
+// Long pattern counts run in slices of their task range, each a launch of
+// bounded length, so that no kernel runs for minutes and a caller's time
+// budget can end the count between two slices.  Slices are sized from the
+// previous slice's measured time (first slice: one task per resident warp or
+// group, then x(target / measured), clamped to [1/4, 4]).
+struct Slicer {
+  bool on = false;
+  double budget_ms = -1.0;  // < 0: no budget
+  double target_ms = 250.0;
+  bool trace = false;
+  double used_ms = 0.0;     // device time of the sliced launches so far
+  int64_t tasks_total = 0, tasks_done = 0, slices = 0;
+  // With a budget the kernels also stop by themselves at a device deadline
+  // (a single hub edge can outlast any slice); stop_flag is the device word
+  // they raise, and h_stop its host copy.
+  unsigned long long *stop_flag = nullptr;
+  unsigned long long *h_stop = nullptr;
+};
+
+__global__ void set_deadline_kernel(unsigned long long *deadline, unsigned long long budget_ns) {
+  *deadline = global_ns() + budget_ns;
+}
+
+// launch(begin, end) runs tasks [begin, end) of a launch whose queue counter
+// is `queue`; total = the launch's task count, first = first slice size.
+template <class Launch>
+int run_slices(mc_dgraph *g, Slicer &sl, const char *what, int64_t total, int64_t first,
+               unsigned long long *queue, Launch launch) {
+  if (!sl.on) return launch(0, -1);
+  if (total <= 0) return MC_OK;
+  cudaStream_t s = g->stream;
+  sl.tasks_total += total;
+  int64_t b = 0, size = std::max<int64_t>(first, 1);
+  while (b < total) {
+    const int64_t e = std::min(total, b + size);
+    MC_CUDA_TRY(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s));
+    MC_CUDA_TRY(cudaEventRecord(g->ev[4], s));
+    const int rc = launch(b, e);
+    if (rc != MC_OK) return rc;
+    if (sl.stop_flag)
+      MC_CUDA_TRY(cudaMemcpyAsync(sl.h_stop, sl.stop_flag, sizeof(unsigned long long),
+                                  cudaMemcpyDeviceToHost, s));
+    MC_CUDA_TRY(cudaEventRecord(g->ev[5], s));
+    MC_CUDA_TRY(cudaEventSynchronize(g->ev[5]));
+    float ms = 0.f;
+    MC_CUDA_TRY(cudaEventElapsedTime(&ms, g->ev[4], g->ev[5]));
+    sl.used_ms += ms;
+    sl.tasks_done += e - b;
+    sl.slices += 1;
+    if (sl.trace)
+      std::fprintf(stderr, "mercury: %s slice [%lld, %lld) of %lld: %.3f ms (total %.1f ms)\n",
+                   what, (long long)b, (long long)e, (long long)total, ms, sl.used_ms);
+    b = e;
+    if (sl.h_stop && *sl.h_stop) return MC_ERR_TIMEOUT;  // stopped at the deadline
+    if (sl.budget_ms > 0 && sl.used_ms > sl.budget_ms && b < total) return MC_ERR_TIMEOUT;
+    // Never below one task per resident warp or group: a smaller slice
+    // leaves the GPU idle.
+    const double f = ms > 0.01f ? std::min(4.0, std::max(0.25, sl.target_ms / ms)) : 4.0;
+    size = std::max<int64_t>(std::max<int64_t>(first, 1), (int64_t)((double)size * f));
+  }
+  return MC_OK;
+}
+
 template <int P, int W>
-int launch_center(mc_dgraph *g, const CenterArgs &a, int num_sms) {
+int launch_center(mc_dgraph *g, const CenterArgs &a, int num_sms, int64_t total, Slicer *sl) {
   constexpr int G = center_group(W);
   const size_t smem = center_group_bytes(P, W) * (kPatThreads / kWarp / G);
   auto kern = center_kernel<P, W>;
@@ -1176,30 +1624,61 @@ int launch_center(mc_dgraph *g, const CenterArgs &a, int num_sms) {
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPatThreads, smem) != cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
-  kern<<<num_sms * per_sm, kPatThreads, smem, g->stream>>>(a);
-  MC_CUDA_TRY(cudaGetLastError());
-  g->launches += 1;
-  return MC_OK;
+  const int grid = num_sms * per_sm;
+  CenterArgs ha = a;
+  if (center_outer(P) && a.hop) {
+    // The scratch split evenly over the resident groups, at most 2^21 words each.
+    const int64_t groups = (int64_t)grid * (kPatThreads / kWarp / G);
+    ha.hop_words = std::min<int64_t>(int64_t(1) << 21,
+                                     (int64_t)(g->hop_scratch_bytes / sizeof(unsigned)) / groups);
+    // MERCURY_HOP_WORDS lowers the share (tests use it to send the larger
+    // centers to the per-edge rows).
+    if (const char *env = std::getenv("MERCURY_HOP_WORDS"))
+      ha.hop_words = std::min<int64_t>(ha.hop_words, std::atoll(env));
+  } else {
+    ha.hop = nullptr;
+  }
+  return run_slices(g, *sl, "centers", total, (int64_t)grid * (kPatThreads / kWarp / G), a.queue,
+                    [&](int64_t b, int64_t e) {
+                      CenterArgs sa = ha;
+                      sa.c_begin = b;
+                      sa.c_end = e;
+                      kern<<<grid, kPatThreads, smem, g->stream>>>(sa);
+                      MC_CUDA_TRY(cudaGetLastError());
+                      g->launches += 1;
+                      return MC_OK;
+                    });
 }
 
 template <int P>
-int launch_center_class(mc_dgraph *g, const CenterArgs &a, int cls) {
+int launch_center_class(mc_dgraph *g, const CenterArgs &a, int cls, int64_t total, Slicer *sl) {
   switch (cls) {
-    case 0: return launch_center<P, 1>(g, a, g->num_sms);
-    case 1: return launch_center<P, 2>(g, a, g->num_sms);
-    case 2: return launch_center<P, 4>(g, a, g->num_sms);
-    case 3: return launch_center<P, 8>(g, a, g->num_sms);
-    case 4: return launch_center<P, 16>(g, a, g->num_sms);
-    default: return launch_center<P, 32>(g, a, g->num_sms);
+    case 0: return launch_center<P, 1>(g, a, g->num_sms, total, sl);
+    case 1: return launch_center<P, 2>(g, a, g->num_sms, total, sl);
+    case 2: return launch_center<P, 4>(g, a, g->num_sms, total, sl);
+    case 3: return launch_center<P, 8>(g, a, g->num_sms, total, sl);
+    case 4: return launch_center<P, 16>(g, a, g->num_sms, total, sl);
+    default: return launch_center<P, 32>(g, a, g->num_sms, total, sl);
   }
 }
 
+// all: task count before sharding (n for star tasks, the restricted edge
+// count with task_off, else nnz).
 template <int P, bool kStar>
-int launch_pattern(mc_dgraph *g, const PatArgs &a, int grid) {
-  pattern_kernel<P, kStar><<<grid, kPatThreads, 0, g->stream>>>(a);
-  MC_CUDA_TRY(cudaGetLastError());
-  g->launches += 1;
-  return MC_OK;
+int launch_pattern(mc_dgraph *g, const PatArgs &a, int grid, int64_t all, Slicer *sl) {
+  const int64_t ntasks =
+      all > a.shard ? (all - a.shard + a.num_shards - 1) / a.num_shards : 0;
+  return run_slices(g, *sl, kStar ? "stars" : "edges", ntasks,
+                    (int64_t)grid * (kPatThreads / kWarp), a.queue,
+                    [&](int64_t b, int64_t e) {
+                      PatArgs sa = a;
+                      sa.task_begin = b;
+                      sa.task_end = e;
+                      pattern_kernel<P, kStar><<<grid, kPatThreads, 0, g->stream>>>(sa);
+                      MC_CUDA_TRY(cudaGetLastError());
+                      g->launches += 1;
+                      return MC_OK;
+                    });
 }
 
 int grid_blocks(mc_dgraph *g, int64_t cap) {
@@ -1315,7 +1794,7 @@ namespace {
 // warp-per-edge kernel's searches.
 bool pattern_uses_centers(int pattern) { return pattern == 1 || pattern == 2 || pattern == 3; }
 
-int center_path(mc_dgraph *g, int pattern, PatArgs a, int grid) {
+int center_path(mc_dgraph *g, int pattern, PatArgs a, int grid, Slicer *sl) {
   cudaStream_t s = g->stream;
   const int64_t n = g->n;
   // Scratch: class lists (kCenterClasses * n), class counts and queues,
@@ -1326,7 +1805,9 @@ int center_path(mc_dgraph *g, int pattern, PatArgs a, int grid) {
   const size_t off_b = sizeof(int64_t) * (size_t)(n + 1);
   const size_t temp_b = scan_temp_bytes(n);
   auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
-  const size_t need = up(lists_b) + words_b + up(deg_b) + up(off_b) + up(temp_b);
+  // P1: per-vertex chunk counts of the large centers and their scan.
+  const size_t need = up(lists_b) + words_b + up(deg_b) + up(off_b) + up(temp_b) +
+                      (pattern == 1 ? up(deg_b) + up(off_b) : 0);
   if (need > g->center_scratch_bytes) {
     if (g->center_scratch) dev_free(g->center_scratch, s);
     g->center_scratch = nullptr;
@@ -1343,6 +1824,23 @@ int center_path(mc_dgraph *g, int pattern, PatArgs a, int grid) {
   int64_t *big_off = reinterpret_cast<int64_t *>(reinterpret_cast<char *>(big_deg) + up(deg_b));
   void *temp = reinterpret_cast<char *>(big_off) + up(off_b);
 
+  // Two-hop rows of the outer patterns: 1 GiB of scratch (or an eighth of the
+  // free memory, if less) shared out among the resident groups of each class
+  // launch.  MERCURY_HOP_ROWS=0: rows per edge only.
+  const char *hop_env = std::getenv("MERCURY_HOP_ROWS");
+  const bool hop_on = center_outer(pattern) && !(hop_env && std::atoi(hop_env) == 0);
+  if (hop_on) {
+    size_t free_b = 0, total_b = 0;
+    MC_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    const size_t want = std::min<size_t>(size_t(1) << 30, free_b / 8) & ~size_t(255);
+    if (want > g->hop_scratch_bytes) {
+      if (g->hop_scratch) dev_free(g->hop_scratch, s);
+      g->hop_scratch = nullptr;
+      g->hop_scratch_bytes = 0;
+      MC_CUDA_TRY(dev_alloc(&g->hop_scratch, want, s));
+      g->hop_scratch_bytes = want;
+    }
+  }
   MC_CUDA_TRY(cudaMemsetAsync(words, 0, words_b, s));
   center_classes_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
       g->rowptr, n, a.shard, a.num_shards, lists, counts, big_deg);
@@ -1357,37 +1855,82 @@ int center_path(mc_dgraph *g, int pattern, PatArgs a, int grid) {
   for (int c = 0; c < kCenterClasses; ++c) {
     if (h_counts[c] == 0) continue;
     CenterArgs ca{g->rowptr, g->col, lists + (int64_t)c * n, counts + c, queues + c, g->counters};
+    ca.hop = hop_on ? static_cast<unsigned *>(g->hop_scratch) : nullptr;
+    ca.deadline = a.deadline;
+    ca.stop_flag = a.stop_flag;
     int rc = MC_OK;
+    const int64_t tc = h_counts[c];
     switch (pattern) {
-      case 1: rc = launch_center_class<1>(g, ca, c); break;
-      case 2: rc = launch_center_class<2>(g, ca, c); break;
-      case 3: rc = launch_center_class<3>(g, ca, c); break;
-      case 4: rc = launch_center_class<4>(g, ca, c); break;
-      case 5: rc = launch_center_class<5>(g, ca, c); break;
-      case 6: rc = launch_center_class<6>(g, ca, c); break;
-      case 7: rc = launch_center_class<7>(g, ca, c); break;
-      default: rc = launch_center_class<8>(g, ca, c); break;
+      case 1: rc = launch_center_class<1>(g, ca, c, tc, sl); break;
+      case 2: rc = launch_center_class<2>(g, ca, c, tc, sl); break;
+      case 3: rc = launch_center_class<3>(g, ca, c, tc, sl); break;
+      case 4: rc = launch_center_class<4>(g, ca, c, tc, sl); break;
+      case 5: rc = launch_center_class<5>(g, ca, c, tc, sl); break;
+      case 6: rc = launch_center_class<6>(g, ca, c, tc, sl); break;
+      case 7: rc = launch_center_class<7>(g, ca, c, tc, sl); break;
+      default: rc = launch_center_class<8>(g, ca, c, tc, sl); break;
     }
     if (rc != MC_OK) return rc;
+  }
+  // P1 on the larger centers: hub_p1_kernel (MERCURY_HUB_P1=0: the
+  // warp-per-edge kernel, as for the other patterns).
+  const char *hub_env = std::getenv("MERCURY_HUB_P1");
+  if (pattern == 1 && big_total > 0 && !(hub_env && std::atoi(hub_env) == 0)) {
+    int32_t *chunks = reinterpret_cast<int32_t *>(reinterpret_cast<char *>(temp) + up(temp_b));
+    int64_t *chunk_off = reinterpret_cast<int64_t *>(reinterpret_cast<char *>(chunks) + up(deg_b));
+    hub_chunks_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(big_deg, n, chunks);
+    MC_CUDA_TRY(cudaGetLastError());
+    MC_CUDA_TRY(exclusive_scan(chunks, chunk_off, n, temp, s));
+    g->launches += 1 + scan_launches(n);
+    int64_t total_chunks = 0;
+    MC_CUDA_TRY(cudaMemcpyAsync(&total_chunks, chunk_off + n, sizeof(int64_t),
+                                cudaMemcpyDeviceToHost, s));
+    MC_CUDA_TRY(cudaStreamSynchronize(s));
+    // One id bitmap per CTA, zero between tasks (cleared here as well, in
+    // case an earlier count stopped at its deadline mid-task).
+    const size_t bits_b = sizeof(unsigned) * (size_t)((n + 31) / 32) * (size_t)grid;
+    if (bits_b > g->hub_bits_bytes) {
+      if (g->hub_bits) dev_free(g->hub_bits, s);
+      g->hub_bits = nullptr;
+      g->hub_bits_bytes = 0;
+      MC_CUDA_TRY(dev_alloc(&g->hub_bits, bits_b, s));
+      g->hub_bits_bytes = bits_b;
+    }
+    MC_CUDA_TRY(cudaMemsetAsync(g->hub_bits, 0, bits_b, s));
+    HubP1Args ha{g->rowptr, g->col, n, chunk_off, static_cast<unsigned *>(g->hub_bits),
+                 a.scratch, a.cap, g->counters + 3, g->counters, a.shard, a.num_shards,
+                 a.deadline, a.stop_flag};
+    const int64_t ntasks = total_chunks > a.shard
+                               ? (total_chunks - a.shard + a.num_shards - 1) / a.num_shards
+                               : 0;
+    return run_slices(g, *sl, "hub P1", ntasks, grid, ha.queue, [&](int64_t b, int64_t e) {
+      HubP1Args sa = ha;
+      sa.task_begin = b;
+      sa.task_end = e;
+      hub_p1_kernel<<<grid, kPatThreads, 0, s>>>(sa);
+      MC_CUDA_TRY(cudaGetLastError());
+      g->launches += 1;
+      return MC_OK;
+    });
   }
   // Larger centers: the warp-per-edge kernel over their edges only.
   a.skip_deg = kCenterMaxDeg;
   if (pattern == 1) {
-    int rc = launch_pattern<1, true>(g, a, grid);  // stars of degree > kCenterMaxDeg
+    int rc = launch_pattern<1, true>(g, a, grid, n, sl);  // stars of degree > kCenterMaxDeg
     if (rc != MC_OK) return rc;
     a.queue = g->counters + 3;
   }
   if (big_total > 0) {
     a.task_off = big_off;
     switch (pattern) {
-      case 1: return launch_pattern<1, false>(g, a, grid);
-      case 2: return launch_pattern<2, false>(g, a, grid);
-      case 3: return launch_pattern<3, false>(g, a, grid);
-      case 4: return launch_pattern<4, false>(g, a, grid);
-      case 5: return launch_pattern<5, false>(g, a, grid);
-      case 6: return launch_pattern<6, false>(g, a, grid);
-      case 7: return launch_pattern<7, false>(g, a, grid);
-      default: return launch_pattern<8, false>(g, a, grid);
+      case 1: return launch_pattern<1, false>(g, a, grid, big_total, sl);
+      case 2: return launch_pattern<2, false>(g, a, grid, big_total, sl);
+      case 3: return launch_pattern<3, false>(g, a, grid, big_total, sl);
+      case 4: return launch_pattern<4, false>(g, a, grid, big_total, sl);
+      case 5: return launch_pattern<5, false>(g, a, grid, big_total, sl);
+      case 6: return launch_pattern<6, false>(g, a, grid, big_total, sl);
+      case 7: return launch_pattern<7, false>(g, a, grid, big_total, sl);
+      default: return launch_pattern<8, false>(g, a, grid, big_total, sl);
     }
   }
   return MC_OK;
@@ -1395,9 +1938,22 @@ int center_path(mc_dgraph *g, int pattern, PatArgs a, int grid) {
 
 }  // namespace
 
+// Graphs whose largest degree exceeds this run their pattern launches in
+// slices (hub edges can take seconds each; see Slicer).
+constexpr int64_t kSliceDegree = 4096;
+
 int pattern_count(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12, mc_timing_t *timing,
-                  int shard, int num_shards) {
+                  int shard, int num_shards, double budget_ms, double *progress) {
   NvtxRange range("pattern_count");
+  // MERCURY_PATTERN_SLICE=1/0 forces slicing on/off (the tests compare both);
+  // MERCURY_PATTERN_SLICE_MS sets the target slice length; MERCURY_TRACE_SLICES
+  // prints each slice to stderr.
+  Slicer sl;
+  sl.budget_ms = budget_ms;
+  sl.on = budget_ms > 0 || g->max_degree > kSliceDegree;
+  if (const char *env = std::getenv("MERCURY_PATTERN_SLICE")) sl.on = std::atoi(env) != 0 || budget_ms > 0;
+  if (const char *env = std::getenv("MERCURY_PATTERN_SLICE_MS")) sl.target_ms = std::max(0.01, std::atof(env));
+  sl.trace = std::getenv("MERCURY_TRACE_SLICES") != nullptr;
   cudaStream_t s = g->stream;
   const int64_t launches_before = g->launches;
   MC_CUDA_TRY(cudaMemsetAsync(g->counters, 0, sizeof(unsigned long long) * 8, s));
@@ -1417,6 +1973,17 @@ int pattern_count(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12, mc_ti
             g->counters + 0, g->counters + 2};
   a.shard = shard;
   a.num_shards = num_shards;
+  if (budget_ms > 0) {
+    // counters[5]: the deadline, counters[6]: the stop flag (zeroed above).
+    set_deadline_kernel<<<1, 1, 0, s>>>(g->counters + 5,
+                                        (unsigned long long)(budget_ms * 1e6));
+    MC_CUDA_TRY(cudaGetLastError());
+    a.deadline = g->counters + 5;
+    a.stop_flag = g->counters + 6;
+    sl.stop_flag = g->counters + 6;
+    sl.h_stop = g->h_counters + 6;
+    g->h_counters[6] = 0;
+  }
   if (const char *env = std::getenv("MERCURY_PATTERN_SETS")) a.use_sets = std::atoi(env) != 0;
   MC_CUDA_TRY(cudaEventRecord(g->ev[0], s));
   int rc = MC_OK;
@@ -1428,32 +1995,39 @@ int pattern_count(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12, mc_ti
     if (route && std::strcmp(route, "edge") == 0) centers = false;
     if (route && std::strcmp(route, "centers") == 0) centers = true;
     if (pattern < 1 || pattern > 8) return MC_ERR_ARG;
+    const int64_t n = g->n, nnz = g->nnz;
     if (centers) {
-      rc = center_path(g, pattern, a, grid);
+      rc = center_path(g, pattern, a, grid, &sl);
     } else {
       switch (pattern) {
         case 1:
-          rc = launch_pattern<1, true>(g, a, grid);
+          rc = launch_pattern<1, true>(g, a, grid, n, &sl);
           if (rc == MC_OK) {
             a.queue = g->counters + 3;
-            rc = launch_pattern<1, false>(g, a, grid);
+            rc = launch_pattern<1, false>(g, a, grid, nnz, &sl);
           }
           break;
-        case 2: rc = launch_pattern<2, false>(g, a, grid); break;
-        case 3: rc = launch_pattern<3, false>(g, a, grid); break;
-        case 4: rc = launch_pattern<4, false>(g, a, grid); break;
-        case 5: rc = launch_pattern<5, false>(g, a, grid); break;
-        case 6: rc = launch_pattern<6, false>(g, a, grid); break;
-        case 7: rc = launch_pattern<7, false>(g, a, grid); break;
-        default: rc = launch_pattern<8, false>(g, a, grid); break;
+        case 2: rc = launch_pattern<2, false>(g, a, grid, nnz, &sl); break;
+        case 3: rc = launch_pattern<3, false>(g, a, grid, nnz, &sl); break;
+        case 4: rc = launch_pattern<4, false>(g, a, grid, nnz, &sl); break;
+        case 5: rc = launch_pattern<5, false>(g, a, grid, nnz, &sl); break;
+        case 6: rc = launch_pattern<6, false>(g, a, grid, nnz, &sl); break;
+        case 7: rc = launch_pattern<7, false>(g, a, grid, nnz, &sl); break;
+        default: rc = launch_pattern<8, false>(g, a, grid, nnz, &sl); break;
       }
     }
   }
-  if (rc != MC_OK) return rc;
+  if (progress)
+    *progress = sl.tasks_total > 0 ? (double)sl.tasks_done / (double)sl.tasks_total : 1.0;
+  if (rc != MC_OK) {
+    cudaStreamSynchronize(s);  // nothing of this call is left running
+    return rc;
+  }
   MC_CUDA_TRY(cudaEventRecord(g->ev[3], s));
   MC_CUDA_TRY(cudaMemcpyAsync(g->h_counters, g->counters, sizeof(unsigned long long) * 8,
                               cudaMemcpyDeviceToHost, s));
   MC_CUDA_TRY(cudaStreamSynchronize(s));
+  if (budget_ms > 0 && g->h_counters[6]) return MC_ERR_TIMEOUT;  // a kernel stopped early
   const unsigned long long c1 = g->h_counters[0], c2 = g->h_counters[1];
   *out = (pattern == 4 || pattern == 6) ? c1 : c1 - c2;
   if (c12) {
@@ -1485,6 +2059,13 @@ extern "C" int mc_pattern_count_shard(mc_dgraph_t *g, int pattern, int shard, in
   return mc::pattern_count(g, pattern, partial, nullptr, timing, shard, num_shards);
 }
 
+extern "C" int mc_pattern_count_budget(mc_dgraph_t *g, int pattern, double budget_ms,
+                                       uint64_t *count, double *progress, mc_timing_t *timing) {
+  if (!g || !count || pattern < 1 || pattern > 8 || !(budget_ms > 0)) return MC_ERR_ARG;
+  MC_CUDA_TRY(cudaSetDevice(g->device));
+  return mc::pattern_count(g, pattern, count, nullptr, timing, 0, 1, budget_ms, progress);
+}
+
 // ---- pattern count without allocation --------------------------------------
 // mc_pattern_count_static: the same kernels as mc_pattern_count over a CSR the
 // caller already holds in device memory, with every byte of scratch taken from
@@ -1503,22 +2084,57 @@ constexpr int kMaxStaticDevices = 64;
 struct StaticScratch {
   int32_t *frontier = nullptr;
   unsigned long long *words = nullptr;
-  bool ready = false;
+  unsigned long long ctx_id = 0;  // context the addresses belong to (0: none)
 };
 StaticScratch g_static_scratch[kMaxStaticDevices];
 std::mutex g_static_mu;
 
+// Unique id of the calling thread's current CUDA context (0 if none), read
+// through the driver entry points the runtime exposes, so the library links
+// no driver library.  A device's primary context is destroyed by
+// cudaDeviceReset and created anew on the next runtime call; the module
+// holding the arrays is then loaded again and their addresses may change.
+unsigned long long current_context_id() {
+  using GetCurrent = CUresult (*)(CUcontext *);
+  using GetId = CUresult (*)(CUcontext, unsigned long long *);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {
+    cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = q1;
+    void *f1 = nullptr, *f2 = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) == cudaSuccess &&
+        cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) == cudaSuccess &&
+        q1 == cudaDriverEntryPointSuccess && q2 == cudaDriverEntryPointSuccess) {
+      get_current = reinterpret_cast<GetCurrent>(f1);
+      get_id = reinterpret_cast<GetId>(f2);
+    }
+    looked_up = true;
+  }
+  if (!get_current || !get_id) return 0;
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
 // Device addresses of the file-scope arrays on device `dev` (the current
 // device).  The host-side names are stand-ins, not device addresses; the
-// addresses come from cudaGetSymbolAddress, once per device.
+// addresses come from cudaGetSymbolAddress, looked up once per device and
+// again whenever the device's context is not the one they were taken in
+// (after a cudaDeviceReset, for example).
 int static_scratch(int dev, StaticScratch *out) {
   if (dev < 0 || dev >= kMaxStaticDevices) return MC_ERR_UNSUPPORTED;
+  // cudaSetDevice makes the device's primary context current (creating it
+  // if needed), so the context id below is the one the kernels will use.
+  MC_CUDA_TRY(cudaSetDevice(dev));
+  const unsigned long long ctx = current_context_id();  // 0: unknown, look up again
   std::lock_guard<std::mutex> lock(g_static_mu);
   StaticScratch &s = g_static_scratch[dev];
-  if (!s.ready) {
+  if (!s.frontier || ctx == 0 || s.ctx_id != ctx) {
     MC_CUDA_TRY(cudaGetSymbolAddress((void **)&s.frontier, g_static_frontier));
     MC_CUDA_TRY(cudaGetSymbolAddress((void **)&s.words, g_static_words));
-    s.ready = true;
+    s.ctx_id = ctx;
   }
   *out = s;
   return MC_OK;

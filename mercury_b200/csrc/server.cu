@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <list>
@@ -35,6 +36,7 @@ struct Resident {
   int64_t *rowptr = nullptr;
   int32_t *col = nullptr;
   int64_t n = 0, nnz = 0, max_degree = 0;
+  int64_t sumsq = 0;  // sum of squared degrees (the pattern work estimate)
   int64_t bytes = 0;
   int pins = 0;  // batches currently using it
   cudaStream_t owner = nullptr;
@@ -47,6 +49,7 @@ struct Request {
   std::vector<int64_t> rowptr;
   std::vector<int32_t> col;
   int64_t n = 0, nnz = 0, max_degree = 0;
+  int64_t sumsq = 0;
   Clock::time_point submitted;
   bool prepinned = false;  // resident graph pinned at submission (no arrays copied)
   bool done = false;
@@ -75,6 +78,14 @@ __global__ void set_last_kernel(int64_t *urp, int64_t n, int64_t nnz) { urp[n] =
 
 int64_t csr_bytes(int64_t n, int64_t nnz) { return 8 * (n + 1) + 4 * nnz; }
 
+// Estimated device work of a request, in entry visits: a triangle job
+// streams its CSR (n + nnz); a pattern job's per-edge sets grow with the
+// degrees at both ends (sum of squared degrees).  A batch is closed once
+// its estimate would pass the server's cap, and a request above the cap on
+// its own runs in a batch of its own, so one large graph never holds a
+// whole batch of small ones behind it.
+int64_t work_of(const Request &r) { return r.job == 0 ? r.n + r.nnz : std::max(r.sumsq, r.nnz); }
+
 // Device memory one request needs inside a batch: its CSR three times
 // (resident copy, batch union, handle copy) and the orientation scratch of a
 // triangle job.  Pattern jobs also share the batch's frontier lists
@@ -100,6 +111,7 @@ struct mc_server {
   int device = 0;
   int64_t budget = 0;
   int max_batch = 0;
+  int64_t batch_work = 0;  // cap on a batch's estimated work (see work_of)
   std::mutex mu;
   std::condition_variable work_cv, done_cv;
   std::deque<std::shared_ptr<mc::Request>> pending;
@@ -259,6 +271,7 @@ void run_batch(mc_server *s, std::vector<std::shared_ptr<Request>> &batch, int64
           res.n = r.n;
           res.nnz = r.nnz;
           res.max_degree = r.max_degree;
+          res.sumsq = r.sumsq;
           res.bytes = bytes;
           res.pins = 1;
           s->cache[r.key] = res;
@@ -308,14 +321,17 @@ void worker_main(mc_server *s) {
   cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
   for (;;) {
     std::vector<std::shared_ptr<Request>> batch;
-    int64_t reserved = 0, pattern_cap = 0;
+    int64_t reserved = 0, pattern_cap = 0, work = 0;
     {
       std::unique_lock<std::mutex> lock(s->mu);
       for (;;) {
         if (s->stop && s->pending.empty()) break;
-        // Admit queued requests in arrival order while they fit the budget.
+        // Admit queued requests in arrival order while they fit the budget
+        // and the batch's work cap.
         while (!s->pending.empty() && (int)batch.size() < s->max_batch) {
           auto &r = s->pending.front();
+          const int64_t w = work_of(*r);
+          if (!batch.empty() && work + w > s->batch_work) break;  // next batch
           int64_t f = footprint(*r);
           const int64_t cap = r->job != 0 ? std::max(pattern_cap, r->max_degree) : pattern_cap;
           if (cap > pattern_cap) f += pattern_scratch(cap) - (pattern_cap ? pattern_scratch(pattern_cap) : 0);
@@ -337,8 +353,10 @@ void worker_main(mc_server *s) {
             break;  // wait for memory from running batches
           reserved += f;
           pattern_cap = cap;
+          work += w;
           batch.push_back(r);
           s->pending.pop_front();
+          if (work > s->batch_work) break;  // a large request runs alone
         }
         if (!batch.empty()) break;
         s->work_cv.wait(lock);
@@ -368,6 +386,11 @@ int mc_server_create(int64_t hbm_budget_bytes, int max_batch, int workers, mc_se
   cudaGetDevice(&s->device);
   s->budget = hbm_budget_bytes;
   s->max_batch = max_batch;
+  // MERCURY_SERVE_BATCH_WORK overrides the default cap of 2^23 entry visits
+  // (about 4 ms of batch kernels on a B200).
+  s->batch_work = int64_t(1) << 23;
+  if (const char *env = std::getenv("MERCURY_SERVE_BATCH_WORK"))
+    s->batch_work = std::max<int64_t>(1, std::atoll(env));
   for (int i = 0; i < workers; ++i) s->workers.emplace_back(mc::worker_main, s);
   *out = s;
   return MC_OK;
@@ -390,6 +413,7 @@ int mc_server_submit(mc_server_t *s, const int64_t *rowptr, const int32_t *col, 
       r->n = it->second.n;
       r->nnz = it->second.nnz;
       r->max_degree = it->second.max_degree;
+      r->sumsq = it->second.sumsq;
       ++it->second.pins;
       r->prepinned = true;
     }
@@ -405,7 +429,11 @@ int mc_server_submit(mc_server_t *s, const int64_t *rowptr, const int32_t *col, 
     }
     r->n = n;
     r->nnz = nnz;
-    for (int64_t v = 0; v < n; ++v) r->max_degree = std::max(r->max_degree, rowptr[v + 1] - rowptr[v]);
+    for (int64_t v = 0; v < n; ++v) {
+      const int64_t d = rowptr[v + 1] - rowptr[v];
+      r->max_degree = std::max(r->max_degree, d);
+      r->sumsq += d * d;
+    }
   }
   r->submitted = mc::Clock::now();
   {

@@ -17,6 +17,7 @@
 // no branch.
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 
 #include "dgraph.cuh"
 #include "device_common.cuh"
@@ -53,6 +54,7 @@ struct CountArgs {
   int dense_factor;  // dense when the AND's words <= dense_factor x list length
   int shard, num_shards;  // this call counts tasks shard, shard + num_shards, ...
   BatchView bv;           // per-graph table factor and counts of a batch
+  int stage_off;          // staged hub kernel: start of the copy slots (ints)
 };
 
 // log2 of the table slots per key of owner x's graph (4 slots per key by
@@ -292,6 +294,115 @@ __device__ __forceinline__ unsigned stream_n(const int32_t *__restrict__ lists, 
   return h;
 }
 
+// ---- bulk-copy staging of long partner lists (MERCURY_TC_TMA=1) -----------
+// Each warp owns two 1 KB slots of shared memory and two mbarriers.  Lane 0
+// copies the next chunk of the claimed lists (up to 252 entries) from global
+// memory into one slot with cp.async.bulk (no multicast: this GPU's own
+// memory, one CTA) while the warp probes the chunk already in the other
+// slot.  A bulk copy starts and ends on 16-byte boundaries, so a chunk's
+// start is rounded down to a multiple of 4 entries and its end up (the list
+// arrays carry 4 entries of padding for that); the warp indexes the slot
+// from the remainder.
+constexpr int kStageInts = 256;
+constexpr int kStageChunk = kStageInts - 4;
+constexpr size_t kStageBytes = (size_t)(kCountThreads / kWarp) * 2 * kStageInts * sizeof(int);
+constexpr int kWaitSpins = 1 << 20;  // try_wait rounds before a wait gives up
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+}
+// Lane 0: expect `bytes` on bar, then copy them (16-byte aligned, multiple of 16).
+__device__ __forceinline__ void bulk_copy(void *dst, const void *src, unsigned bytes,
+                                          unsigned long long *bar) {
+  // The warp's earlier (generic) reads of dst are ordered before this
+  // asynchronous write by the __syncwarp before the call and this fence.
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+// Waits for the phase of `parity` on bar; false after kWaitSpins rounds.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
+  for (int i = 0; i < kWaitSpins; ++i) {
+    unsigned done = 0;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+struct Stage {
+  int *slot[2];                  // this warp's two slots
+  unsigned long long *bar;       // this warp's two mbarriers
+  unsigned phase;                // bit s: parity of slot s's next completion
+  unsigned *err;
+};
+
+// The N claimed lists (starts st[i], lengths len[i]) as chunks through the
+// two slots; returns this lane's hits.  A wait that gives up raises
+// kErrWaitTimeout and waits once more for the copy before returning.
+template <int N, class Probe>
+__device__ __forceinline__ unsigned stream_n_staged(const int32_t *__restrict__ lists,
+                                                    const long long *st, const int *len,
+                                                    int lane, const Probe &probe, Stage &sg) {
+  int ci = 0;
+  while (ci < N && len[ci] <= 0) ++ci;
+  if (ci >= N) return 0;
+  int co = 0, s = 0;
+  auto issue = [&](int i, int o, int slot) {
+    if (lane == 0) {
+      const long long first = st[i] + o;
+      const long long a = first & ~3LL;
+      const int cnt = min(kStageChunk, len[i] - o);
+      const unsigned bytes = (unsigned)((((first - a) + cnt + 3) & ~3LL) * sizeof(int));
+      bulk_copy(sg.slot[slot], lists + a, bytes, sg.bar + slot);
+    }
+  };
+  issue(ci, co, s);
+  unsigned h = 0;
+  for (;;) {
+    // The chunk after (ci, co), issued into the other slot before waiting.
+    int ni = ci, no = co + kStageChunk;
+    if (no >= len[ni]) {
+      no = 0;
+      ++ni;
+      while (ni < N && len[ni] <= 0) ++ni;
+    }
+    if (ni < N) issue(ni, no, s ^ 1);
+    const unsigned parity = (sg.phase >> s) & 1u;
+    if (!mbar_wait(sg.bar + s, parity)) {
+      if (lane == 0) atomicOr(sg.err, kErrWaitTimeout);
+      mbar_wait(sg.bar + s, parity);
+      if (ni < N) mbar_wait(sg.bar + (s ^ 1), (sg.phase >> (s ^ 1)) & 1u);
+      return h;
+    }
+    sg.phase ^= 1u << s;
+    const int shift = (int)((st[ci] + co) & 3LL);
+    const int cnt = min(kStageChunk, len[ci] - co);
+    const int *buf = sg.slot[s] + shift;
+    for (int k = lane; k < cnt; k += kWarp) h += probe(buf[k]);
+    __syncwarp();  // every lane is done with slot s before it is refilled
+    if (ni >= N) break;
+    ci = ni;
+    co = no;
+    s ^= 1;
+  }
+  return h;
+}
+
 // The short stream: warp w takes windows of 32 x kU consecutive elements
 // (w, w + 8, ...), lane l element window + 32u + l, so every load
 // instruction reads one 128-byte span and every lane has kU loads in
@@ -369,12 +480,12 @@ __device__ __forceinline__ unsigned and_count_n(const unsigned *bits, int owner_
 // All partner lists of the task: the long ones (two per claim) and the
 // dense partners (four per claim) claimed by the warps, then the short
 // stream.  Returns this thread's hits.
-template <class Probe>
+template <bool kStaged, class Probe>
 __device__ __forceinline__ unsigned long long stream_partners(const int32_t *__restrict__ lists,
                                                               const long long *s_base,
                                                               const int *s_off, Partners pt,
                                                               int *s_next, int warp, int lane,
-                                                              const Probe &probe,
+                                                              const Probe &probe, Stage &sg,
                                                               const unsigned *bits = nullptr,
                                                               int owner_bits = 0,
                                                               const unsigned *core = nullptr) {
@@ -395,7 +506,8 @@ __device__ __forceinline__ unsigned long long stream_partners(const int32_t *__r
         st[i] = a < pt.nl ? s_base[a] : 0;
         len[i] = a < pt.nl ? s_off[a] : 0;
       }
-      hits += stream_n<kNL>(lists, st, len, lane, probe);
+      if constexpr (kStaged) hits += stream_n_staged<kNL>(lists, st, len, lane, probe, sg);
+      else hits += stream_n<kNL>(lists, st, len, lane, probe);
     } else {
       int ry[kND];
 #pragma unroll
@@ -447,16 +559,34 @@ __device__ __forceinline__ int ceil_log2(int v) { return v <= 1 ? 0 : 32 - __clz
 // as ranks), else as a cuckoo table of 2^lg slots (load <= 1/4 when it fits,
 // <= 1/2 at the size cap).  Owners beyond the cap, or whose table could not
 // be built, are probed by binary search in global memory instead.
-__global__ void __launch_bounds__(kCountThreads, 5) tc_hub_kernel(CountArgs a) {
-  extern __shared__ int table[];
+// kStaged: long partner lists through the bulk-copy slots (stream_n_staged),
+// which follow the table in dynamic shared memory at a.stage_off ints.
+// (The copy slots' 16 KB leave room for 4 CTAs per SM, which the register
+// bound then follows.)
+template <bool kStaged>
+__global__ void __launch_bounds__(kCountThreads, kStaged ? 4 : 5) tc_hub_kernel(CountArgs a) {
+  extern __shared__ __align__(128) int table[];
   __shared__ unsigned long long s_task;
   __shared__ int s_fail, s_next;
   __shared__ long long s_base[kHubChunk];
   __shared__ int s_off[kHubChunk + 1];
   __shared__ unsigned long long s_warp[kCountThreads / kWarp];
+  __shared__ unsigned long long s_bar[kStaged ? kCountThreads / kWarp * 2 : 1];
   const int lane = threadIdx.x & (kWarp - 1), warp = threadIdx.x / kWarp;
   const int64_t ntasks = shard_tasks(a);
   unsigned long long hits = 0;
+  Stage sg{{nullptr, nullptr}, s_bar + (kStaged ? 2 * warp : 0), 0u, a.err};
+  if constexpr (kStaged) {
+    int *base = table + a.stage_off + warp * 2 * kStageInts;
+    sg.slot[0] = base;
+    sg.slot[1] = base + kStageInts;
+    if (lane == 0) {
+      mbar_init(sg.bar);
+      mbar_init(sg.bar + 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+  }
   // Thread 0 claims each task one task ahead, so the queue atomic's latency
   // overlaps the current task.
   unsigned long long t_next = 0;
@@ -529,15 +659,16 @@ __global__ void __launch_bounds__(kCountThreads, 5) tc_hub_kernel(CountArgs a) {
     use_table = use_table && s_fail == 0;
     unsigned long long th = 0;
     if (bitmap)
-      th = stream_partners(a.dag_rank, s_base, s_off, pt, &s_next, warp, lane,
-                           BitmapProbe{reinterpret_cast<const unsigned *>(table), (unsigned)R},
-                           reinterpret_cast<const unsigned *>(table), R, a.core);
+      th = stream_partners<kStaged>(
+          a.dag_rank, s_base, s_off, pt, &s_next, warp, lane,
+          BitmapProbe{reinterpret_cast<const unsigned *>(table), (unsigned)R}, sg,
+          reinterpret_cast<const unsigned *>(table), R, a.core);
     else if (use_table)
-      th = stream_partners(a.dag_col, s_base, s_off, pt, &s_next, warp, lane,
-                           CuckooProbe{table, shift});
+      th = stream_partners<kStaged>(a.dag_col, s_base, s_off, pt, &s_next, warp, lane,
+                                    CuckooProbe{table, shift}, sg);
     else
-      th = stream_partners(a.dag_col, s_base, s_off, pt, &s_next, warp, lane,
-                           ListProbe{a.dag_col + a0, d});
+      th = stream_partners<false>(a.dag_col, s_base, s_off, pt, &s_next, warp, lane,
+                                  ListProbe{a.dag_col + a0, d}, sg);
     hits += th;
     flush_task(a, x, th, lane);
     if (threadIdx.x == 0) s_task = t_next;  // every thread read s_task two barriers ago
@@ -727,25 +858,33 @@ int tc_count_launch(mc_dgraph *g, cudaEvent_t after_hub, int shard, int num_shar
   a.core = ranked && g->core_used > 0 ? g->core_bits : nullptr;
   a.core_ranks = a.core ? g->core_used : 0;
   a.dense_factor = g->dense_factor;
-  MC_CUDA_TRY(cudaFuncSetAttribute(tc_hub_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)big_smem));
+  // MERCURY_TC_TMA=1: long partner lists staged by bulk copies (the table's
+  // shared memory is followed by 16 KB of copy slots).
+  const char *tma_env = std::getenv("MERCURY_TC_TMA");
+  const bool staged = tma_env && std::atoi(tma_env) != 0;
+  auto kern = staged ? tc_hub_kernel<true> : tc_hub_kernel<false>;
+  const size_t extra = staged ? kStageBytes : 0;
+  MC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(big_smem + extra)));
   a.table_log2_max = small_lg;
   a.tasks = g->hub_tasks;
   a.ntasks = g->hub_off + g->n;
   a.queue = g->counters + 1;
   a.bitmap_bits = (int)std::min<size_t>(small_smem * 8, (size_t)g->bitmap_bits_cap);
+  a.stage_off = (int)(small_smem / sizeof(int));
   const int small_grid =
-      g->num_sms * resident_blocks((const void *)tc_hub_kernel, kCountThreads, small_smem);
-  tc_hub_kernel<<<small_grid, kCountThreads, small_smem, g->stream>>>(a);
+      g->num_sms * resident_blocks((const void *)kern, kCountThreads, small_smem + extra);
+  kern<<<small_grid, kCountThreads, small_smem + extra, g->stream>>>(a);
   MC_CUDA_TRY(cudaGetLastError());
   a.table_log2_max = big_lg;
   a.tasks = g->mega_tasks;
   a.ntasks = g->mega_off + g->n;
   a.queue = g->counters + 6;
   a.bitmap_bits = (int)std::min<size_t>(big_smem * 8, (size_t)g->bitmap_bits_cap);
+  a.stage_off = (int)(big_smem / sizeof(int));
   const int big_grid =
-      g->num_sms * resident_blocks((const void *)tc_hub_kernel, kCountThreads, big_smem);
-  tc_hub_kernel<<<big_grid, kCountThreads, big_smem, g->stream>>>(a);
+      g->num_sms * resident_blocks((const void *)kern, kCountThreads, big_smem + extra);
+  kern<<<big_grid, kCountThreads, big_smem + extra, g->stream>>>(a);
   MC_CUDA_TRY(cudaGetLastError());
   g->launches += 3;
   if (after_hub) MC_CUDA_TRY(cudaEventRecord(after_hub, g->stream));

@@ -212,6 +212,19 @@ class DeviceGraph:
               f"pattern P{k}")
         return out.value
 
+    def pattern_count_budget(self, pattern, budget_ms: float):
+        """(count, 1.0) within budget_ms of device time, or (None, fraction of
+        the tasks done) when the budget ran out (mc_pattern_count_budget)."""
+        k = int(str(pattern).upper().lstrip("P"))
+        out = C.c_uint64()
+        prog = C.c_double(0.0)
+        rc = lib().mc_pattern_count_budget(self._h, k, float(budget_ms), C.byref(out),
+                                           C.byref(prog), C.byref(self.last_timing))
+        if rc == _ffi.MC_ERR_TIMEOUT:
+            return None, prog.value
+        check(rc, f"pattern P{k} (budget)")
+        return out.value, prog.value
+
     def pattern_count_shard(self, pattern, shard: int, num_shards: int) -> int:
         """Partial count of one shard (partials of all shards sum to the count mod 2^64)."""
         k = int(str(pattern).upper().lstrip("P"))

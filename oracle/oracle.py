@@ -45,6 +45,8 @@ def lib() -> C.CDLL:
         L.orc_tc.restype = C.c_uint64
         L.orc_pattern.argtypes = [C.c_int64, P, P, C.c_int, P]
         L.orc_pattern.restype = C.c_uint64
+        L.orc_pattern_fast.argtypes = [C.c_int64, P, P, C.c_int, P]
+        L.orc_pattern_fast.restype = C.c_uint64
         L.orc_csr_build.argtypes = [C.c_int64, C.c_int64, P, P, P, P]
         L.orc_csr_build.restype = C.c_int64
         L.orc_rmat_draws.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
@@ -120,6 +122,21 @@ def pattern(rowptr, col, k: int, return_counters: bool = False):
     c12 = np.zeros(2, dtype=np.uint64)
     r = int(lib().orc_pattern(len(rowptr) - 1, rowptr.ctypes.data, col.ctypes.data, k,
                               c12.ctypes.data))
+    if return_counters:
+        return r, int(c12[0]), int(c12[1])
+    return r
+
+
+def pattern_fast(rowptr, col, k: int, return_counters: bool = False):
+    """P1 or P4 from the second restatement (patterns_fast.cpp: the same sets
+    counted through position marks), for graphs whose hubs make pattern()
+    take hours."""
+    if k not in (1, 4):
+        raise ValueError("pattern_fast restates P1 and P4 only")
+    rowptr, col = _csr(rowptr, col)
+    c12 = np.zeros(2, dtype=np.uint64)
+    r = int(lib().orc_pattern_fast(len(rowptr) - 1, rowptr.ctypes.data, col.ctypes.data, k,
+                                   c12.ctypes.data))
     if return_counters:
         return r, int(c12[0]), int(c12[1])
     return r

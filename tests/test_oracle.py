@@ -99,3 +99,26 @@ def test_chung_lu_restatement_equals_library_generator(n, mean, cap, seed):
     rp, col = orc.chung_lu(n, 2.1, mean, cap, seed=seed)
     g = Graph.chung_lu(n, 2.1, mean, cap, seed=seed)
     assert np.array_equal(rp, g.rowptr) and np.array_equal(col, g.col)
+
+
+@pytest.mark.parametrize("seed", range(5))
+def test_fast_p1_p4_restatement_equals_literal_oracle(seed):
+    """patterns_fast.cpp counts P1 and P4 through position marks; its counters
+    c1 and c2 equal the literal restatement's on random graphs, the golden
+    fixtures and a Chung-Lu graph with hubs."""
+    n = 30 + 25 * seed
+    rp, col = csr_from_edges(n, random_graph(n, 0.15 + 0.07 * seed, 100 + seed))
+    for k in (1, 4):
+        assert orc.pattern_fast(rp, col, k, True) == orc.pattern(rp, col, k, True), k
+
+
+def test_fast_p1_p4_restatement_on_fixtures_and_hubs():
+    for name in ("cl3000", "rmat10", "petersen", "isolated", "dense400"):
+        prefix = os.path.join(GOLDEN, "graphs", name, "graph")
+        rp = np.fromfile(prefix + ".vertex.bin", dtype=np.int64)
+        col = np.fromfile(prefix + ".edge.bin", dtype=np.int32)
+        for k in (1, 4):
+            assert orc.pattern_fast(rp, col, k, True) == orc.pattern(rp, col, k, True), (name, k)
+    rp, col = orc.chung_lu(20000, 2.1, 12.0, 2000.0, seed=4)
+    for k in (1, 4):
+        assert orc.pattern_fast(rp, col, k, True) == orc.pattern(rp, col, k, True), k

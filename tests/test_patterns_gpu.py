@@ -2,6 +2,7 @@
 and the oracle (bit-exact uint64), through the C ABI."""
 import json
 import os
+import sys
 
 import numpy as np
 import pytest
@@ -192,3 +193,90 @@ def test_pattern_shards_sum_to_the_count(monkeypatch, route, shards):
             assert sum(parts) % (1 << 64) == full, k
         with pytest.raises(Exception):
             d.pattern_count_shard(1, shards, shards)
+
+
+@pytest.mark.parametrize("route", ["edge", "centers"])
+def test_sliced_launches_equal_one_launch(monkeypatch, route):
+    """Counting in slices of the task range (each slice a launch with its own
+    queue) gives the same counts as one launch per kernel, on both routes."""
+    g = Graph.chung_lu(30000, 2.1, 12.0, 2000.0, seed=9)
+    monkeypatch.setenv("MERCURY_PATTERN_KERNEL", route)
+    with DeviceGraph(g) as d:
+        monkeypatch.setenv("MERCURY_PATTERN_SLICE", "0")
+        whole = [d.pattern_count(k) for k in range(1, 9)]
+        monkeypatch.setenv("MERCURY_PATTERN_SLICE", "1")
+        monkeypatch.setenv("MERCURY_PATTERN_SLICE_MS", "0.2")  # many small slices
+        sliced = [d.pattern_count(k) for k in range(1, 9)]
+        assert d.last_timing.launches > 8
+    assert sliced == whole
+
+
+def test_budget_stops_between_slices_and_counts_within_it():
+    g = Graph.chung_lu(30000, 2.1, 12.0, 2000.0, seed=9)
+    with DeviceGraph(g) as d:
+        want = d.pattern_count(5)
+        got, frac = d.pattern_count_budget(5, 60000.0)
+        assert got == want and frac == 1.0
+        # A budget below one slice: the first slice runs (one task per
+        # resident warp), then the count stops with the rest undone.
+        got, frac = d.pattern_count_budget(5, 1e-6)
+        assert got is None and 0.0 < frac < 1.0
+        assert d.pattern_count(5) == want  # the handle stays usable
+
+
+def test_pattern_bench_graph_counts_equal_committed_oracle():
+    """The graph bench.py --mode patterns counts (Chung-Lu n 100,000, mean 10,
+    cap 200, seed 1): all eight counts equal the oracle's, committed by
+    tests/golden/make_pattern_golden.py."""
+    with open(os.path.join(GOLDEN, "pattern_counts.json")) as f:
+        rec = json.load(f)["chung_lu_n100000_mean10_cap200_seed1"]
+    g = Graph.chung_lu(100000, 2.1, 10.0, 200.0, seed=1)
+    assert g.nnz // 2 == rec["m"]
+    with DeviceGraph(g) as d:
+        for k in range(1, 9):
+            assert d.pattern_count(k) == rec["counts"][f"P{k}"], k
+
+
+@pytest.mark.parametrize("words", [None, "2048"])
+@pytest.mark.parametrize("make", [lambda: Graph.chung_lu(30000, 2.1, 12.0, 900.0, seed=7),
+                                  lambda: Graph.rmat(12, 16, seed=5)])
+def test_center_route_two_hop_rows_equal_per_edge_rows(monkeypatch, make, words):
+    """The center route's outer rows R(y) = N(y) & N0 come from the center's
+    two-hop rows (built once per center) or are built per edge
+    (MERCURY_HOP_ROWS=0); with a small scratch share (words = 2048) the
+    larger centers fall back to per-edge rows within the same launch.  Every
+    outer pattern gives the same counts either way, and the oracle's."""
+    g = make()
+    monkeypatch.setenv("MERCURY_PATTERN_KERNEL", "centers")
+    if words:
+        monkeypatch.setenv("MERCURY_HOP_WORDS", words)
+    outer = (2, 4, 5, 6, 8)
+    with DeviceGraph(g) as d:
+        hop = [d.pattern_count(k) for k in outer]
+        monkeypatch.setenv("MERCURY_HOP_ROWS", "0")
+        per_edge = [d.pattern_count(k) for k in outer]
+    assert hop == per_edge
+    if g.n <= 5000:
+        assert hop == [orc.pattern(g.rowptr, g.col, k) for k in outer]
+
+
+@pytest.mark.parametrize("hub", ["1", "0"])
+def test_p1_large_centers_by_bitmap_tasks(monkeypatch, hub):
+    """P1 on centers above degree 1,024: one CTA per (center, 256 edges)
+    with the center's neighbourhood as an id bitmap (MERCURY_HUB_P1=1, the
+    default) or the warp-per-edge kernel (=0); both give the oracle's counts,
+    whole and in shards, on a graph with a vertex of degree 20,000 and on a
+    Chung-Lu graph with hubs up to ~5,000."""
+    sys.path.insert(0, GOLDEN)
+    from make_hub_golden import hub_graph
+    with open(os.path.join(GOLDEN, "hub_counts.json")) as f:
+        hub_want = json.load(f)["counts"]["P1"]
+    monkeypatch.setenv("MERCURY_HUB_P1", hub)
+    rp, col = hub_graph()
+    with DeviceGraph(rp, col) as d:
+        assert d.pattern_count(1) == hub_want
+    g = Graph.chung_lu(60000, 2.1, 16.0, 5000.0, seed=23)
+    want = orc.pattern_fast(g.rowptr, g.col, 1)
+    with DeviceGraph(g) as d:
+        assert d.pattern_count(1) == want
+        assert sum(d.pattern_count_shard(1, s, 3) for s in range(3)) % (1 << 64) == want

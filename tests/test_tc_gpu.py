@@ -202,6 +202,25 @@ def test_dense_partners_with_mixed_owner_kinds(monkeypatch, bits):
         assert d.tc_count() == want
 
 
+@pytest.mark.parametrize("cap", ["0", "1000000"])
+@pytest.mark.parametrize("make", [lambda: Graph.rmat(16, 16, seed=41),
+                                  lambda: Graph.chung_lu(80000, 2.1, 24.0, 8000.0, seed=42),
+                                  lambda: fixture("dense400")])
+def test_hub_lists_staged_by_bulk_copies(monkeypatch, make, cap):
+    """MERCURY_TC_TMA=1: long partner lists reach shared memory by
+    cp.async.bulk chunks (double-buffered per warp) instead of lane loads;
+    bitmap owners (cap 1000000) and table owners (cap 0) both give the
+    oracle's count, whole and in shards."""
+    g = make()
+    want = orc.tc(g.rowptr, g.col)
+    monkeypatch.setenv("MERCURY_TC_TMA", "1")
+    monkeypatch.setenv("MERCURY_TC_BITMAP_BITS", cap)
+    with DeviceGraph(g) as d:
+        assert d.tc_count() == want
+        assert d.tc_count() == want
+        assert sum(d.tc_count_shard(s, 3) for s in range(3)) == want
+
+
 def test_empty_and_edgeless_graphs():
     with DeviceGraph(np.zeros(1, dtype=np.int64), np.zeros(0, dtype=np.int32)) as d:
         assert d.tc_count() == 0
