@@ -64,6 +64,8 @@ def parse_args():
     p.add_argument("--pat-cap", type=float, default=200.0)
     p.add_argument("--pat-budget-ms", type=float, default=0.0,
                    help="patterns mode: device-time budget per pattern (0: none)")
+    p.add_argument("--pat-list", default="1,2,3,4,5,6,7,8",
+                   help="patterns mode: which patterns to count")
     p.add_argument("--serve-rates", default="100,1000,5000,20000")
     p.add_argument("--serve-seconds", type=float, default=2.0)
     p.add_argument("--serve-pool", type=int, default=512)
@@ -663,13 +665,20 @@ def run_serve(a, local_rank):
             got = [0] * n_req
             end_times = [0.0] * n_req
 
+            errors = []
+
             def collect():
-                for i in range(n_req):
-                    while tickets[i] is None:
-                        time.sleep(0)
-                    got[i], lat[i] = s.wait(tickets[i], 600000)
-                    end_times[i] = time.perf_counter()
-                done.set()
+                try:
+                    for i in range(n_req):
+                        while tickets[i] is None:
+                            time.sleep(0)
+                        try:
+                            got[i], lat[i] = s.wait(tickets[i], 600000)
+                        except Exception as e:  # recorded; the run is then refused below
+                            errors.append(f"request {i}: {e}")
+                        end_times[i] = time.perf_counter()
+                finally:
+                    done.set()
             th = threading.Thread(target=collect)
             th.start()
             t_start = time.perf_counter()
@@ -683,6 +692,7 @@ def run_serve(a, local_rank):
             done.wait()
             th.join()
             st = s.stats()
+        assert not errors, f"{len(errors)} served requests failed, first: {errors[0]}"
         assert got == [want[int(k)] for k in picks], "served counts differ from the plain path"
         span = max(end_times) - t_start
         runs.append({"rate_req_per_s": rate, "run": rep, "requests": n_req,
@@ -768,7 +778,7 @@ def run_patterns(a, rank, world, local_rank):
                 return d.pattern_count(k), d.last_timing.count_ms
             part = d.pattern_count_shard(k, *shard_of(rank, world))
             return combine_ranks(part, d.last_timing.count_ms, "cuda")
-        for k in range(1, 9):
+        for k in [int(x) for x in a.pat_list.split(",") if x]:
             if a.pat_budget_ms > 0 and world == 1:
                 first, frac = d.pattern_count_budget(k, a.pat_budget_ms)
                 if first is None:

@@ -94,6 +94,14 @@ const char *mc_version(void);
 int mc_graph_load(const char *prefix, mc_graph_t **out);
 /* Writes the same three files (the layout the reference reader expects). */
 int mc_graph_write(const mc_graph_t *g, const char *prefix);
+/* Reads <prefix>.vlabel.bin, one uint8 label per vertex, into the graph:
+ * the vertex-label part of the reference loader (graph.cc:37-58, with
+ * use_vlabel).  MC_ERR_IO when the file is missing (the reference then draws
+ * random labels; here the caller decides), MC_ERR_FORMAT when its size is
+ * not n bytes. */
+int mc_graph_load_vlabels(mc_graph_t *g, const char *prefix);
+/* The graph's labels (n bytes, owned by the graph), or NULL if none. */
+int mc_graph_vlabels(const mc_graph_t *g, const uint8_t **labels);
 /* Wraps caller arrays into a host graph (copied; the caller keeps its own). */
 int mc_graph_from_csr(const int64_t *rowptr, const int32_t *col, int64_t n,
                       int64_t nnz, mc_graph_t **out);
@@ -329,6 +337,31 @@ int mc_batch_autotune(mc_batch_t *b, int32_t *choice);
 /* counts[g] for every graph, from one replay of the captured launch. */
 int mc_batch_count(mc_batch_t *b, uint64_t *counts, mc_timing_t *timing);
 void mc_batch_free(mc_batch_t *b);
+
+/* ---- vertex labels ----------------------------------------------------------
+ * Labels live on the device beside the CSR, one uint8 per vertex, each at most
+ * max_label (the reference's num_vertex_classes; vlabel_t is uint8,
+ * include/common.h:33).  mc_dgraph_set_vlabels copies them (MC_ERR_FORMAT if
+ * a label exceeds max_label).  The queries restate the reference's label
+ * helpers on the device:
+ *   mc_label_frequency: freq[l] = vertices of label l, l = 0..max_label
+ *     (Graph::computeLabelsFrequency, graph.cc:440-460);
+ *   mc_label_reverse_index: offsets[max_label + 2] and vertices[n], the
+ *     vertices grouped by label in id order (Graph::BuildReverseIndex,
+ *     graph.cc:413-436, getVerticesByLabel);
+ *   mc_label_nlf: for v in [v_begin, v_end), row v - v_begin of
+ *     (max_label + 1) counts of N(v)'s labels (Graph::BuildNLF,
+ *     graph.cc:483-495, as a dense table instead of one map per vertex);
+ *   mc_tc_count_by_label: counts[l] = the sum over DAG edges v -> u of
+ *     |{w in N+(v) & N+(u) : label(w) = l}|, the reference's labelled
+ *     intersection Graph::intersect_num(v, u, label) (graph.cc:396-411) over
+ *     the degree-ordered DAG: triangles split by the label of their DAG sink
+ *     (the vertex of largest (degree, id)), summing to the triangle count. */
+int mc_dgraph_set_vlabels(mc_dgraph_t *g, const uint8_t *labels, int max_label);
+int mc_label_frequency(mc_dgraph_t *g, uint64_t *freq);
+int mc_label_reverse_index(mc_dgraph_t *g, int64_t *offsets, int32_t *vertices);
+int mc_label_nlf(mc_dgraph_t *g, int64_t v_begin, int64_t v_end, uint32_t *nlf);
+int mc_tc_count_by_label(mc_dgraph_t *g, uint64_t *counts, mc_timing_t *timing);
 
 /* ---- serving ---------------------------------------------------------------
  * A request loop with continuous batching (no reference counterpart).

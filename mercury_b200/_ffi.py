@@ -91,6 +91,8 @@ SIGNATURES = {
     "mc_graph_rowptr": (_P, [_P]),
     "mc_graph_col": (_P, [_P]),
     "mc_graph_validate": (C.c_int, [_P, C.c_int]),
+    "mc_graph_load_vlabels": (C.c_int, [_P, C.c_char_p]),
+    "mc_graph_vlabels": (C.c_int, [_P, _PP]),
     "mc_graph_free": (None, [_P]),
     "mc_gen_rmat": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_uint64, _PP]),
     "mc_gen_chung_lu": (C.c_int, [_I64, C.c_double, C.c_double, C.c_double, C.c_uint64, _PP]),
@@ -125,6 +127,11 @@ SIGNATURES = {
     "mc_batch_autotune": (C.c_int, [_P, _P]),
     "mc_batch_count": (C.c_int, [_P, _PU64, C.POINTER(Timing)]),
     "mc_batch_free": (None, [_P]),
+    "mc_dgraph_set_vlabels": (C.c_int, [_P, _P, C.c_int]),
+    "mc_label_frequency": (C.c_int, [_P, _PU64]),
+    "mc_label_reverse_index": (C.c_int, [_P, _P, _P]),
+    "mc_label_nlf": (C.c_int, [_P, _I64, _I64, _P]),
+    "mc_tc_count_by_label": (C.c_int, [_P, _PU64, C.POINTER(Timing)]),
     "mc_server_create": (C.c_int, [_I64, C.c_int, C.c_int, _PP]),
     "mc_server_submit": (C.c_int, [_P, _P, _P, _I64, _I64, C.c_int, C.c_uint64, _PU64]),
     "mc_server_wait": (C.c_int, [_P, C.c_uint64, C.c_int, _PU64, C.POINTER(C.c_double)]),

@@ -38,6 +38,8 @@ constexpr unsigned kErrContract = kErrIdRange | kErrUnsorted | kErrSelfLoop | kE
   } while (0)
 
 void set_last_cuda_error(cudaError_t e);
+// The calling thread's last CUDA error seen by MC_CUDA_TRY.
+cudaError_t last_cuda_error();
 
 // A named NVTX range for the lifetime of the object: the library's phases
 // (upload, orientation, counting, builds, batches) show up by name in a

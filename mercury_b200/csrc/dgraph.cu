@@ -32,7 +32,7 @@ void release(mc_dgraph *g) {
                   g->mega_cnt,   g->mega_off,   g->mega_tasks, g->rank,
                   g->dag_rank,   g->rank_keys,  g->rank_counts, g->rank_offsets,
                   g->center_scratch, g->stage, g->chunk_offsets, g->core_bits, g->pinfo,
-                  g->hop_scratch, g->hub_bits};
+                  g->hop_scratch, g->hub_bits, g->vlabels};
   if (g->col_host) bufs[1] = nullptr;  // pinned host memory, freed below
   // Stream-ordered frees: no device-wide synchronisation, so other handles'
   // work keeps running while this one is released.
@@ -165,6 +165,7 @@ thread_local HostCache t_cache;
 }  // namespace
 
 void set_last_cuda_error(cudaError_t e) { t_last_cuda = e; }
+cudaError_t last_cuda_error() { return t_last_cuda; }
 
 void retain_pool_memory(int device) {
   static std::atomic<unsigned long long> done{0};  // one bit per device (first 64)

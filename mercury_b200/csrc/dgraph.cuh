@@ -75,6 +75,10 @@ struct mc_dgraph {
   void *hub_bits = nullptr;        // per-CTA id bitmaps of the large P1 centers
   size_t hub_bits_bytes = 0;
 
+  // ---- vertex labels (mc_dgraph_set_vlabels), one uint8 per vertex -------
+  uint8_t *vlabels = nullptr;
+  int max_label = -1;
+
   // ---- triangle-count scratch, allocated on the first mc_tc_count -------
   bool tc_ready = false;
   int2 *key = nullptr;            // n      {symmetric degree, DAG out-degree}

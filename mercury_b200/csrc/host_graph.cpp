@@ -244,6 +244,32 @@ int mc_graph_write(const mc_graph_t *g, const char *prefix) {
   return rc;
 }
 
+int mc_graph_load_vlabels(mc_graph_t *g, const char *prefix) {
+  if (!g || !prefix) return MC_ERR_ARG;
+  const std::string path = std::string(prefix) + ".vlabel.bin";
+  FILE *f = std::fopen(path.c_str(), "rb");
+  if (!f) return MC_ERR_IO;
+  std::fseek(f, 0, SEEK_END);
+  const long size = std::ftell(f);
+  std::fclose(f);
+  if (size != (long)g->n) return MC_ERR_FORMAT;  // one uint8 per vertex
+  std::vector<uint8_t> labels;
+  try {
+    const int rc = read_exact(path, labels, (size_t)g->n);
+    if (rc != MC_OK) return rc;
+  } catch (const std::bad_alloc &) {
+    return MC_ERR_OOM;
+  }
+  g->vlabels.swap(labels);
+  return MC_OK;
+}
+
+int mc_graph_vlabels(const mc_graph_t *g, const uint8_t **labels) {
+  if (!g || !labels) return MC_ERR_ARG;
+  *labels = g->vlabels.empty() ? nullptr : g->vlabels.data();
+  return MC_OK;
+}
+
 int mc_graph_from_csr(const int64_t *rowptr, const int32_t *col, int64_t n,
                       int64_t nnz, mc_graph_t **out) {
   if (!out || n < 0 || nnz < 0 || !rowptr || (nnz > 0 && !col)) return MC_ERR_ARG;

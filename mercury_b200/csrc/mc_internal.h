@@ -10,6 +10,7 @@ struct mc_graph {
   int64_t max_degree = 0;
   std::vector<int64_t> rowptr;  // n + 1
   std::vector<int32_t> col;     // nnz
+  std::vector<uint8_t> vlabels; // n, or empty (mc_graph_load_vlabels)
 };
 
 namespace mc {

@@ -498,6 +498,73 @@ __device__ void edge_pattern(const Warp &w, int v0, int v1, int32_t *L, int64_t 
   } else if (P == 6) {  // P6_subgraph_matching (:736-853)
     const int nA = w.inter(n0, d0, v1, -1, L0);
     const int nB = w.diff(n1, d1, v0, -1, L1);
+    if (nA == 0) {
+      __syncwarp();
+      return;
+    }
+    if (w.H && w.M && nA <= kWarp && nA + nB <= kSetMax) {
+      // Bit-mask form.  Lane j walks N(A[j]) once against B (tag 0) and A
+      // (tag 1) in the shared-memory set, recording the B positions it holds
+      // (row j of mask, ceil(nB / 32) words in the warp's scratch) and the A
+      // positions (M[j]).  For v2 = A[j] the reference's D = A - N(v2) is
+      // ~M[j] and E = B - N(v2) is ~mask[j]; its count for v3 in D,
+      // #{key in E : key not in N(v3)}, is popc(~mask[j] & ~mask[v3]) over
+      // B's positions (the graph is symmetric).
+      const int wb = (nB + kWarp - 1) / kWarp;
+      unsigned *mask = reinterpret_cast<unsigned *>(L2);
+      const WarpSet s0{w.H};
+      s0.clear(w.lane);
+      s0.insert(L1, nB, 0, w.lane);
+      s0.insert(L0, nA, 1, w.lane);
+      unsigned mrow = 0;
+      if (w.lane < nA) {
+        const int j = w.lane;
+        unsigned *mj = mask + j * wb;
+        for (int k = 0; k < wb; ++k) mj[k] = 0u;
+        const int x = L0[j];
+        const int32_t *p = w.N(x);
+        const int dx = w.deg(x);
+        if (dx <= (nB + nA) * ceil_log2_int(dx)) {
+          for (int k = 0; k < dx; ++k) {
+            const int y = __ldg(p + k);
+            const int r = s0.lookup(y);
+            if (r == 1) {
+              const int q = pos_of(L1, nB, y);
+              mj[q >> 5] |= 1u << (q & 31);
+            } else if (r == 2) {
+              mrow |= 1u << pos_of(L0, nA, y);
+            }
+          }
+        } else {
+          for (int k = 0; k < nB; ++k)
+            if (bsearch(p, dx, L1[k])) mj[k >> 5] |= 1u << (k & 31);
+          for (int k = 0; k < nA; ++k)
+            if (k != j && bsearch(p, dx, L0[k])) mrow |= 1u << k;
+        }
+      }
+      w.M[w.lane] = mrow;
+      __syncwarp();
+      if (w.lane < nA) {
+        const int j = w.lane;
+        const unsigned *mj = mask + j * wb;
+        const unsigned valid_a = nA == kWarp ? kFull : ((1u << nA) - 1u);
+        unsigned dset = ~mrow & valid_a;  // D = A - N(v2), v2 itself included
+        unsigned long long c = 0;
+        while (dset) {
+          const int t = __ffs(dset) - 1;
+          dset &= dset - 1u;
+          const unsigned *mt = mask + t * wb;
+          for (int k = 0; k < wb; ++k) {
+            const int left = nB - 32 * k;
+            const unsigned valid = left >= 32 ? kFull : ((1u << left) - 1u);
+            c += (unsigned long long)__popc(valid & ~(mj[k] | mt[k]));
+          }
+        }
+        acc.c1 += c;
+      }
+      __syncwarp();
+      return;
+    }
     for (int i = 0; i < nA; ++i) {
       if ((i & 15) == 15 && w.out_of_time()) return;
       const int v2 = L0[i];
@@ -790,6 +857,8 @@ struct CenterArgs {
   // null: rows are built per edge.
   unsigned *hop = nullptr;
   int64_t hop_words = 0;
+  int64_t hop_walk = 0;  // host side: the class's largest two-hop walk (0: no rows)
+  unsigned long long *hop_misses = nullptr;  // centers whose rows did not fit
   // Budgeted count: stop at *deadline (globaltimer ns), raising *stop_flag.
   const unsigned long long *deadline = nullptr;
   unsigned long long *stop_flag = nullptr;
@@ -1341,9 +1410,13 @@ __global__ void __launch_bounds__(kPatThreads) center_kernel(CenterArgs a) {
     if constexpr (center_outer(P)) {
       const HopRows *hop = nullptr;
       HopRows hr{};
-      if (a.hop && build_hop_rows<W, G>(a, idx, v0, grp, gl, wg, lane, s_hop_walk + grp,
-                                        s_hop_keys + grp, s_hop_rows + grp, &hr))
-        hop = &hr;
+      if (a.hop) {
+        if (build_hop_rows<W, G>(a, idx, v0, grp, gl, wg, lane, s_hop_walk + grp,
+                                 s_hop_keys + grp, s_hop_rows + grp, &hr))
+          hop = &hr;
+        else if (gl == 0)
+          atomicAdd(a.hop_misses, 1ull);
+      }
       center_outer_edges<P, W>(a.rp, a.ci, M, idx, v0, wg, G, lane, Rw, cnt, slots, hop,
                                a.deadline, a.stop_flag, acc);
     } else
@@ -1482,26 +1555,42 @@ __global__ void __launch_bounds__(kPatThreads) hub_p1_kernel(HubP1Args a) {
         if (__any_sync(kFull, y >= v1)) break;
       }
       __syncwarp();
-      unsigned long long c2 = 0;
-      for (int tb = lane; tb < nb; tb += kWarp) {
+      // Per v2 in B the whole warp counts #{k : v2 < k < v1, k in N0 & N(v2),
+      // k notin N1} over the shorter of N(v2) and N0 within (v2, v1).
+      long long c2 = 0;
+      for (int tb = 0; tb < nb; ++tb) {
         const int v2 = B[tb];
-        long long term = (long long)(p - lower_pos(n0, d0, v2) - 1) - (nb - 1 - tb);
+        const int q2 = lower_pos(n0, d0, v2);  // v2's position in N0
         const int64_t b2 = __ldg(a.rp + v2), e2 = __ldg(a.rp + v2 + 1);
-        // N(v2) from its first entry above v2, up to v1.
-        int64_t lo = b2, hi = e2;
+        int64_t lo = b2, hi = e2;  // first entry of N(v2) above v2
         while (lo < hi) {
           const int64_t mid = (lo + hi) >> 1;
           if (__ldg(a.ci + mid) <= v2) lo = mid + 1;
           else hi = mid;
         }
-        for (int64_t k = lo; k < e2; ++k) {
-          const int y = __ldg(a.ci + k);
-          if (y >= v1) break;
-          if (bit_set(bits, y) && !bsearch(n1, d1, y)) --term;
+        int64_t top = lo, hi2 = e2;  // first entry of N(v2) at or above v1
+        while (top < hi2) {
+          const int64_t mid = (top + hi2) >> 1;
+          if (__ldg(a.ci + mid) < v1) top = mid + 1;
+          else hi2 = mid;
         }
-        c2 += (unsigned long long)term;
+        const int d2 = (int)(e2 - b2);
+        int drop = 0;
+        if (top - lo <= p - q2 - 1) {
+          for (int64_t k = lo + lane; k < top; k += kWarp) {
+            const int y = __ldg(a.ci + k);
+            drop += bit_set(bits, y) && !bsearch(n1, d1, y);
+          }
+        } else {
+          for (int j = q2 + 1 + lane; j < p; j += kWarp) {
+            const int y = __ldg(n0 + j);
+            drop += bsearch(a.ci + b2, d2, y) && !bsearch(n1, d1, y);
+          }
+        }
+        drop = warp_sum_int(drop);
+        c2 += (long long)(p - q2 - 1) - (nb - 1 - tb) - drop;
       }
-      acc.c2 += c2;
+      if (lane == 0) acc.c2 += (unsigned long long)c2;
       __syncwarp();  // B is rewritten by the warp's next edge
     }
     __syncthreads();
@@ -1614,6 +1703,34 @@ int run_slices(mc_dgraph *g, Slicer &sl, const char *what, int64_t total, int64_
   return MC_OK;
 }
 
+// Largest two-hop walk (sum over x in N(v) of d(x)) among the centers of each
+// class: sizes the two-hop row maps (walk[c], c = class).
+__global__ void hop_need_kernel(const int64_t *__restrict__ rp, const int32_t *__restrict__ ci,
+                                int64_t n, int shard, int num_shards,
+                                unsigned long long *__restrict__ walk) {
+  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n) return;
+  const int64_t b = rp[v], e = rp[v + 1];
+  const int d = (int)(e - b);
+  if (d < 1 || d > kCenterMaxDeg || v % num_shards != shard) return;
+  int cls = 0;
+  while (32 * center_words(cls) < d) ++cls;
+  unsigned long long sum = 0;
+  for (int64_t k = b; k < e; ++k) {
+    const int x = __ldg(ci + k);
+    sum += (unsigned long long)(__ldg(rp + x + 1) - __ldg(rp + x));
+  }
+  atomicMax(walk + cls, sum);
+}
+
+// Words of two-hop scratch one group needs for a center whose walk is B
+// (the map of build_hop_rows plus at most B rows of W words).
+__host__ __device__ inline int64_t hop_group_words(int64_t B, int W) {
+  int lg = 6;
+  while ((int64_t(1) << lg) < 2 * B) ++lg;
+  return 2 * (int64_t(1) << lg) + B * W;
+}
+
 template <int P, int W>
 int launch_center(mc_dgraph *g, const CenterArgs &a, int num_sms, int64_t total, Slicer *sl) {
   constexpr int G = center_group(W);
@@ -1626,15 +1743,31 @@ int launch_center(mc_dgraph *g, const CenterArgs &a, int num_sms, int64_t total,
     per_sm = 1;
   const int grid = num_sms * per_sm;
   CenterArgs ha = a;
-  if (center_outer(P) && a.hop) {
-    // The scratch split evenly over the resident groups, at most 2^21 words each.
+  if (center_outer(P) && a.hop_walk > 0) {
+    // Each resident group gets the words its largest center needs, within
+    // 4 GiB (or a quarter of the free memory) in all; centers that do not
+    // fit build their rows per edge.
     const int64_t groups = (int64_t)grid * (kPatThreads / kWarp / G);
-    ha.hop_words = std::min<int64_t>(int64_t(1) << 21,
-                                     (int64_t)(g->hop_scratch_bytes / sizeof(unsigned)) / groups);
+    const int64_t need = hop_group_words(a.hop_walk, W);
+    size_t free_b = 0, total_b = 0;
+    MC_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    const int64_t cap_words =
+        (int64_t)(std::min<size_t>(size_t(4) << 30, free_b / 4) / sizeof(unsigned));
+    int64_t per_group = std::min<int64_t>(need, cap_words / groups);
     // MERCURY_HOP_WORDS lowers the share (tests use it to send the larger
     // centers to the per-edge rows).
     if (const char *env = std::getenv("MERCURY_HOP_WORDS"))
-      ha.hop_words = std::min<int64_t>(ha.hop_words, std::atoll(env));
+      per_group = std::min<int64_t>(per_group, std::atoll(env));
+    const size_t bytes = (size_t)(per_group * groups) * sizeof(unsigned);
+    if (per_group > 0 && bytes > g->hop_scratch_bytes) {
+      if (g->hop_scratch) dev_free(g->hop_scratch, g->stream);
+      g->hop_scratch = nullptr;
+      g->hop_scratch_bytes = 0;
+      MC_CUDA_TRY(dev_alloc(&g->hop_scratch, bytes, g->stream));
+      g->hop_scratch_bytes = bytes;
+    }
+    ha.hop = per_group > 0 ? static_cast<unsigned *>(g->hop_scratch) : nullptr;
+    ha.hop_words = per_group;
   } else {
     ha.hop = nullptr;
   }
@@ -1688,7 +1821,12 @@ int grid_blocks(mc_dgraph *g, int64_t cap) {
     per_sm = 4;
   const int64_t resident = (int64_t)g->num_sms * std::max(per_sm, 1);
   const int64_t block_bytes = (int64_t)(kPatThreads / kWarp) * kLists * cap * 4;
-  const int64_t fit = std::max<int64_t>(1, (int64_t)kScratchBudget / block_bytes);
+  // The frontier scratch a handle keeps grows with its graph (256 bytes per
+  // CSR entry, 8 MiB at least, kScratchBudget at most), so that thousands of
+  // small resident graphs do not each hold the full budget.
+  const int64_t budget = std::min<int64_t>(
+      (int64_t)kScratchBudget, std::max<int64_t>(int64_t(8) << 20, 256 * std::max<int64_t>(g->nnz, 1)));
+  const int64_t fit = std::max<int64_t>(1, budget / block_bytes);
   return (int)std::min(resident, fit);
 }
 
@@ -1824,38 +1962,36 @@ int center_path(mc_dgraph *g, int pattern, PatArgs a, int grid, Slicer *sl) {
   int64_t *big_off = reinterpret_cast<int64_t *>(reinterpret_cast<char *>(big_deg) + up(deg_b));
   void *temp = reinterpret_cast<char *>(big_off) + up(off_b);
 
-  // Two-hop rows of the outer patterns: 1 GiB of scratch (or an eighth of the
+  // Two-hop rows of the outer patterns: 4 GiB of scratch (or a quarter of the
   // free memory, if less) shared out among the resident groups of each class
   // launch.  MERCURY_HOP_ROWS=0: rows per edge only.
   const char *hop_env = std::getenv("MERCURY_HOP_ROWS");
   const bool hop_on = center_outer(pattern) && !(hop_env && std::atoi(hop_env) == 0);
-  if (hop_on) {
-    size_t free_b = 0, total_b = 0;
-    MC_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
-    const size_t want = std::min<size_t>(size_t(1) << 30, free_b / 8) & ~size_t(255);
-    if (want > g->hop_scratch_bytes) {
-      if (g->hop_scratch) dev_free(g->hop_scratch, s);
-      g->hop_scratch = nullptr;
-      g->hop_scratch_bytes = 0;
-      MC_CUDA_TRY(dev_alloc(&g->hop_scratch, want, s));
-      g->hop_scratch_bytes = want;
-    }
-  }
+  unsigned long long *hop_walk = reinterpret_cast<unsigned long long *>(words + 128);  // 6 words
   MC_CUDA_TRY(cudaMemsetAsync(words, 0, words_b, s));
+  if (hop_on) {
+    hop_need_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g->rowptr, g->col, n, a.shard,
+                                                                a.num_shards, hop_walk);
+    MC_CUDA_TRY(cudaGetLastError());
+    g->launches += 1;
+  }
   center_classes_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
       g->rowptr, n, a.shard, a.num_shards, lists, counts, big_deg);
   MC_CUDA_TRY(cudaGetLastError());
   MC_CUDA_TRY(exclusive_scan(big_deg, big_off, n, temp, s));
   g->launches += 1 + scan_launches(n);
   int32_t h_counts[kCenterClasses];
+  unsigned long long h_walk[kCenterClasses];
   int64_t big_total = 0;
   MC_CUDA_TRY(cudaMemcpyAsync(h_counts, counts, sizeof(h_counts), cudaMemcpyDeviceToHost, s));
+  MC_CUDA_TRY(cudaMemcpyAsync(h_walk, hop_walk, sizeof(h_walk), cudaMemcpyDeviceToHost, s));
   MC_CUDA_TRY(cudaMemcpyAsync(&big_total, big_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   MC_CUDA_TRY(cudaStreamSynchronize(s));
   for (int c = 0; c < kCenterClasses; ++c) {
     if (h_counts[c] == 0) continue;
     CenterArgs ca{g->rowptr, g->col, lists + (int64_t)c * n, counts + c, queues + c, g->counters};
-    ca.hop = hop_on ? static_cast<unsigned *>(g->hop_scratch) : nullptr;
+    ca.hop_walk = hop_on ? (int64_t)h_walk[c] : 0;
+    ca.hop_misses = g->counters + 7;
     ca.deadline = a.deadline;
     ca.stop_flag = a.stop_flag;
     int rc = MC_OK;
@@ -1886,9 +2022,17 @@ int center_path(mc_dgraph *g, int pattern, PatArgs a, int grid, Slicer *sl) {
     MC_CUDA_TRY(cudaMemcpyAsync(&total_chunks, chunk_off + n, sizeof(int64_t),
                                 cudaMemcpyDeviceToHost, s));
     MC_CUDA_TRY(cudaStreamSynchronize(s));
+    // Grid: every resident CTA, as far as the frontier scratch allows (each
+    // warp of this kernel needs cap ints of it, the edge kernel kLists x cap).
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hub_p1_kernel, kPatThreads, 0) !=
+            cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+    const int hub_grid = (int)std::min<int64_t>((int64_t)g->num_sms * per_sm, (int64_t)grid * kLists);
     // One id bitmap per CTA, zero between tasks (cleared here as well, in
     // case an earlier count stopped at its deadline mid-task).
-    const size_t bits_b = sizeof(unsigned) * (size_t)((n + 31) / 32) * (size_t)grid;
+    const size_t bits_b = sizeof(unsigned) * (size_t)((n + 31) / 32) * (size_t)hub_grid;
     if (bits_b > g->hub_bits_bytes) {
       if (g->hub_bits) dev_free(g->hub_bits, s);
       g->hub_bits = nullptr;
@@ -1903,11 +2047,11 @@ int center_path(mc_dgraph *g, int pattern, PatArgs a, int grid, Slicer *sl) {
     const int64_t ntasks = total_chunks > a.shard
                                ? (total_chunks - a.shard + a.num_shards - 1) / a.num_shards
                                : 0;
-    return run_slices(g, *sl, "hub P1", ntasks, grid, ha.queue, [&](int64_t b, int64_t e) {
+    return run_slices(g, *sl, "hub P1", ntasks, hub_grid, ha.queue, [&](int64_t b, int64_t e) {
       HubP1Args sa = ha;
       sa.task_begin = b;
       sa.task_end = e;
-      hub_p1_kernel<<<grid, kPatThreads, 0, s>>>(sa);
+      hub_p1_kernel<<<hub_grid, kPatThreads, 0, s>>>(sa);
       MC_CUDA_TRY(cudaGetLastError());
       g->launches += 1;
       return MC_OK;
@@ -2027,6 +2171,9 @@ int pattern_count(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12, mc_ti
   MC_CUDA_TRY(cudaMemcpyAsync(g->h_counters, g->counters, sizeof(unsigned long long) * 8,
                               cudaMemcpyDeviceToHost, s));
   MC_CUDA_TRY(cudaStreamSynchronize(s));
+  if (sl.trace && g->h_counters[7])
+    std::fprintf(stderr, "mercury: %llu centers built their outer rows per edge\n",
+                 (unsigned long long)g->h_counters[7]);
   if (budget_ms > 0 && g->h_counters[6]) return MC_ERR_TIMEOUT;  // a kernel stopped early
   const unsigned long long c1 = g->h_counters[0], c2 = g->h_counters[1];
   *out = (pattern == 4 || pattern == 6) ? c1 : c1 - c2;

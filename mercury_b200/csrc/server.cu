@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <deque>
@@ -189,7 +190,10 @@ void run_batch(mc_server *s, std::vector<std::shared_ptr<Request>> &batch, int64
   std::vector<uint64_t> counts(G, 0);
   int status = MC_OK;
   auto cuda_ok = [&](cudaError_t e) {
-    if (e != cudaSuccess && status == MC_OK) status = e == cudaErrorMemoryAllocation ? MC_ERR_OOM : MC_ERR_CUDA;
+    if (e != cudaSuccess && status == MC_OK) {
+      status = e == cudaErrorMemoryAllocation ? MC_ERR_OOM : MC_ERR_CUDA;
+      set_last_cuda_error(e);
+    }
     return status == MC_OK;
   };
   int64_t e_total = 0;
@@ -312,6 +316,11 @@ void run_batch(mc_server *s, std::vector<std::shared_ptr<Request>> &batch, int64
     s->stats.max_batch_seen = std::max<int64_t>(s->stats.max_batch_seen, G);
   }
   s->work_cv.notify_all();  // memory came back: queued requests may now fit
+  if (status == MC_ERR_CUDA) {
+    const cudaError_t e = last_cuda_error() != cudaSuccess ? last_cuda_error() : cudaGetLastError();
+    std::fprintf(stderr, "mercury server: a batch of %d requests failed: %s\n", G,
+                 cudaGetErrorString(e));
+  }
   finish(s, batch, counts, status);
 }
 

@@ -104,6 +104,18 @@ class Graph:
         arr.flags.writeable = False
         return arr
 
+    def load_vlabels(self, prefix: str) -> None:
+        """Reads <prefix>.vlabel.bin (one uint8 per vertex, graph.cc:37-58)."""
+        check(lib().mc_graph_load_vlabels(self._h, prefix.encode()), f"labels of {prefix}")
+
+    @property
+    def vlabels(self) -> Optional[np.ndarray]:
+        p = C.c_void_p()
+        check(lib().mc_graph_vlabels(self._h, C.byref(p)), "graph labels")
+        if not p.value:
+            return None
+        return np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint8)), shape=(self.n,)).copy()
+
     def validate(self, symmetry: bool = True) -> None:
         check(lib().mc_graph_validate(self._h, 1 if symmetry else 0), "graph contract")
 
@@ -245,6 +257,48 @@ class DeviceGraph:
         col = np.zeros(max(int(rp[-1]), 1), dtype=np.int32)
         check(lib().mc_dgraph_export_dag(self._h, rp.ctypes.data, col.ctypes.data), "export dag")
         return rp, col[: int(rp[-1])]
+
+    # -- vertex labels (graph.cc:37-58, :396-495) -------------------------
+    def set_vlabels(self, labels, max_label: int) -> None:
+        """Copies one uint8 label per vertex to the device (labels <= max_label)."""
+        labels = np.ascontiguousarray(labels, dtype=np.uint8)
+        if len(labels) != self.n:
+            raise ValueError("one label per vertex")
+        self._max_label = int(max_label)
+        check(lib().mc_dgraph_set_vlabels(self._h, labels.ctypes.data, int(max_label)),
+              "vertex labels")
+
+    def label_frequency(self) -> np.ndarray:
+        """Vertices per label 0..max_label (computeLabelsFrequency)."""
+        out = np.zeros(self._max_label + 1, dtype=np.uint64)
+        check(lib().mc_label_frequency(self._h, out.ctypes.data_as(C.POINTER(C.c_uint64))),
+              "label frequency")
+        return out
+
+    def label_reverse_index(self) -> Tuple[np.ndarray, np.ndarray]:
+        """(offsets, vertices): vertices grouped by label in id order
+        (BuildReverseIndex / getVerticesByLabel)."""
+        off = np.zeros(self._max_label + 2, dtype=np.int64)
+        verts = np.zeros(max(self.n, 1), dtype=np.int32)
+        check(lib().mc_label_reverse_index(self._h, off.ctypes.data, verts.ctypes.data),
+              "label reverse index")
+        return off, verts[: self.n]
+
+    def label_nlf(self, v_begin: int = 0, v_end: Optional[int] = None) -> np.ndarray:
+        """Rows of neighbour-label counts for vertices [v_begin, v_end) (BuildNLF)."""
+        v_end = self.n if v_end is None else v_end
+        out = np.zeros((max(v_end - v_begin, 0), self._max_label + 1), dtype=np.uint32)
+        check(lib().mc_label_nlf(self._h, v_begin, v_end, out.ctypes.data if out.size else None),
+              "neighbourhood label frequency")
+        return out
+
+    def tc_count_by_label(self) -> np.ndarray:
+        """Triangles split by the label of their DAG sink (intersect_num with a
+        label over the degree-ordered DAG); the entries sum to tc_count()."""
+        out = np.zeros(self._max_label + 1, dtype=np.uint64)
+        check(lib().mc_tc_count_by_label(self._h, out.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                         C.byref(self.last_timing)), "labelled triangle count")
+        return out
 
     def close(self) -> None:
         if self._h and self._h.value:

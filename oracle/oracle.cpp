@@ -17,6 +17,11 @@
 //                       dropped).  Parity pinned in tests/test_oracle.py
 //                       against brute-force triangle enumeration and the
 //                       fixtures in tests/golden/.
+//   * orc_tc_by_label -- the labelled two-pointer merge of
+//                       Graph::intersect_num(v, u, label) (graph.cc:396-411,
+//                       counted only when vlabels[a] == label), summed over
+//                       the DAG edges v->u for every label at once: counts[l]
+//                       = triangles whose common out-neighbour has label l.
 //   * orc_pattern    -- the P1..P8 formulas of
 //                       subgraph_matching/pattern_kernels.cuh (see the
 //                       comment above each case below).
@@ -173,6 +178,39 @@ double orc_merge_volume(int64_t n, const int64_t *dag_rowptr, const int32_t *dag
 }
 
 // Whole triangle count of a symmetric CSR.
+// counts[0..max_label]; labels[v] <= max_label.
+void orc_tc_by_label(int64_t n, const int64_t *rowptr, const int32_t *col, const uint8_t *labels,
+                     int max_label, uint64_t *counts) {
+  std::vector<int64_t> drp(n + 1);
+  orc_orient(n, rowptr, col, drp.data(), nullptr);
+  std::vector<int32_t> dcol(std::max<int64_t>(drp[n], 1));
+  orc_orient(n, rowptr, col, drp.data(), dcol.data());
+  const int L1 = max_label + 1;
+  std::vector<uint64_t> total(L1, 0);
+#pragma omp parallel
+  {
+    std::vector<uint64_t> mine(L1, 0);
+#pragma omp for schedule(dynamic, 256)
+    for (int64_t v = 0; v < n; ++v) {
+      for (int64_t e = drp[v]; e < drp[v + 1]; ++e) {
+        const int32_t u = dcol[e];
+        const int32_t *a = dcol.data() + drp[v], *b = dcol.data() + drp[u];
+        const int64_t na = drp[v + 1] - drp[v], nb = drp[u + 1] - drp[u];
+        int64_t i = 0, j = 0;
+        while (i < na && j < nb) {  // intersect_num's merge, label per hit
+          const int32_t x = a[i], y = b[j];
+          if (x <= y) ++i;
+          if (y <= x) ++j;
+          if (x == y) ++mine[labels[x]];
+        }
+      }
+    }
+#pragma omp critical
+    for (int l = 0; l < L1; ++l) total[l] += mine[l];
+  }
+  for (int l = 0; l < L1; ++l) counts[l] = total[l];
+}
+
 uint64_t orc_tc(int64_t n, const int64_t *rowptr, const int32_t *col) {
   std::vector<int64_t> drp(n + 1);
   orc_orient(n, rowptr, col, drp.data(), nullptr);

@@ -45,6 +45,8 @@ def lib() -> C.CDLL:
         L.orc_tc.restype = C.c_uint64
         L.orc_pattern.argtypes = [C.c_int64, P, P, C.c_int, P]
         L.orc_pattern.restype = C.c_uint64
+        L.orc_tc_by_label.argtypes = [C.c_int64, P, P, P, C.c_int, P]
+        L.orc_tc_by_label.restype = None
         L.orc_pattern_fast.argtypes = [C.c_int64, P, P, C.c_int, P]
         L.orc_pattern_fast.restype = C.c_uint64
         L.orc_csr_build.argtypes = [C.c_int64, C.c_int64, P, P, P, P]
@@ -92,6 +94,36 @@ def division(rowptr, col, deg_thd: int = 128) -> dict:
 def tc(rowptr, col) -> int:
     rowptr, col = _csr(rowptr, col)
     return int(lib().orc_tc(len(rowptr) - 1, rowptr.ctypes.data, col.ctypes.data))
+
+
+def tc_by_label(rowptr, col, labels, max_label: int) -> np.ndarray:
+    """Triangles split by the label of their DAG sink (labelled intersect_num)."""
+    rowptr, col = _csr(rowptr, col)
+    labels = np.ascontiguousarray(labels, dtype=np.uint8)
+    out = np.zeros(max_label + 1, dtype=np.uint64)
+    lib().orc_tc_by_label(len(rowptr) - 1, rowptr.ctypes.data, col.ctypes.data,
+                          labels.ctypes.data, max_label, out.ctypes.data)
+    return out
+
+
+def nlf(rowptr, col, labels, max_label: int) -> np.ndarray:
+    """Dense neighbourhood label frequency (Graph::BuildNLF, numpy)."""
+    rowptr, col = _csr(rowptr, col)
+    labels = np.asarray(labels, dtype=np.int64)
+    n = len(rowptr) - 1
+    src = np.repeat(np.arange(n), np.diff(rowptr))
+    out = np.zeros((n, max_label + 1), dtype=np.uint32)
+    np.add.at(out, (src, labels[col]), 1)
+    return out
+
+
+def label_reverse_index(labels, max_label: int):
+    """(offsets, vertices) of Graph::BuildReverseIndex (numpy, stable by id)."""
+    labels = np.asarray(labels, dtype=np.int64)
+    freq = np.bincount(labels, minlength=max_label + 1)
+    off = np.zeros(max_label + 2, dtype=np.int64)
+    np.cumsum(freq, out=off[1:])
+    return off, np.argsort(labels, kind="stable").astype(np.int32)
 
 
 def tc_dag(dag_rowptr, dag_col, v0: int = 0, v1: int | None = None) -> int:
