@@ -11,7 +11,10 @@ constexpr int kEdgesPerThread = 16;        // consecutive CSR entries per thread
 constexpr int64_t kTileEdges = (int64_t)kTileThreads * kEdgesPerThread;
 constexpr int kLeafMaxOut = 64;            // d+(owner) <= this: warp task
 constexpr int kLeafSlots = 256;            // per-warp hash slots for leaf owners
-constexpr int kHubChunk = 512;             // owner's neighbours per CTA (hub) task
+#ifndef MC_HUB_CHUNK
+#define MC_HUB_CHUNK 512
+#endif
+constexpr int kHubChunk = MC_HUB_CHUNK;    // owner's neighbours per CTA (hub) task
 constexpr int kLeafChunk = 64;             // owner's neighbours per warp (leaf) task
 constexpr int kCountThreads = 256;         // threads per counting CTA
 constexpr int kHubTableLog2Max = 15;       // at most 32768 slots (128 KB smem)

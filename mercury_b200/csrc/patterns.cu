@@ -2086,8 +2086,39 @@ int center_path(mc_dgraph *g, int pattern, PatArgs a, int grid, Slicer *sl) {
 // slices (hub edges can take seconds each; see Slicer).
 constexpr int64_t kSliceDegree = 4096;
 
+namespace {
+int pattern_count_body(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12,
+                       mc_timing_t *timing, int shard, int num_shards, double budget_ms,
+                       double *progress);
+
+// The pattern scratch (frontier lists, center classes, two-hop rows, hub
+// bitmaps) goes back to the stream-ordered pool after every count: a later
+// count on any handle reuses it from the pool, and a process that keeps
+// thousands of small graphs resident holds their CSRs only.
+void release_pattern_scratch(mc_dgraph *g) {
+  void **bufs[] = {&g->pat_scratch, &g->center_scratch, &g->hop_scratch, &g->hub_bits};
+  size_t *sizes[] = {&g->pat_scratch_bytes, &g->center_scratch_bytes, &g->hop_scratch_bytes,
+                     &g->hub_bits_bytes};
+  for (int i = 0; i < 4; ++i) {
+    if (*bufs[i]) dev_free(*bufs[i], g->stream);
+    *bufs[i] = nullptr;
+    *sizes[i] = 0;
+  }
+}
+}  // namespace
+
 int pattern_count(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12, mc_timing_t *timing,
                   int shard, int num_shards, double budget_ms, double *progress) {
+  const int rc = pattern_count_body(g, pattern, out, c12, timing, shard, num_shards, budget_ms,
+                                    progress);
+  release_pattern_scratch(g);
+  return rc;
+}
+
+namespace {
+int pattern_count_body(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12,
+                       mc_timing_t *timing, int shard, int num_shards, double budget_ms,
+                       double *progress) {
   NvtxRange range("pattern_count");
   // MERCURY_PATTERN_SLICE=1/0 forces slicing on/off (the tests compare both);
   // MERCURY_PATTERN_SLICE_MS sets the target slice length; MERCURY_TRACE_SLICES
@@ -2192,6 +2223,7 @@ int pattern_count(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12, mc_ti
   return MC_OK;
 }
 
+}  // namespace
 }  // namespace mc
 
 extern "C" int mc_pattern_count(mc_dgraph_t *g, int pattern, uint64_t *count, mc_timing_t *timing) {

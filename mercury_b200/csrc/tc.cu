@@ -188,15 +188,17 @@ struct Partners {
 __device__ __forceinline__ Partners find_partners(const CountArgs &a, int x, int px, int64_t e0,
                                                   int nc, long long *s_base, int *s_off,
                                                   unsigned long long *s_warp, int owner_bits) {
-  static_assert(kHubChunk == 2 * kCountThreads, "two neighbours per thread");
+  constexpr int kR = kHubChunk / kCountThreads;  // neighbours per thread
+  static_assert(kR * kCountThreads == kHubChunk && kHubChunk <= 1024,
+                "whole neighbours per thread; 16-bit scan fields");
   constexpr int kWarps = kCountThreads / kWarp;
   const int lane = threadIdx.x & (kWarp - 1), warp = threadIdx.x / kWarp;
-  int len[2] = {0, 0};
-  long long st[2] = {0, 0};
-  bool dense[2] = {false, false};
+  int len[kR] = {};
+  long long st[kR] = {};
+  bool dense[kR] = {};
 #pragma unroll
-  for (int r = 0; r < 2; ++r) {
-    const int i = 2 * threadIdx.x + r;
+  for (int r = 0; r < kR; ++r) {
+    const int i = kR * threadIdx.x + r;
     if (i < nc) {
       const int y = __ldg(a.col + e0 + i);
       const int4 pi = __ldg(a.pinfo + y);
@@ -215,7 +217,7 @@ __device__ __forceinline__ Partners find_partners(const CountArgs &a, int x, int
   }
   unsigned long long mine = 0;
 #pragma unroll
-  for (int r = 0; r < 2; ++r) {
+  for (int r = 0; r < kR; ++r) {
     if (dense[r]) mine += 1ull << 16;
     else if (len[r] >= kLongList) mine += 1ull << 48;
     else if (len[r] > 0) mine += (1ull << 32) + (unsigned)len[r];
@@ -242,7 +244,7 @@ __device__ __forceinline__ Partners find_partners(const CountArgs &a, int x, int
   int sslot = nl + (int)((excl >> 32) & 0xffff), off = (int)(excl & 0xffff);
   int dslot = (int)((excl >> 16) & 0xffff);
 #pragma unroll
-  for (int r = 0; r < 2; ++r) {
+  for (int r = 0; r < kR; ++r) {
     if (dense[r]) {
       s_base[kHubChunk - 1 - dslot] = st[r];
       ++dslot;

@@ -239,7 +239,7 @@ def test_pattern_bench_graph_counts_equal_committed_oracle():
 
 @pytest.mark.parametrize("words", [None, "2048"])
 @pytest.mark.parametrize("make", [lambda: Graph.chung_lu(30000, 2.1, 12.0, 900.0, seed=7),
-                                  lambda: Graph.rmat(12, 16, seed=5)])
+                                  lambda: Graph.rmat(10, 16, seed=5)])
 def test_center_route_two_hop_rows_equal_per_edge_rows(monkeypatch, make, words):
     """The center route's outer rows R(y) = N(y) & N0 come from the center's
     two-hop rows (built once per center) or are built per edge
