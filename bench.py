@@ -741,6 +741,55 @@ def run_serve(a, local_rank):
     return 0
 
 
+def pattern_bytes(rowptr, col):
+    """Algorithmic bytes of each pattern on one graph, per the pinned formula
+    B_P = 8 (n + 1) + 8 * 2m + sum over directed edges (v0, v1) of
+    4 (d(v0) + d(v1)) + sum over the edge's first-level list L1 of
+    (16 + 4 d(x)): L1 = N(v0) per vertex for P1's star, A = N(v0) - N(v1)
+    for P2/P3/P4 (P4 only over v1 < v0), A = N(v0) & N(v1) for P5-P8.  The
+    per-edge sums over N(v0) & N(v1) come from sparse products ((A D A) o A
+    and (A A) o A, D = diag(degree)); None above 5 M entries (the products
+    grow with the sum of squared degrees)."""
+    import scipy.sparse as sp
+    rowptr, col = np.asarray(rowptr), np.asarray(col)
+    n, nnz = len(rowptr) - 1, len(col)
+    if nnz > 5_000_000:
+        return None
+    d = np.diff(rowptr).astype(np.float64)
+    A = sp.csr_matrix((np.ones(nnz), col, rowptr), shape=(n, n))
+    W = (A.multiply(d[None, :]).tocsr() @ A).multiply(A).tocsr()  # sum of d(x), x in N0 & N1
+    S = (A @ A).multiply(A).tocsr()                                # |N0 & N1|
+    bv = A @ d                                                     # sum of d(x), x in N(v)
+    sumsq = float((d * d).sum())
+    base = 8.0 * (n + 1) + 8.0 * nnz + 8.0 * sumsq
+    w_all, s_all = float(W.sum()), float(S.sum())
+    low = sp.tril(A, -1).tocsr()                                   # v1 < v0
+    low_d0 = float((np.asarray(low.sum(axis=1)).ravel() * d).sum())
+    low_b0 = float((np.asarray(low.sum(axis=1)).ravel() * bv).sum())
+    w_low, s_low = float(sp.tril(W, -1).sum()), float(sp.tril(S, -1).sum())
+    outer = 16.0 * (sumsq - s_all) + 4.0 * (float((d * bv).sum()) - w_all)
+    inner = 16.0 * s_all + 4.0 * w_all
+    out = {"P1": base + float((16.0 * d + 4.0 * bv).sum()), "P2": base + outer, "P3": base + outer,
+           "P4": base + 16.0 * (low_d0 - s_low) + 4.0 * (low_b0 - w_low)}
+    for k in (5, 6, 7, 8):
+        out[f"P{k}"] = base + inner
+    return out
+
+
+def pattern_cpu_baseline(rowptr, col, patterns=(1, 4, 6, 7, 8)):
+    """The oracle's restatement of the cheaper formulas, timed on the host cores."""
+    from oracle import oracle as orc
+    total, secs, done = 0, 0.0, []
+    for k in patterns:
+        t0 = time.perf_counter()
+        total += orc.pattern(rowptr, col, k)
+        secs += time.perf_counter() - t0
+        done.append(f"P{k}")
+    return {"value": total / secs, "unit": "matches/s", "cores": orc.num_threads(), "kind": "port",
+            "sample": f"oracle restatement of {','.join(done)} on the whole graph, {secs:.1f} s; "
+                      f"counts summed over those patterns / their summed time"}
+
+
 def load_pattern_golden(a):
     """Committed counts for this pattern workload (tests/golden/pattern_counts.json)."""
     path = os.path.join(ROOT, "tests", "golden", "pattern_counts.json")
@@ -810,6 +859,19 @@ def run_patterns(a, rank, world, local_rank):
         dist.destroy_process_group()
         if rank != 0:
             return 0
+    # Algorithmic bytes per pattern (information: the graph is L2-resident at
+    # the default size, so the HBM fraction is reported, not targeted).
+    peak, peak_kind = load_peaks()
+    bp = pattern_bytes(g.rowptr, g.col) if rank == 0 else None
+    if bp:
+        for p in per:
+            b = bp[p["pattern"]]
+            p["algorithmic_bytes"] = b
+            p["algorithmic_gbs"] = b / (p["ms"] / 1e3) / 1e9
+            p["hbm_frac"] = p["algorithmic_gbs"] / peak
+    cpu = None
+    if world == 1 and not a.no_cpu_baseline and g.nnz <= 5_000_000:
+        cpu = pattern_cpu_baseline(g.rowptr, g.col)
     done = [p["matches_per_s"] for p in per if p["matches_per_s"]]
     line = {"metric": "P1-P8 matches/s", "value": statistics.mean(done) if done else None,
             "unit": "matches/s", "n_gpus": world, "higher_is_better": True, "vs_baseline": None,
@@ -818,7 +880,12 @@ def run_patterns(a, rank, world, local_rank):
                                    f"{a.pat_cap} seed 1", "n": g.n, "m": g.nnz // 2,
                        "max_degree": g.max_degree,
                        "budget_ms_per_pattern": a.pat_budget_ms if a.pat_budget_ms > 0 else None},
-            "patterns": per, "unfinished": unfinished}
+            "patterns": per, "unfinished": unfinished,
+            "roofline_note": (f"per pattern: algorithmic_bytes = 8(n+1) + 16m + sum over directed "
+                              f"edges of 4(d0+d1) + sum over L1 of (16 + 4 d(x)); hbm_frac against "
+                              f"the {peak_kind} {peak:.0f} GB/s")}
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
     return 0
 

@@ -142,3 +142,30 @@ def test_workload_config_names_the_placement():
     a.host_columns = True
     cfg = bench.workload_config(a)
     assert cfg["columns"] == "host" and "host memory" in cfg["workload"]
+
+
+def loop_pattern_bytes(n, rp, col):
+    nb = [set(col[rp[v]:rp[v + 1]].tolist()) for v in range(n)]
+    d = [len(x) for x in nb]
+    m2 = len(col)
+    base = 8.0 * (n + 1) + 8.0 * m2
+    edges = [(v0, int(v1)) for v0 in range(n) for v1 in col[rp[v0]:rp[v0 + 1]]]
+    base += sum(4 * (d[v0] + d[v1]) for v0, v1 in edges)
+    cost = lambda xs: sum(16 + 4 * d[x] for x in xs)  # noqa: E731
+    out = {"P1": base + sum(cost(nb[v]) for v in range(n))}
+    outer = sum(cost(nb[v0] - nb[v1]) for v0, v1 in edges)
+    out["P2"] = out["P3"] = base + outer
+    out["P4"] = base + sum(cost(nb[v0] - nb[v1]) for v0, v1 in edges if v1 < v0)
+    inner = sum(cost(nb[v0] & nb[v1]) for v0, v1 in edges)
+    for k in (5, 6, 7, 8):
+        out[f"P{k}"] = base + inner
+    return out
+
+
+@pytest.mark.parametrize("n,p,seed", [(40, 0.3, 4), (120, 0.2, 5)])
+def test_pattern_bytes_equal_the_loop_restatement(n, p, seed):
+    rp, col = csr_from_edges(n, random_graph(n, p, seed))
+    got = bench.pattern_bytes(np.asarray(rp), np.asarray(col))
+    want = loop_pattern_bytes(n, np.asarray(rp), np.asarray(col))
+    for k, v in want.items():
+        assert got[k] == pytest.approx(v, rel=1e-12), k
