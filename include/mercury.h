@@ -369,7 +369,8 @@ int mc_tc_count_by_label(mc_dgraph_t *g, uint64_t *counts, mc_timing_t *timing);
  * fits the HBM budget -- up to max_batch per batch, in arrival order, and
  * closing a batch once its estimated work (n + nnz per triangle job, the sum
  * of squared degrees per pattern job) would pass 2^23 entry visits
- * (MERCURY_SERVE_BATCH_WORK), so a request above that runs alone --
+ * (MERCURY_SERVE_BATCH_WORK), or the queued work's share per worker when
+ * that is larger; a request above 2^23 runs alone --
  * assemble the batch on the device, count it with the batch kernels and
  * deliver each graph's count; requests that arrive while batches run are
  * admitted as memory is returned, and batches of different workers overlap

@@ -32,7 +32,7 @@ void release(mc_dgraph *g) {
                   g->mega_cnt,   g->mega_off,   g->mega_tasks, g->rank,
                   g->dag_rank,   g->rank_keys,  g->rank_counts, g->rank_offsets,
                   g->center_scratch, g->stage, g->chunk_offsets, g->core_bits, g->pinfo,
-                  g->hop_scratch, g->hub_bits, g->vlabels};
+                  g->hop_scratch, g->hub_bits, g->vlabels, g->tile_rows};
   if (g->col_host) bufs[1] = nullptr;  // pinned host memory, freed below
   // Stream-ordered frees: no device-wide synchronisation, so other handles'
   // work keeps running while this one is released.
@@ -158,8 +158,40 @@ int finish_create(mc_dgraph *g, unsigned flags, mc_dgraph **out, int rc) {
 struct HostCache {
   mc_dgraph *g = nullptr;
   int64_t cap_n = -1, cap_nnz = -1;
-  ~HostCache() { release(g); }
+  // Pinned staging for callers that pass pageable arrays: two column slots
+  // of one upload chunk each, and the row offsets.
+  int32_t *pin_col[2] = {nullptr, nullptr};
+  int64_t pin_col_entries = 0;
+  int64_t *pin_rowptr = nullptr;
+  int64_t pin_rowptr_entries = 0;
+  cudaEvent_t pin_done[2] = {nullptr, nullptr};
+  void drop_pins() {
+    for (auto &p : pin_col) {
+      if (p) cudaFreeHost(p);
+      p = nullptr;
+    }
+    if (pin_rowptr) cudaFreeHost(pin_rowptr);
+    pin_rowptr = nullptr;
+    pin_col_entries = pin_rowptr_entries = 0;
+    for (auto &e : pin_done) {
+      if (e) cudaEventDestroy(e);
+      e = nullptr;
+    }
+  }
+  ~HostCache() {
+    release(g);
+    drop_pins();
+  }
 };
+
+bool is_pageable(const void *p) {
+  cudaPointerAttributes attr{};
+  if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return attr.type == cudaMemoryTypeUnregistered;
+}
 thread_local HostCache t_cache;
 
 }  // namespace
@@ -522,12 +554,54 @@ int mc_tc_count_host(const int64_t *rowptr, const int32_t *col, int64_t n, int64
   mc_dgraph *g = c.g;
   g->n = n;
   g->nnz = nnz;
+  // Pageable arrays (the reference loader's new[] arrays) cross the link
+  // through pinned slots that the host threads fill (see staged_dag_passes).
+  const bool pageable = !g->col_host && nnz > 0 && mc::is_pageable(col);
+  g->pin_slot[0] = g->pin_slot[1] = nullptr;
+  g->pin_entries = 0;
+  if (pageable) {
+    const int64_t want = g->chunk_edges;  // one upload chunk (whole tiles)
+    if (c.pin_col_entries < want || c.pin_rowptr_entries < n + 1) {
+      c.drop_pins();
+      MC_CUDA_TRY(cudaHostAlloc((void **)&c.pin_col[0], sizeof(int32_t) * (size_t)want,
+                                cudaHostAllocPortable));
+      MC_CUDA_TRY(cudaHostAlloc((void **)&c.pin_col[1], sizeof(int32_t) * (size_t)want,
+                                cudaHostAllocPortable));
+      MC_CUDA_TRY(cudaHostAlloc((void **)&c.pin_rowptr, sizeof(int64_t) * (size_t)(n + 1),
+                                cudaHostAllocPortable));
+      MC_CUDA_TRY(cudaEventCreateWithFlags(&c.pin_done[0], cudaEventDisableTiming));
+      MC_CUDA_TRY(cudaEventCreateWithFlags(&c.pin_done[1], cudaEventDisableTiming));
+      c.pin_col_entries = want;
+      c.pin_rowptr_entries = n + 1;
+    }
+    g->pin_slot[0] = c.pin_col[0];
+    g->pin_slot[1] = c.pin_col[1];
+    g->pin_entries = c.pin_col_entries;
+    g->pin_done[0] = c.pin_done[0];
+    g->pin_done[1] = c.pin_done[1];
+  }
   cudaEvent_t e0, e1;
   MC_CUDA_TRY(cudaEventCreate(&e0));
   MC_CUDA_TRY(cudaEventCreate(&e1));
   MC_CUDA_TRY(cudaEventRecord(e0, g->stream));
-  MC_CUDA_TRY(cudaMemcpyAsync(g->rowptr, rowptr, sizeof(int64_t) * (size_t)(n + 1),
-                              cudaMemcpyHostToDevice, g->stream));
+  if (pageable) {
+    // The previous call's copy out of the pinned offsets has finished (that
+    // call synchronised its stream before returning).
+    const int64_t *src = rowptr;
+    int64_t *dst = c.pin_rowptr;
+    const int64_t count = n + 1;
+    constexpr int64_t kPiece = 1 << 17;
+#pragma omp parallel for schedule(static)
+    for (int64_t p = 0; p < (count + kPiece - 1) / kPiece; ++p) {
+      const int64_t a = p * kPiece, b = std::min(count, a + kPiece);
+      std::memcpy(dst + a, src + a, sizeof(int64_t) * (size_t)(b - a));
+    }
+    MC_CUDA_TRY(cudaMemcpyAsync(g->rowptr, c.pin_rowptr, sizeof(int64_t) * (size_t)(n + 1),
+                                cudaMemcpyHostToDevice, g->stream));
+  } else {
+    MC_CUDA_TRY(cudaMemcpyAsync(g->rowptr, rowptr, sizeof(int64_t) * (size_t)(n + 1),
+                                cudaMemcpyHostToDevice, g->stream));
+  }
   if (nnz > 0 && g->col_host) mc::copy_to_pinned(g->col_h, col, nnz);  // while the offsets upload
   MC_CUDA_TRY(cudaEventRecord(e1, g->stream));
   g->launches = 0;

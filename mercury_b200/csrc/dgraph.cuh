@@ -107,6 +107,13 @@ struct mc_dgraph {
   uint16_t *keep = nullptr;       // one DAG keep mask per orientation thread
   int32_t *tile_counts = nullptr; // tiles
   int64_t *tile_offsets = nullptr;// tiles + 1
+  int64_t *tile_rows = nullptr;   // 2 x tiles: first and last row of each tile
+  // Streamed upload from pageable host memory: two pinned slots of
+  // pin_entries column entries (owned by the caller of the upload) and the
+  // events that mark each slot's copy to the device done.
+  int32_t *pin_slot[2] = {nullptr, nullptr};
+  int64_t pin_entries = 0;
+  cudaEvent_t pin_done[2] = {nullptr, nullptr};
   int32_t *hub_cnt = nullptr, *leaf_cnt = nullptr, *mega_cnt = nullptr;    // n
   int64_t *hub_off = nullptr, *leaf_off = nullptr, *mega_off = nullptr;    // n + 1
   uint64_t *hub_tasks = nullptr, *leaf_tasks = nullptr, *mega_tasks = nullptr;  // capacity

@@ -21,6 +21,7 @@
 //   B  DAG entries and row offsets written from the keep masks
 // Each vertex's (degree, d+) pair is one 8-byte word (key[]).
 #include <algorithm>
+#include <cstring>
 #include <climits>
 #include <cstdio>
 #include <cstdlib>
@@ -82,11 +83,19 @@ struct TileRows {
   }
 };
 
+// rows (optional): {first row, last row} of this tile, precomputed by
+// tile_rows_kernel; without it two threads binary-search rowptr (22
+// dependent loads at n = 4 M, which the rest of the CTA waits for).
 __device__ __forceinline__ TileRows load_tile_rows(const int64_t *rowptr, int64_t n, int64_t t0,
-                                                   int64_t t1, int64_t *seg) {
+                                                   int64_t t1, int64_t *seg,
+                                                   const int64_t *rows = nullptr) {
   __shared__ int64_t sh[2];
-  if (threadIdx.x == 0) sh[0] = upper_row(rowptr, 0, n - 1, t0);
-  if (threadIdx.x == kTileThreads - 1) sh[1] = upper_row(rowptr, 0, n - 1, t1 - 1);
+  if (rows) {
+    if (threadIdx.x < 2) sh[threadIdx.x] = __ldg(rows + threadIdx.x);
+  } else {
+    if (threadIdx.x == 0) sh[0] = upper_row(rowptr, 0, n - 1, t0);
+    if (threadIdx.x == kTileThreads - 1) sh[1] = upper_row(rowptr, 0, n - 1, t1 - 1);
+  }
   __syncthreads();
   TileRows tr{rowptr, nullptr, sh[0], sh[1]};
   const int64_t len = tr.hi - tr.lo + 2;
@@ -186,7 +195,8 @@ __global__ void __launch_bounds__(kTileThreads)
                     uint16_t *keep_masks, int32_t *counts_out,
                     const int64_t *__restrict__ offs_in, int64_t *out_rowptr, int32_t *out_col,
                     const int32_t *__restrict__ rank, int32_t *out_rank,
-                    const int64_t *chunk_end, int64_t cap, const unsigned *stop) {
+                    const int64_t *chunk_end, int64_t cap, const unsigned *stop,
+                    const int64_t *__restrict__ tile_rows) {
   __shared__ int64_t seg[kSegMax];
   // Both checks read one word, the same for the whole CTA.  `stop`: the
   // contract checks of a chunk validated just before found a bad entry, so
@@ -196,7 +206,8 @@ __global__ void __launch_bounds__(kTileThreads)
   const int64_t tile = cc.tile_base + blockIdx.x;
   const int64_t t0 = tile * kTileEdges;
   const int64_t t1 = min(t0 + kTileEdges, nnz);
-  const TileRows tr = load_tile_rows(rowptr, n, t0, t1, seg);
+  const TileRows tr =
+      load_tile_rows(rowptr, n, t0, t1, seg, tile_rows ? tile_rows + 2 * tile : nullptr);
   const int64_t s = t0 + (int64_t)threadIdx.x * kEdgesPerThread;
   const int64_t e_end = min(s + kEdgesPerThread, t1);
   const int64_t slot = tile * kTileThreads + threadIdx.x;
@@ -252,6 +263,23 @@ __global__ void __launch_bounds__(kTileThreads)
     for (int64_t q = tr.hi + 1 + threadIdx.x; q <= n; q += kTileThreads) out_rowptr[q] = base + total;
 }
 
+// rows[2t] / rows[2t + 1] = the rows holding the first and the last entry of
+// tile t: each non-empty row marks the tiles whose first or last entry it
+// holds (rowptr validated: monotone, ends at nnz).
+__global__ void tile_rows_kernel(const int64_t *__restrict__ rowptr, int64_t n, int64_t nnz,
+                                 int64_t tiles, int64_t *rows) {
+  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n) return;
+  const int64_t b = rowptr[v], e = rowptr[v + 1];
+  if (b >= e) return;
+  for (int64_t t = b / kTileEdges; t <= (e - 1) / kTileEdges && t < tiles; ++t) {
+    const int64_t first = t * kTileEdges;
+    const int64_t last = min(first + kTileEdges, nnz) - 1;
+    if (first >= b && first < e) rows[2 * t] = v;
+    if (last >= b && last < e) rows[2 * t + 1] = v;
+  }
+}
+
 // Tile offsets of one staged chunk: offs[0] holds the DAG entries of the
 // earlier chunks; offs[i] = offs[0] + local[i] for i in [0, count] (local is
 // the chunk's exclusive scan, local[0] = 0, so offs[0] is rewritten with its
@@ -271,11 +299,13 @@ __global__ void chunk_offsets_kernel(const int64_t *__restrict__ local, int64_t 
 __global__ void __launch_bounds__(kTileThreads)
     validate_entries_kernel(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ col,
                             int64_t n, int64_t nnz, int check_sym, unsigned *err,
-                            int64_t tile_base) {
+                            int64_t tile_base, const int64_t *__restrict__ tile_rows = nullptr) {
   __shared__ int64_t seg[kSegMax];
-  const int64_t t0 = (tile_base + blockIdx.x) * kTileEdges;
+  const int64_t tile = tile_base + blockIdx.x;
+  const int64_t t0 = tile * kTileEdges;
   const int64_t t1 = min(t0 + kTileEdges, nnz);
-  const TileRows tr = load_tile_rows(rowptr, n, t0, t1, seg);
+  const TileRows tr =
+      load_tile_rows(rowptr, n, t0, t1, seg, tile_rows ? tile_rows + 2 * tile : nullptr);
   const int64_t s = t0 + (int64_t)threadIdx.x * kEdgesPerThread;
   const int64_t e_end = min(s + kEdgesPerThread, t1);
   if (s >= t1) return;
@@ -580,7 +610,7 @@ int64_t tc_device_bytes(int64_t n, int64_t nnz, bool col_host) {
   const int64_t staging =
       col_host ? 2 * 4 * stage_capacity(nnz) + 8 * (stage_capacity(nnz) / kTileEdges + 1) : 0;
   return (n + 1) * (8 + 16 + 8 + 3 * 4 + 3 * 8 + 4 + 16) + 3 * 8 * tasks +
-         2 * 4 * dag_capacity(nnz, col_host) + tiles * (2 * kTileThreads + 12) +
+         2 * 4 * (dag_capacity(nnz, col_host) + 4) + tiles * (2 * kTileThreads + 28) +
          2 * 12 * (radix_entries(n) + 1) + scan + staging + 4 * core_offset(core_rank_count(n));
 }
 
@@ -604,6 +634,7 @@ int tc_alloc(mc_dgraph *g) {
   MC_ALLOC(g->keep, tiles * kTileThreads);
   MC_ALLOC(g->tile_counts, tiles);
   MC_ALLOC(g->tile_offsets, tiles + 1);
+  MC_ALLOC(g->tile_rows, 2 * tiles);
   MC_ALLOC(g->hub_cnt, n + 1);
   MC_ALLOC(g->leaf_cnt, n + 1);
   MC_ALLOC(g->hub_off, n + 1);
@@ -654,12 +685,33 @@ int tc_alloc(mc_dgraph *g) {
 // The DAG holds dag_cap entries; a chunk that would end past it raises
 // kErrDagCapacity and writes nothing.  The caller reads the flags before
 // counting.
+// Host copy of count entries by all host threads, in 1 MB pieces.
+static void parallel_copy(int32_t *dst, const int32_t *src, int64_t count) {
+  constexpr int64_t kPiece = 1 << 18;
+  const int64_t pieces = (count + kPiece - 1) / kPiece;
+#pragma omp parallel for schedule(static)
+  for (int64_t p = 0; p < pieces; ++p) {
+    const int64_t a = p * kPiece, b = std::min(count, a + kPiece);
+    std::memcpy(dst + a, src + a, sizeof(int32_t) * (size_t)(b - a));
+  }
+}
+
 static int staged_dag_passes(mc_dgraph *g, const int32_t *deg, const int32_t *src, bool in_place) {
   const int64_t n = g->n, nnz = g->nnz;
   cudaStream_t s = g->stream, cs = g->copy_stream;
   cudaEvent_t *copied = g->stage_ev, *drained = g->stage_ev + 2;
   const int64_t chunk = in_place ? g->chunk_edges : g->stage_edges;
   const unsigned *stop = in_place ? g->err : nullptr;
+  // A streamed upload from pageable memory goes through the pinned slots when
+  // the caller provided them (the driver's own pageable copies are slower).
+  bool pageable = false;
+  if (in_place && g->pin_slot[0] && g->pin_slot[1] && g->pin_entries >= chunk) {
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, src) == cudaSuccess)
+      pageable = attr.type == cudaMemoryTypeUnregistered;
+    else
+      cudaGetLastError();  // an unknown pointer: plain copies
+  }
   MC_CUDA_TRY(cudaMemsetAsync(g->tile_offsets, 0, sizeof(int64_t), s));
   // Copies start after the work already queued on the handle's stream.
   MC_CUDA_TRY(cudaEventRecord(drained[0], s));
@@ -671,20 +723,31 @@ static int staged_dag_passes(mc_dgraph *g, const int32_t *deg, const int32_t *sr
     const int64_t tb = e0 / kTileEdges, ct = (e1 - e0 + kTileEdges - 1) / kTileEdges;
     int32_t *buf = in_place ? g->col + e0 : g->stage + (int64_t)slot * g->stage_edges;
     if (!in_place && c >= 2) MC_CUDA_TRY(cudaStreamWaitEvent(cs, drained[slot], 0));
-    MC_CUDA_TRY(cudaMemcpyAsync(buf, src + e0, sizeof(int32_t) * (size_t)(e1 - e0),
-                                cudaMemcpyHostToDevice, cs));
+    if (pageable) {
+      // The host threads copy the chunk into a pinned slot (free once its
+      // previous copy to the device is done), then the DMA engine takes it,
+      // while the threads fill the other slot.
+      if (c >= 2) MC_CUDA_TRY(cudaEventSynchronize(g->pin_done[slot]));
+      parallel_copy(g->pin_slot[slot], src + e0, e1 - e0);
+      MC_CUDA_TRY(cudaMemcpyAsync(buf, g->pin_slot[slot], sizeof(int32_t) * (size_t)(e1 - e0),
+                                  cudaMemcpyHostToDevice, cs));
+      MC_CUDA_TRY(cudaEventRecord(g->pin_done[slot], cs));
+    } else {
+      MC_CUDA_TRY(cudaMemcpyAsync(buf, src + e0, sizeof(int32_t) * (size_t)(e1 - e0),
+                                  cudaMemcpyHostToDevice, cs));
+    }
     MC_CUDA_TRY(cudaEventRecord(copied[slot], cs));
     MC_CUDA_TRY(cudaStreamWaitEvent(s, copied[slot], 0));
     if (in_place) {
       validate_entries_kernel<<<(unsigned)ct, kTileThreads, 0, s>>>(g->rowptr, g->col, n, nnz, 0,
-                                                                    g->err, tb);
+                                                                    g->err, tb, g->tile_rows);
       MC_CUDA_TRY(cudaGetLastError());
       g->launches += 1;
     }
     const ColumnChunk cc = in_place ? ColumnChunk{g->col, 0, tb} : ColumnChunk{buf, e0, tb};
     dag_pass_kernel<false><<<(unsigned)ct, kTileThreads, 0, s>>>(
         g->rowptr, cc, deg, n, nnz, g->key, g->keep, g->tile_counts, nullptr, nullptr, nullptr,
-        nullptr, nullptr, nullptr, 0, stop);
+        nullptr, nullptr, nullptr, 0, stop, g->tile_rows);
     MC_CUDA_TRY(cudaGetLastError());
     MC_CUDA_TRY(exclusive_scan(g->tile_counts + tb, g->chunk_offsets, ct, g->scan_temp, s));
     chunk_offsets_kernel<<<grid_for(ct + 1, 256), 256, 0, s>>>(g->chunk_offsets, ct,
@@ -693,7 +756,8 @@ static int staged_dag_passes(mc_dgraph *g, const int32_t *deg, const int32_t *sr
     MC_CUDA_TRY(cudaGetLastError());
     dag_pass_kernel<true><<<(unsigned)ct, kTileThreads, 0, s>>>(
         g->rowptr, cc, deg, n, nnz, g->key, g->keep, nullptr, g->tile_offsets, g->dag_rowptr,
-        g->dag_col, g->rank, g->dag_rank, g->tile_offsets + tb + ct, g->dag_cap, stop);
+        g->dag_col, g->rank, g->dag_rank, g->tile_offsets + tb + ct, g->dag_cap, stop,
+        g->tile_rows);
     MC_CUDA_TRY(cudaGetLastError());
     MC_CUDA_TRY(cudaEventRecord(drained[slot], s));
     g->launches += 3 + scan_launches(ct);
@@ -728,6 +792,11 @@ int tc_orient(mc_dgraph *g, const int32_t *upload) {
     g->rank_sorted = sorted;
     g->launches += 2;
   }
+  if (tiles > 0) {
+    tile_rows_kernel<<<grid_for(n, 256), 256, 0, s>>>(g->rowptr, n, nnz, tiles, g->tile_rows);
+    MC_CUDA_TRY(cudaGetLastError());
+    g->launches += 1;
+  }
   if (tiles == 0) {
     MC_CUDA_TRY(cudaMemsetAsync(g->dag_rowptr, 0, sizeof(int64_t) * (n + 1), s));
   } else if (upload) {
@@ -744,13 +813,13 @@ int tc_orient(mc_dgraph *g, const int32_t *upload) {
     const ColumnChunk all{g->col, 0, 0};
     dag_pass_kernel<false><<<grid, kTileThreads, 0, s>>>(
         g->rowptr, all, deg, n, nnz, g->key, g->keep, g->tile_counts, nullptr, nullptr, nullptr,
-        nullptr, nullptr, nullptr, 0, nullptr);
+        nullptr, nullptr, nullptr, 0, nullptr, g->tile_rows);
     MC_CUDA_TRY(cudaGetLastError());
     MC_CUDA_TRY(exclusive_scan(g->tile_counts, g->tile_offsets, tiles, g->scan_temp, s));
     dag_pass_kernel<true><<<grid, kTileThreads, 0, s>>>(
         g->rowptr, all, deg, n, nnz, g->key, g->keep, nullptr, g->tile_offsets, g->dag_rowptr,
         g->dag_col, g->batch.gid ? nullptr : g->rank, g->batch.gid ? nullptr : g->dag_rank,
-        nullptr, 0, nullptr);
+        nullptr, 0, nullptr, g->tile_rows);
     MC_CUDA_TRY(cudaGetLastError());
     g->launches += 2 + scan_launches(tiles);
   }

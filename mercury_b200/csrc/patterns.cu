@@ -1555,42 +1555,80 @@ __global__ void __launch_bounds__(kPatThreads) hub_p1_kernel(HubP1Args a) {
         if (__any_sync(kFull, y >= v1)) break;
       }
       __syncwarp();
-      // Per v2 in B the whole warp counts #{k : v2 < k < v1, k in N0 & N(v2),
-      // k notin N1} over the shorter of N(v2) and N0 within (v2, v1).
+      // For v2 in B: #{k : v2 < k < v1, k in N0 & N(v2), k notin N1}, over the
+      // shorter of N(v2) and N0 within (v2, v1).  Lane t takes B[t], B[t + 32],
+      // ... and scans a short range itself; ranges above kLaneScan entries
+      // are scanned by the whole warp, one after the other.
+      constexpr int kLaneScan = 64;
       long long c2 = 0;
-      for (int tb = 0; tb < nb; ++tb) {
-        const int v2 = B[tb];
-        const int q2 = lower_pos(n0, d0, v2);  // v2's position in N0
-        const int64_t b2 = __ldg(a.rp + v2), e2 = __ldg(a.rp + v2 + 1);
-        int64_t lo = b2, hi = e2;  // first entry of N(v2) above v2
-        while (lo < hi) {
-          const int64_t mid = (lo + hi) >> 1;
-          if (__ldg(a.ci + mid) <= v2) lo = mid + 1;
-          else hi = mid;
-        }
-        int64_t top = lo, hi2 = e2;  // first entry of N(v2) at or above v1
-        while (top < hi2) {
-          const int64_t mid = (top + hi2) >> 1;
-          if (__ldg(a.ci + mid) < v1) top = mid + 1;
-          else hi2 = mid;
-        }
-        const int d2 = (int)(e2 - b2);
-        int drop = 0;
-        if (top - lo <= p - q2 - 1) {
-          for (int64_t k = lo + lane; k < top; k += kWarp) {
-            const int y = __ldg(a.ci + k);
-            drop += bit_set(bits, y) && !bsearch(n1, d1, y);
+      for (int base = 0; base < nb; base += kWarp) {
+        const int tb = base + lane;
+        int q2 = 0, side = 0;  // side 1: scan N(v2) [lo, top); 0: N0 (q2, p)
+        int64_t lo = 0, top = 0, b2 = 0;
+        int d2 = 0, len = 0;
+        if (tb < nb) {
+          const int v2 = B[tb];
+          q2 = lower_pos(n0, d0, v2);
+          b2 = __ldg(a.rp + v2);
+          const int64_t e2 = __ldg(a.rp + v2 + 1);
+          d2 = (int)(e2 - b2);
+          lo = b2;
+          int64_t hi = e2;  // first entry of N(v2) above v2
+          while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (__ldg(a.ci + mid) <= v2) lo = mid + 1;
+            else hi = mid;
           }
-        } else {
-          for (int j = q2 + 1 + lane; j < p; j += kWarp) {
-            const int y = __ldg(n0 + j);
-            drop += bsearch(a.ci + b2, d2, y) && !bsearch(n1, d1, y);
+          top = lo;
+          hi = e2;  // first entry at or above v1
+          while (top < hi) {
+            const int64_t mid = (top + hi) >> 1;
+            if (__ldg(a.ci + mid) < v1) top = mid + 1;
+            else hi = mid;
+          }
+          side = top - lo <= p - q2 - 1;
+          len = side ? (int)(top - lo) : p - q2 - 1;
+          c2 += (long long)(p - q2 - 1) - (nb - 1 - tb);
+          if (len <= kLaneScan) {
+            int drop = 0;
+            if (side) {
+              for (int64_t k = lo; k < top; ++k) {
+                const int y = __ldg(a.ci + k);
+                drop += bit_set(bits, y) && !bsearch(n1, d1, y);
+              }
+            } else {
+              for (int j = q2 + 1; j < p; ++j) {
+                const int y = __ldg(n0 + j);
+                drop += bsearch(a.ci + b2, d2, y) && !bsearch(n1, d1, y);
+              }
+            }
+            c2 -= drop;
           }
         }
-        drop = warp_sum_int(drop);
-        c2 += (long long)(p - q2 - 1) - (nb - 1 - tb) - drop;
+        unsigned longs = __ballot_sync(kFull, tb < nb && len > kLaneScan);
+        while (longs) {
+          const int src = __ffs(longs) - 1;
+          longs &= longs - 1u;
+          const int s_side = __shfl_sync(kFull, side, src);
+          const int64_t s_lo = __shfl_sync(kFull, lo, src), s_top = __shfl_sync(kFull, top, src);
+          const int64_t s_b2 = __shfl_sync(kFull, b2, src);
+          const int s_d2 = __shfl_sync(kFull, d2, src), s_q2 = __shfl_sync(kFull, q2, src);
+          int drop = 0;
+          if (s_side) {
+            for (int64_t k = s_lo + lane; k < s_top; k += kWarp) {
+              const int y = __ldg(a.ci + k);
+              drop += bit_set(bits, y) && !bsearch(n1, d1, y);
+            }
+          } else {
+            for (int j = s_q2 + 1 + lane; j < p; j += kWarp) {
+              const int y = __ldg(n0 + j);
+              drop += bsearch(a.ci + s_b2, s_d2, y) && !bsearch(n1, d1, y);
+            }
+          }
+          c2 -= drop;
+        }
       }
-      if (lane == 0) acc.c2 += (unsigned long long)c2;
+      acc.c2 += (unsigned long long)c2;
       __syncwarp();  // B is rewritten by the warp's next edge
     }
     __syncthreads();

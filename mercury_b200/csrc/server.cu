@@ -113,6 +113,8 @@ struct mc_server {
   int64_t budget = 0;
   int max_batch = 0;
   int64_t batch_work = 0;  // cap on a batch's estimated work (see work_of)
+  int64_t pending_work = 0;  // estimated work of the queued requests
+  int num_workers = 1;
   std::mutex mu;
   std::condition_variable work_cv, done_cv;
   std::deque<std::shared_ptr<mc::Request>> pending;
@@ -337,13 +339,18 @@ void worker_main(mc_server *s) {
         if (s->stop && s->pending.empty()) break;
         // Admit queued requests in arrival order while they fit the budget
         // and the batch's work cap.
+        // The cap grows with the backlog (its share per worker), so a queue
+        // that builds up is drained in larger batches; a request above the
+        // base cap still runs alone.
+        const int64_t cap = std::max(s->batch_work, s->pending_work / s->num_workers);
         while (!s->pending.empty() && (int)batch.size() < s->max_batch) {
           auto &r = s->pending.front();
           const int64_t w = work_of(*r);
-          if (!batch.empty() && work + w > s->batch_work) break;  // next batch
+          if (!batch.empty() && (work + w > cap || w > s->batch_work)) break;  // next batch
           int64_t f = footprint(*r);
-          const int64_t cap = r->job != 0 ? std::max(pattern_cap, r->max_degree) : pattern_cap;
-          if (cap > pattern_cap) f += pattern_scratch(cap) - (pattern_cap ? pattern_scratch(pattern_cap) : 0);
+          const int64_t cap_deg = r->job != 0 ? std::max(pattern_cap, r->max_degree) : pattern_cap;
+          if (cap_deg > pattern_cap)
+            f += pattern_scratch(cap_deg) - (pattern_cap ? pattern_scratch(pattern_cap) : 0);
           if (f > s->budget) {  // can never fit: refuse it
             if (r->prepinned) {
               auto c = s->cache.find(r->key);
@@ -353,6 +360,7 @@ void worker_main(mc_server *s) {
             r->done = true;
             r->latency_ms = ms_since(r->submitted);
             ++s->stats.failed;
+            s->pending_work -= w;
             s->pending.pop_front();
             s->done_cv.notify_all();
             continue;
@@ -361,11 +369,12 @@ void worker_main(mc_server *s) {
           if (s->in_use + s->cache_bytes + reserved + f > s->budget && (!batch.empty() || s->in_use > 0))
             break;  // wait for memory from running batches
           reserved += f;
-          pattern_cap = cap;
+          pattern_cap = cap_deg;
           work += w;
+          s->pending_work -= w;
           batch.push_back(r);
           s->pending.pop_front();
-          if (work > s->batch_work) break;  // a large request runs alone
+          if (w > s->batch_work) break;  // a large request runs alone
         }
         if (!batch.empty()) break;
         s->work_cv.wait(lock);
@@ -400,6 +409,7 @@ int mc_server_create(int64_t hbm_budget_bytes, int max_batch, int workers, mc_se
   s->batch_work = int64_t(1) << 23;
   if (const char *env = std::getenv("MERCURY_SERVE_BATCH_WORK"))
     s->batch_work = std::max<int64_t>(1, std::atoll(env));
+  s->num_workers = workers;
   for (int i = 0; i < workers; ++i) s->workers.emplace_back(mc::worker_main, s);
   *out = s;
   return MC_OK;
@@ -456,6 +466,7 @@ int mc_server_submit(mc_server_t *s, const int64_t *rowptr, const int32_t *col, 
     }
     r->ticket = s->next_ticket++;
     s->tickets[r->ticket] = r;
+    s->pending_work += mc::work_of(*r);
     s->pending.push_back(r);
     ++s->stats.submitted;
     *ticket = r->ticket;
