@@ -1434,7 +1434,8 @@ __global__ void __launch_bounds__(kPatThreads) center_kernel(CenterArgs a) {
 // One CTA per (center v0, chunk of kHubEdgeChunk of its edges), persistent
 // over an atomic queue.  The CTA marks N0 = N(v0) in its own bitmap over the
 // vertex ids (global memory, n bits, cleared again after the task), so that
-// "x in N0" is one bit read.  Chunk 0 also adds v0's star term.  With
+// "x in N0" is one bit read.  Chunk c also adds the star terms of positions
+// [256c, 256c + 256) of N0.  With
 // positions in N0 equal to id order (N0 is sorted):
 //   star  (P1_frequency_count, pattern_kernels.cuh:68-133): for x = N0[i],
 //         lo / hi = neighbours of x in N0 below / above x;
@@ -1520,8 +1521,9 @@ __global__ void __launch_bounds__(kPatThreads) hub_p1_kernel(HubP1Args a) {
       atomicOr(bits + (y >> 5), 1u << (y & 31));
     }
     __syncthreads();
-    if (chunk == 0) {  // the star term of v0
-      for (int i = warp; i < d0; i += kWarps) {
+    {  // the star term of v0 over this chunk's positions (balanced with the edges)
+      const int i_end = min(d0, (chunk + 1) * kHubEdgeChunk);
+      for (int i = chunk * kHubEdgeChunk + warp; i < i_end; i += kWarps) {
         const int x = __ldg(n0 + i);
         const int64_t bx = __ldg(a.rp + x), ex = __ldg(a.rp + x + 1);
         int lo = 0, hi = 0;
