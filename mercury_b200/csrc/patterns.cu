@@ -1464,6 +1464,7 @@ struct HubP1Args {
   const unsigned long long *deadline = nullptr;
   unsigned long long *stop_flag = nullptr;
   int64_t task_begin = 0, task_end = -1;  // slice of the queue positions
+  int lane_scan = 64;  // ranges up to this many entries are scanned by one lane
 };
 
 __device__ __forceinline__ int warp_sum_int(int v) {
@@ -1561,7 +1562,7 @@ __global__ void __launch_bounds__(kPatThreads) hub_p1_kernel(HubP1Args a) {
       // shorter of N(v2) and N0 within (v2, v1).  Lane t takes B[t], B[t + 32],
       // ... and scans a short range itself; ranges above kLaneScan entries
       // are scanned by the whole warp, one after the other.
-      constexpr int kLaneScan = 64;
+      const int kLaneScan = a.lane_scan;
       long long c2 = 0;
       for (int base = 0; base < nb; base += kWarp) {
         const int tb = base + lane;
@@ -2084,6 +2085,9 @@ int center_path(mc_dgraph *g, int pattern, PatArgs a, int grid, Slicer *sl) {
     HubP1Args ha{g->rowptr, g->col, n, chunk_off, static_cast<unsigned *>(g->hub_bits),
                  a.scratch, a.cap, g->counters + 3, g->counters, a.shard, a.num_shards,
                  a.deadline, a.stop_flag};
+    // MERCURY_HUB_LANE_SCAN: longest range one lane scans alone (0: every
+    // range by the whole warp).
+    if (const char *env = std::getenv("MERCURY_HUB_LANE_SCAN")) ha.lane_scan = std::max(0, std::atoi(env));
     const int64_t ntasks = total_chunks > a.shard
                                ? (total_chunks - a.shard + a.num_shards - 1) / a.num_shards
                                : 0;

@@ -260,8 +260,8 @@ def test_center_route_two_hop_rows_equal_per_edge_rows(monkeypatch, make, words)
         assert hop == [orc.pattern(g.rowptr, g.col, k) for k in outer]
 
 
-@pytest.mark.parametrize("hub", ["1", "0"])
-def test_p1_large_centers_by_bitmap_tasks(monkeypatch, hub):
+@pytest.mark.parametrize("hub,lane_scan", [("1", "64"), ("1", "0"), ("1", "100000"), ("0", "64")])
+def test_p1_large_centers_by_bitmap_tasks(monkeypatch, hub, lane_scan):
     """P1 on centers above degree 1,024: one CTA per (center, 256 edges)
     with the center's neighbourhood as an id bitmap (MERCURY_HUB_P1=1, the
     default) or the warp-per-edge kernel (=0); both give the oracle's counts,
@@ -272,6 +272,7 @@ def test_p1_large_centers_by_bitmap_tasks(monkeypatch, hub):
     with open(os.path.join(GOLDEN, "hub_counts.json")) as f:
         hub_want = json.load(f)["counts"]["P1"]
     monkeypatch.setenv("MERCURY_HUB_P1", hub)
+    monkeypatch.setenv("MERCURY_HUB_LANE_SCAN", lane_scan)
     rp, col = hub_graph()
     with DeviceGraph(rp, col) as d:
         assert d.pattern_count(1) == hub_want
