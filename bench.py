@@ -55,6 +55,8 @@ def parse_args():
     p.add_argument("--host-columns", action="store_true",
                    help="TC mode: keep the column array in host memory (the placement the "
                         "library picks for graphs larger than the device)")
+    p.add_argument("--host-dag", action="store_true",
+                   help="TC mode: keep the columns and the DAG in host memory (MC_HOST_DAG)")
     p.add_argument("--mode", choices=["tc", "batch", "serve", "patterns", "build"], default="tc",
                    help="tc: plain triangle count (the headline); batch: batched graphs/s; "
                         "serve: Poisson request stream, p50/p99 latency; patterns: P1..P8 "
@@ -89,9 +91,12 @@ def workload_config(a):
         "scale": a.scale, "edge_factor": a.edge_factor, "seed": a.seed,
         "l2": "no flush: inputs larger than L2 (symmetric CSR > 126 MB per step)",
     }
-    if getattr(a, "host_columns", False):
+    if getattr(a, "host_columns", False) or getattr(a, "host_dag", False):
         cfg["workload"] += ", column array in pinned host memory read through the device mapping"
         cfg["columns"] = "host"
+    if getattr(a, "host_dag", False):
+        cfg["workload"] += ", DAG in pinned host memory as well"
+        cfg["dag"] = "host"
     return cfg
 
 
@@ -179,7 +184,8 @@ def hub_profile(a):
     written, warp instructions issued and the launch's duration, as the
     committed summary records them ("key = value" lines).  None for any other
     workload: traffic is not carried over from one graph to another."""
-    if (a.scale, a.edge_factor, a.seed) != (22, 16, 1) or getattr(a, "host_columns", False):
+    if ((a.scale, a.edge_factor, a.seed) != (22, 16, 1) or getattr(a, "host_columns", False)
+            or getattr(a, "host_dag", False)):
         return None
     if not os.path.exists(HUB_DRAM_PROFILE):
         return None
@@ -410,10 +416,10 @@ def run_ours(a, rank, world, local_rank):
     g = Graph.rmat(a.scale, a.edge_factor, seed=a.seed)
     n, nnz = g.n, g.nnz
     m = nnz // 2
-    if a.host_columns:
-        # The one-shot call below then takes the host-column placement too.
-        os.environ["MERCURY_DEVICE_BYTES"] = "1"
-    dg = DeviceGraph(g, host_columns=a.host_columns)
+    if a.host_columns or a.host_dag:
+        # The one-shot call below then takes the same host placement.
+        os.environ["MERCURY_PLACEMENT"] = "dag" if a.host_dag else "columns"
+    dg = DeviceGraph(g, host_columns=a.host_columns, host_dag=a.host_dag)
     stream = torch.cuda.ExternalStream(dg.stream)
 
     def step():

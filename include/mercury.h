@@ -49,6 +49,16 @@ extern "C" {
  * (include/graph_gpu.h:102-119).  Every pass over the columns then runs at
  * the host link's bandwidth instead of HBM's. */
 #define MC_HOST_COLUMNS 0x2u
+/* mc_dgraph_create* flag: keep the degree-ordered DAG (its entries and their
+ * ranks) in pinned host memory as well, read by the counting kernels through
+ * the device's mapping; implies MC_HOST_COLUMNS.  Chosen by itself when the
+ * device cannot hold the DAG next to the per-vertex arrays even with the
+ * columns on the host.  Only O(n) arrays (offsets, degrees, ranks, partner
+ * records, task lists) and the core bitmaps stay in device memory: the
+ * whole-CSR counterpart of the reference's unified-memory fallback
+ * (include/graph_gpu.h:100-119).  Counting then reads partner lists across
+ * the host link. */
+#define MC_HOST_DAG 0x4u
 
 /* Opaque handles. */
 typedef struct mc_graph mc_graph_t;   /* host CSR (loaded or generated)      */
@@ -224,6 +234,9 @@ int mc_dgraph_export_csr(const mc_dgraph_t *g, int64_t *rowptr_out,
 /* *on_host = 1 when the handle's columns are in host memory
  * (MC_HOST_COLUMNS, asked for or chosen), else 0. */
 int mc_dgraph_columns_on_host(const mc_dgraph_t *g, int *on_host);
+/* *on_host = 1 if the handle keeps its DAG in host memory (MC_HOST_DAG,
+ * asked for or chosen), else 0. */
+int mc_dgraph_dag_on_host(const mc_dgraph_t *g, int *on_host);
 void mc_dgraph_free(mc_dgraph_t *g);
 
 /* Triangle count.  Replaces TCSolver(Graph&, uint64_t&) (tc_challenge.cu:11,

@@ -26,6 +26,7 @@ MC_ERR_TIMEOUT = -10
 
 MC_VALIDATE_SYMMETRY = 0x1
 MC_HOST_COLUMNS = 0x2
+MC_HOST_DAG = 0x4
 MC_BUILD_DEVICE_INPUT = 0x100
 
 MC_EDGES_MTX = 1
@@ -112,6 +113,7 @@ SIGNATURES = {
     "mc_dgraph_info": (C.c_int, [_P, _PI64, _PI64, _PI64]),
     "mc_dgraph_export_csr": (C.c_int, [_P, _P, _P]),
     "mc_dgraph_columns_on_host": (C.c_int, [_P, C.POINTER(C.c_int)]),
+    "mc_dgraph_dag_on_host": (C.c_int, [_P, C.POINTER(C.c_int)]),
     "mc_dgraph_free": (None, [_P]),
     "mc_tc_count": (C.c_int, [_P, _PU64, C.POINTER(Timing)]),
     "mc_tc_count_shard": (C.c_int, [_P, C.c_int, C.c_int, _PU64, C.POINTER(Timing)]),

@@ -34,12 +34,17 @@ void release(mc_dgraph *g) {
                   g->center_scratch, g->stage, g->chunk_offsets, g->core_bits, g->pinfo,
                   g->hop_scratch, g->hub_bits, g->vlabels, g->tile_rows};
   if (g->col_host) bufs[1] = nullptr;  // pinned host memory, freed below
+  if (g->dag_host)  // DAG entries and ranks: pinned host memory, freed below
+    for (void *&p : bufs)
+      if (p == g->dag_col || p == g->dag_rank) p = nullptr;
   // Stream-ordered frees: no device-wide synchronisation, so other handles'
   // work keeps running while this one is released.
   for (void *p : bufs)
     if (p) dev_free(p, g->stream);
   if (g->stream) cudaStreamSynchronize(g->stream);
   if (g->col_host && g->col_h) cudaFreeHost(g->col_h);
+  if (g->dag_col_h) cudaFreeHost(g->dag_col_h);
+  if (g->dag_rank_h) cudaFreeHost(g->dag_rank_h);
   delete[] g->h_counters;
   for (cudaEvent_t e : g->ev)
     if (e) cudaEventDestroy(e);
@@ -80,14 +85,32 @@ int device_bytes_available(int device, int64_t *avail) {
 // kernels read through the device's mapping of it.
 constexpr int64_t kPlacementMargin = 256ll << 20;
 constexpr unsigned kDeviceColumns = 0x80000000u;  // internal: skip the decision
-int columns_on_host(int device, int64_t n, int64_t nnz, unsigned flags, bool *host) {
-  *host = (flags & MC_HOST_COLUMNS) != 0;
-  if (*host || nnz == 0 || (flags & kDeviceColumns)) return MC_OK;
+// The DAG goes to host memory too (dag_host) when asked, or when the device
+// cannot hold it even with the columns on the host.
+int columns_on_host(int device, int64_t n, int64_t nnz, unsigned flags, bool *host,
+                    bool *dag_host = nullptr) {
+  const bool want_dag = (flags & MC_HOST_DAG) != 0;
+  *host = want_dag || (flags & MC_HOST_COLUMNS) != 0;
+  if (dag_host) *dag_host = want_dag;
+  if (want_dag || nnz == 0 || (flags & kDeviceColumns)) return MC_OK;
+  // MERCURY_PLACEMENT=columns / dag forces the automatic choice (benchmarks
+  // of the host placements use it).
+  if (const char *env = std::getenv("MERCURY_PLACEMENT")) {
+    if (std::strcmp(env, "columns") == 0 || std::strcmp(env, "dag") == 0) {
+      *host = true;
+      if (dag_host) *dag_host = std::strcmp(env, "dag") == 0;
+      return MC_OK;
+    }
+  }
   int64_t avail = 0;
   const int rc = device_bytes_available(device, &avail);
   if (rc != MC_OK) return rc;
   const int64_t in_core = 8 * (n + 1) + 4 * nnz + tc_device_bytes(n, nnz, false);
-  *host = in_core + kPlacementMargin > avail;
+  if (!*host) *host = in_core + kPlacementMargin > avail;
+  if (*host && dag_host) {
+    const int64_t with_dag = 8 * (n + 1) + tc_device_bytes(n, nnz, true, false);
+    *dag_host = with_dag + kPlacementMargin > avail;
+  }
   return MC_OK;
 }
 
@@ -124,7 +147,7 @@ int create_common(int64_t n, int64_t nnz, void *stream, mc_dgraph **out, mc_dgra
   g->n = n;
   g->nnz = nnz;
   MC_CUDA_TRY(dev_alloc((void **)&g->rowptr, sizeof(int64_t) * (size_t)(n + 1), g->stream));
-  const int rc = columns_on_host(g->device, n, nnz, flags, &g->col_host);
+  const int rc = columns_on_host(g->device, n, nnz, flags, &g->col_host, &g->dag_host);
   if (rc != MC_OK) return rc;
   const size_t col_bytes = sizeof(int32_t) * (size_t)std::max<int64_t>(nnz, 1);
   if (g->col_host) {
@@ -384,6 +407,12 @@ int mc_dgraph_export_csr(const mc_dgraph_t *g, int64_t *rowptr_out, int32_t *col
   return MC_OK;
 }
 
+int mc_dgraph_dag_on_host(const mc_dgraph_t *g, int *on_host) {
+  if (!g || !on_host) return MC_ERR_ARG;
+  *on_host = g->dag_host ? 1 : 0;
+  return MC_OK;
+}
+
 int mc_dgraph_columns_on_host(const mc_dgraph_t *g, int *on_host) {
   if (!g || !on_host) return MC_ERR_ARG;
   *on_host = g->col_host ? 1 : 0;
@@ -523,11 +552,11 @@ int mc_tc_count_host(const int64_t *rowptr, const int32_t *col, int64_t n, int64
   // A graph the device cannot hold is counted with its columns in host
   // memory. A cached handle of that kind is kept only while the graphs
   // still need it.
-  bool host = false;
+  bool host = false, dag_host = false;
   if (!c.g || c.g->col_host) {
-    const int prc = mc::columns_on_host(dev, n, nnz, 0, &host);
+    const int prc = mc::columns_on_host(dev, n, nnz, 0, &host, &dag_host);
     if (prc != MC_OK) return prc;
-    if (c.g && !host) {
+    if (c.g && (!host || c.g->dag_host != dag_host)) {
       release(c.g);
       c.g = nullptr;
     }
@@ -536,7 +565,8 @@ int mc_tc_count_host(const int64_t *rowptr, const int32_t *col, int64_t n, int64
     mc_dgraph *g = nullptr;
     mc_dgraph *tmp = nullptr;
     int rc = mc::create_common(n, nnz, nullptr, &tmp, &g,
-                               host ? MC_HOST_COLUMNS : mc::kDeviceColumns);
+                               dag_host ? MC_HOST_DAG
+                                        : (host ? MC_HOST_COLUMNS : mc::kDeviceColumns));
     if (rc != MC_OK) {
       release(g);
       return rc;

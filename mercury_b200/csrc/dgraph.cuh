@@ -66,6 +66,8 @@ struct mc_dgraph {
   // memory mapped into the device's address space (graphs whose columns do
   // not fit the device; every kernel reads them over the host link).
   bool col_host = false;
+  bool dag_host = false;      // DAG entries and ranks in pinned mapped host memory
+  int32_t *dag_col_h = nullptr, *dag_rank_h = nullptr;  // their host views
   int32_t *col_h = nullptr;   // host view of col when col_host
 
   // ---- pattern-count scratch (frontier lists), grown on demand ----------
@@ -149,7 +151,7 @@ int validate_graph(mc_dgraph *g, unsigned flags);
 int tc_alloc(mc_dgraph *g);
 // Device bytes tc_alloc takes for a single graph of n vertices and nnz
 // entries (the DAG at half the entries when the columns are on the host).
-int64_t tc_device_bytes(int64_t n, int64_t nnz, bool col_host);
+int64_t tc_device_bytes(int64_t n, int64_t nnz, bool col_host, bool dag_host = false);
 // upload (host memory, nnz entries): the column array is copied into the
 // handle in chunks during the passes, each chunk checked against the CSR
 // contract first (the row offsets must have been checked: validate_rowptr).

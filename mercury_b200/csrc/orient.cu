@@ -601,7 +601,7 @@ int core_rank_count(int64_t n) {
   return (int)std::min<int64_t>(k, n);
 }
 
-int64_t tc_device_bytes(int64_t n, int64_t nnz, bool col_host) {
+int64_t tc_device_bytes(int64_t n, int64_t nnz, bool col_host, bool dag_host) {
   const int64_t cap = std::max<int64_t>(nnz, 1);
   const int64_t tiles = std::max<int64_t>((nnz + kTileEdges - 1) / kTileEdges, 1);
   const int64_t tasks = n + cap / std::min(kHubChunk, kLeafChunk) + 1;
@@ -610,7 +610,8 @@ int64_t tc_device_bytes(int64_t n, int64_t nnz, bool col_host) {
   const int64_t staging =
       col_host ? 2 * 4 * stage_capacity(nnz) + 8 * (stage_capacity(nnz) / kTileEdges + 1) : 0;
   return (n + 1) * (8 + 16 + 8 + 3 * 4 + 3 * 8 + 4 + 16) + 3 * 8 * tasks +
-         2 * 4 * (dag_capacity(nnz, col_host) + 4) + tiles * (2 * kTileThreads + 28) +
+         (dag_host ? 0 : 2 * 4 * (dag_capacity(nnz, col_host) + 4)) +
+         tiles * (2 * kTileThreads + 28) +
          2 * 12 * (radix_entries(n) + 1) + scan + staging + 4 * core_offset(core_rank_count(n));
 }
 
@@ -630,7 +631,16 @@ int tc_alloc(mc_dgraph *g) {
   MC_ALLOC(g->pinfo, n + 1);
   MC_ALLOC(g->dag_rowptr, n + 1);
   // 4 entries of padding: the staged hub kernel copies whole 16-byte groups.
-  MC_ALLOC(g->dag_col, g->dag_cap + 4);
+  // With the DAG on the host, its entries and ranks live in pinned memory
+  // that the kernels reach through the device's mapping.
+  auto dag_alloc = [&](int32_t **dev, int32_t **host) -> cudaError_t {
+    if (!g->dag_host) return dev_alloc((void **)dev, sizeof(int32_t) * (size_t)(g->dag_cap + 4), g->stream);
+    cudaError_t e = cudaHostAlloc((void **)host, sizeof(int32_t) * (size_t)(g->dag_cap + 4),
+                                  cudaHostAllocMapped);
+    if (e != cudaSuccess) return e;
+    return cudaHostGetDevicePointer((void **)dev, *host, 0);
+  };
+  MC_CUDA_TRY(dag_alloc(&g->dag_col, &g->dag_col_h));
   MC_ALLOC(g->keep, tiles * kTileThreads);
   MC_ALLOC(g->tile_counts, tiles);
   MC_ALLOC(g->tile_offsets, tiles + 1);
@@ -646,7 +656,7 @@ int tc_alloc(mc_dgraph *g) {
   MC_ALLOC(g->mega_tasks, g->task_capacity);
   if (ranked) {
     MC_ALLOC(g->rank, n + 1);
-    MC_ALLOC(g->dag_rank, g->dag_cap + 4);
+    MC_CUDA_TRY(dag_alloc(&g->dag_rank, &g->dag_rank_h));
     MC_ALLOC(g->rank_keys, 2 * n + 2);
     MC_ALLOC(g->rank_counts, radix_entries(n) + 1);
     MC_ALLOC(g->rank_offsets, radix_entries(n) + 1);
@@ -672,6 +682,17 @@ int tc_alloc(mc_dgraph *g) {
   return MC_OK;
 }
 
+// Host copy of count entries by all host threads, in 1 MB pieces.
+static void parallel_copy(int32_t *dst, const int32_t *src, int64_t count) {
+  constexpr int64_t kPiece = 1 << 18;
+  const int64_t pieces = (count + kPiece - 1) / kPiece;
+#pragma omp parallel for schedule(static)
+  for (int64_t p = 0; p < pieces; ++p) {
+    const int64_t a = p * kPiece, b = std::min(count, a + kPiece);
+    std::memcpy(dst + a, src + a, sizeof(int32_t) * (size_t)(b - a));
+  }
+}
+
 // Passes A and B over a column array that crosses from host memory in
 // chunks of whole tiles, copied by DMA on a copy stream while the passes run
 // on the previous chunk.  Each chunk runs A, the scan of its tile counts on
@@ -685,17 +706,6 @@ int tc_alloc(mc_dgraph *g) {
 // The DAG holds dag_cap entries; a chunk that would end past it raises
 // kErrDagCapacity and writes nothing.  The caller reads the flags before
 // counting.
-// Host copy of count entries by all host threads, in 1 MB pieces.
-static void parallel_copy(int32_t *dst, const int32_t *src, int64_t count) {
-  constexpr int64_t kPiece = 1 << 18;
-  const int64_t pieces = (count + kPiece - 1) / kPiece;
-#pragma omp parallel for schedule(static)
-  for (int64_t p = 0; p < pieces; ++p) {
-    const int64_t a = p * kPiece, b = std::min(count, a + kPiece);
-    std::memcpy(dst + a, src + a, sizeof(int32_t) * (size_t)(b - a));
-  }
-}
-
 static int staged_dag_passes(mc_dgraph *g, const int32_t *deg, const int32_t *src, bool in_place) {
   const int64_t n = g->n, nnz = g->nnz;
   cudaStream_t s = g->stream, cs = g->copy_stream;

@@ -863,7 +863,8 @@ int tc_count_launch(mc_dgraph *g, cudaEvent_t after_hub, int shard, int num_shar
   // MERCURY_TC_TMA=1: long partner lists staged by bulk copies (the table's
   // shared memory is followed by 16 KB of copy slots).
   const char *tma_env = std::getenv("MERCURY_TC_TMA");
-  const bool staged = tma_env && std::atoi(tma_env) != 0;
+  // (Lists in host memory, MC_HOST_DAG, always take the lane loads.)
+  const bool staged = tma_env && std::atoi(tma_env) != 0 && !g->dag_host;
   auto kern = staged ? tc_hub_kernel<true> : tc_hub_kernel<false>;
   const size_t extra = staged ? kStageBytes : 0;
   MC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,

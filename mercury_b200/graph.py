@@ -138,10 +138,13 @@ class DeviceGraph:
     """Device-resident symmetric CSR (``mc_dgraph_t``) on the current GPU."""
 
     def __init__(self, rowptr, col=None, *, stream: Optional[int] = None,
-                 validate_symmetry: bool = False, host_columns: bool = False):
+                 validate_symmetry: bool = False, host_columns: bool = False,
+                 host_dag: bool = False):
         """host_columns=True keeps the column array in pinned host memory that
         the kernels read through the device's mapping (MC_HOST_COLUMNS); the
-        library also chooses it when the device cannot hold the graph."""
+        library also chooses it when the device cannot hold the graph.
+        host_dag=True keeps the degree-ordered DAG there as well
+        (MC_HOST_DAG), chosen by itself when even that does not fit."""
         if isinstance(rowptr, Graph):
             g = rowptr
             rowptr, col = g.rowptr, g.col
@@ -152,6 +155,8 @@ class DeviceGraph:
         flags = _ffi.MC_VALIDATE_SYMMETRY if validate_symmetry else 0
         if host_columns:
             flags |= _ffi.MC_HOST_COLUMNS
+        if host_dag:
+            flags |= _ffi.MC_HOST_DAG
         check(lib().mc_dgraph_create(rowptr.ctypes.data, col.ctypes.data if self.nnz else None,
                                      self.n, self.nnz, stream, flags, C.byref(self._h)),
               "uploading the graph")
@@ -196,6 +201,13 @@ class DeviceGraph:
         chosen because the device could not hold the graph)."""
         v = C.c_int()
         check(lib().mc_dgraph_columns_on_host(self._h, C.byref(v)), "column placement")
+        return bool(v.value)
+
+    @property
+    def dag_on_host(self) -> bool:
+        """True when the DAG lives in host memory (MC_HOST_DAG, asked for or chosen)."""
+        v = C.c_int()
+        check(lib().mc_dgraph_dag_on_host(self._h, C.byref(v)), "DAG placement")
         return bool(v.value)
 
     @property

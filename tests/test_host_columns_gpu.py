@@ -146,3 +146,41 @@ def test_asymmetric_rows_are_refused_before_the_dag_is_written():
                 assert ex.value.status == MC_ERR_FORMAT
         finally:
             os.environ.pop("MERCURY_STAGE_EDGES", None)
+
+
+@pytest.mark.parametrize("name", sorted(GOLD))
+def test_golden_counts_with_the_dag_on_the_host(name):
+    """MC_HOST_DAG: the columns and the DAG (entries and ranks) in pinned host
+    memory, the counting kernels reading partner lists through the mapping."""
+    g = fixture(name)
+    with DeviceGraph(g, host_dag=True) as d:
+        assert d.columns_on_host and d.dag_on_host
+        assert d.tc_count() == GOLD[name]["TC"]
+        assert d.tc_count() == GOLD[name]["TC"]
+
+
+@pytest.mark.parametrize("make", [lambda: Graph.rmat(14, 16, seed=61),
+                                  lambda: Graph.chung_lu(50000, 2.1, 16.0, 5000.0, seed=62)])
+def test_host_dag_equals_device_dag(make):
+    g = make()
+    with DeviceGraph(g) as d:
+        want = d.tc_count()
+        drp, dcol = d.export_dag()
+        parts = [d.tc_count_shard(s, 3) for s in range(3)]
+    with DeviceGraph(g, host_dag=True) as h:
+        assert h.tc_count() == want == orc.tc(g.rowptr, g.col)
+        hrp, hcol = h.export_dag()
+        assert np.array_equal(drp, hrp) and np.array_equal(dcol, hcol)
+        assert [h.tc_count_shard(s, 3) for s in range(3)] == parts
+
+
+def test_placement_moves_the_dag_to_the_host_when_the_device_is_too_small(monkeypatch):
+    """With a device figure below the host-column footprint the library puts
+    the DAG on the host too, by itself (one-shot call and handle)."""
+    g = Graph.rmat(13, 16, seed=63)
+    want = orc.tc(g.rowptr, g.col)
+    monkeypatch.setenv("MERCURY_DEVICE_BYTES", "1")
+    with DeviceGraph(g) as d:
+        assert d.columns_on_host and d.dag_on_host
+        assert d.tc_count() == want
+    assert tc_count_host(np.asarray(g.rowptr), np.asarray(g.col)) == want
