@@ -265,14 +265,20 @@ uint64_t orc_pattern(int64_t n, const int64_t *rowptr, const int32_t *col, int p
     V A, B, C, D, E;
     std::vector<int64_t> freq;
     Acc acc;
+    // Threads share out single directed edges, not vertices: the hubs of a
+    // power-law graph hold most of the work (the sums wrap mod 2^64, so the
+    // order of the additions does not change the result).
+    if (pattern == 1) {
 #pragma omp for schedule(dynamic, 16)
-    for (int64_t v0 = 0; v0 < n; ++v0) {
-      if (pattern == 1) acc.c1 += p1_star(g, (int32_t)v0, freq);
-      for (int64_t e = rowptr[v0]; e < rowptr[v0 + 1]; ++e) {
-        const int32_t v1 = col[e];
-        if (v1 == v0) continue;  // init_edgelist skips self-loops
-        edge_pattern(g, pattern, (int32_t)v0, v1, acc, A, B, C, D, E, freq);
-      }
+      for (int64_t v0 = 0; v0 < n; ++v0) acc.c1 += p1_star(g, (int32_t)v0, freq);
+    }
+    const int64_t nnz = rowptr[n];
+#pragma omp for schedule(dynamic, 4)
+    for (int64_t e = 0; e < nnz; ++e) {
+      const int64_t v0 = std::upper_bound(rowptr, rowptr + n + 1, e) - rowptr - 1;
+      const int32_t v1 = col[e];
+      if (v1 == v0) continue;  // init_edgelist skips self-loops
+      edge_pattern(g, pattern, (int32_t)v0, v1, acc, A, B, C, D, E, freq);
     }
     c1 += acc.c1;
     c2 += acc.c2;

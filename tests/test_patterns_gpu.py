@@ -237,6 +237,31 @@ def test_pattern_bench_graph_counts_equal_committed_oracle():
             assert d.pattern_count(k) == rec["counts"][f"P{k}"], k
 
 
+@pytest.mark.parametrize("route", ["default", "centers", "edge"])
+def test_survey_shape_graph_with_hubs_counts_equal_committed_oracle(monkeypatch, route):
+    """The survey's pattern graph shape (Chung-Lu gamma 2.1, mean 20, weight
+    cap 50,000) at 5,000 vertices, small enough for the literal oracle:
+    hubs of degree 2,187, 1,525 and 1,173 (above the 1,024 limit of the
+    bitmap kernels, P1's hub tasks included). All eight counts equal the
+    oracle's, committed by tests/golden/make_pattern_golden.py, on every
+    route and in sliced launches."""
+    with open(os.path.join(GOLDEN, "pattern_counts.json")) as f:
+        rec = json.load(f)["chung_lu_n5000_mean20_cap50000_seed1"]
+    g = Graph.chung_lu(5000, 2.1, 20.0, 50000.0, seed=1)
+    assert g.nnz // 2 == rec["m"]
+    deg = np.diff(np.asarray(g.rowptr))
+    assert int(deg.max()) == rec["max_degree"] and int((deg > 1024).sum()) == 3
+    if route != "default":
+        monkeypatch.setenv("MERCURY_PATTERN_KERNEL", route)
+    with DeviceGraph(g) as d:
+        for k in range(1, 9):
+            assert d.pattern_count(k) == rec["counts"][f"P{k}"], k
+        monkeypatch.setenv("MERCURY_PATTERN_SLICE", "1")
+        monkeypatch.setenv("MERCURY_PATTERN_SLICE_MS", "0.2")  # many small slices
+        for k in (1, 2, 5, 8):
+            assert d.pattern_count(k) == rec["counts"][f"P{k}"], ("sliced", k)
+
+
 @pytest.mark.parametrize("words", [None, "2048"])
 @pytest.mark.parametrize("make", [lambda: Graph.chung_lu(30000, 2.1, 12.0, 900.0, seed=7),
                                   lambda: Graph.rmat(10, 16, seed=5)])
