@@ -140,17 +140,30 @@ __device__ __forceinline__ int block_exclusive_int(int v, int *total) {
 // Writes the kept entries of this thread's span [s, e_end) (row r holds s)
 // from position pos on, and out_rowptr[q] = position for every row q that
 // starts inside the span.  Rows starting at nnz are written by the caller.
+// kStage: the entries go to stage[pos - stage_base] in shared memory (the
+// caller copies the tile's range out, coalesced, and gathers the ranks
+// there); otherwise straight to out_col / out_rank.
+template <bool kStage>
 __device__ __forceinline__ void write_span(const TileRows &tr, const int64_t *rowptr, int64_t t0,
                                            int64_t s, int64_t e_end, int64_t r,
                                            const int32_t (&vals)[kEdgesPerThread], unsigned keep,
                                            int64_t pos, int64_t *out_rowptr, int32_t *out_col,
-                                           const int32_t *__restrict__ rank, int32_t *out_rank) {
+                                           const int32_t *__restrict__ rank, int32_t *out_rank,
+                                           int32_t *stage, int64_t stage_base) {
   if (tr.at(r) == s) {
     // Rows starting exactly at s: row r and the empty rows just before it.
     // For s > t0 they all lie in the staged range; the tile's first span may
     // share its start with rows before the range.
     const int64_t rf = s == t0 ? lower_row(rowptr, 0, r, s) : tr.first_at(tr.lo, r, s);
     for (int64_t q = rf; q <= r; ++q) out_rowptr[q] = pos;
+  }
+  // The ranks of the kept entries, gathered before the row walk so that
+  // they are all in flight at once.
+  int32_t ranks[kEdgesPerThread];
+  if (!kStage) {
+#pragma unroll
+    for (int k = 0; k < kEdgesPerThread; ++k)
+      ranks[k] = out_rank && (keep & (1u << k)) ? __ldg(rank + vals[k]) : 0;
   }
   int64_t next = tr.at(r + 1);
 #pragma unroll
@@ -163,8 +176,12 @@ __device__ __forceinline__ void write_span(const TileRows &tr, const int64_t *ro
         next = tr.at(r + 1);
       }
       if (keep & (1u << k)) {
-        out_col[pos] = vals[k];
-        if (out_rank) out_rank[pos] = __ldg(rank + vals[k]);
+        if (kStage) {
+          stage[pos - stage_base] = vals[k];
+        } else {
+          out_col[pos] = vals[k];
+          if (out_rank) out_rank[pos] = ranks[k];
+        }
         ++pos;
       }
     }
@@ -188,7 +205,7 @@ struct ColumnChunk {
 // chunk_end given, pass B writes nothing when *chunk_end (the DAG entries
 // up to the end of this chunk) exceeds cap; with stop given, neither pass
 // does anything once a contract bit is set there.
-template <bool kWrite>
+template <bool kWrite, bool kStage = false>
 __global__ void __launch_bounds__(kTileThreads)
     dag_pass_kernel(const int64_t *__restrict__ rowptr, ColumnChunk cc,
                     const int32_t *__restrict__ deg, int64_t n, int64_t nnz, int2 *key,
@@ -218,6 +235,12 @@ __global__ void __launch_bounds__(kTileThreads)
     load_span(cc.col + (s - cc.col_base), nnz - s, vals);
     r = tr.row_of(s);
     if (!kWrite) {
+      // All sixteen degree gathers are issued before the row walk below
+      // (whose loop would otherwise serialise them); entries past the span
+      // hold id 0, a valid vertex.
+      int du[kEdgesPerThread];
+#pragma unroll
+      for (int k = 0; k < kEdgesPerThread; ++k) du[k] = __ldg(deg + vals[k]);
       int64_t v = r, next = tr.at(r + 1);
       int dv = __ldg(deg + v);
       int run = 0;  // DAG entries of row v seen in this span
@@ -235,8 +258,7 @@ __global__ void __launch_bounds__(kTileThreads)
             dv = __ldg(deg + v);
           }
           const int u = vals[k];
-          const int du = __ldg(deg + u);
-          if (du > dv || (du == dv && u > (int)v)) {
+          if (du[k] > dv || (du[k] == dv && u > (int)v)) {
             keep |= 1u << k;
             ++run;
           }
@@ -256,8 +278,25 @@ __global__ void __launch_bounds__(kTileThreads)
   int total = 0;
   const int64_t base = offs_in[tile];
   const int64_t pos = base + block_exclusive_int(__popc(keep), &total);
-  if (s < t1)
-    write_span(tr, rowptr, t0, s, e_end, r, vals, keep, pos, out_rowptr, out_col, rank, out_rank);
+  if (kStage) {
+    // The tile's DAG entries are the range [base, base + total): staged in
+    // shared memory, then written with whole-line stores, the rank gathers
+    // issued four per thread at a time.
+    __shared__ int32_t stage[kTileEdges];
+    if (s < t1)
+      write_span<true>(tr, rowptr, t0, s, e_end, r, vals, keep, pos, out_rowptr, nullptr,
+                       nullptr, nullptr, stage, base);
+    __syncthreads();
+#pragma unroll 4
+    for (int i = threadIdx.x; i < total; i += kTileThreads) {
+      const int32_t c = stage[i];
+      out_col[base + i] = c;
+      if (out_rank) out_rank[base + i] = __ldg(rank + c);
+    }
+  } else if (s < t1) {
+    write_span<false>(tr, rowptr, t0, s, e_end, r, vals, keep, pos, out_rowptr, out_col, rank,
+                      out_rank, nullptr, 0);
+  }
   // Rows after the last entry (trailing empty rows and q == n) start at nnz.
   if (t1 == nnz)
     for (int64_t q = tr.hi + 1 + threadIdx.x; q <= n; q += kTileThreads) out_rowptr[q] = base + total;
@@ -706,6 +745,14 @@ static void parallel_copy(int32_t *dst, const int32_t *src, int64_t count) {
 // The DAG holds dag_cap entries; a chunk that would end past it raises
 // kErrDagCapacity and writes nothing.  The caller reads the flags before
 // counting.
+// Pass B stages each tile's DAG entries in shared memory and writes them
+// out with whole-line stores (MERCURY_DAG_STAGE=0: each thread writes its
+// own kept entries directly).
+static bool stage_dag_writes() {
+  const char *env = std::getenv("MERCURY_DAG_STAGE");
+  return env ? std::atoi(env) != 0 : true;
+}
+
 static int staged_dag_passes(mc_dgraph *g, const int32_t *deg, const int32_t *src, bool in_place) {
   const int64_t n = g->n, nnz = g->nnz;
   cudaStream_t s = g->stream, cs = g->copy_stream;
@@ -764,7 +811,8 @@ static int staged_dag_passes(mc_dgraph *g, const int32_t *deg, const int32_t *sr
                                                                g->tile_offsets + tb, g->dag_cap,
                                                                g->err);
     MC_CUDA_TRY(cudaGetLastError());
-    dag_pass_kernel<true><<<(unsigned)ct, kTileThreads, 0, s>>>(
+    (stage_dag_writes() ? dag_pass_kernel<true, true> : dag_pass_kernel<true, false>)
+        <<<(unsigned)ct, kTileThreads, 0, s>>>(
         g->rowptr, cc, deg, n, nnz, g->key, g->keep, nullptr, g->tile_offsets, g->dag_rowptr,
         g->dag_col, g->rank, g->dag_rank, g->tile_offsets + tb + ct, g->dag_cap, stop,
         g->tile_rows);
@@ -826,7 +874,8 @@ int tc_orient(mc_dgraph *g, const int32_t *upload) {
         nullptr, nullptr, nullptr, 0, nullptr, g->tile_rows);
     MC_CUDA_TRY(cudaGetLastError());
     MC_CUDA_TRY(exclusive_scan(g->tile_counts, g->tile_offsets, tiles, g->scan_temp, s));
-    dag_pass_kernel<true><<<grid, kTileThreads, 0, s>>>(
+    (stage_dag_writes() ? dag_pass_kernel<true, true> : dag_pass_kernel<true, false>)
+        <<<grid, kTileThreads, 0, s>>>(
         g->rowptr, all, deg, n, nnz, g->key, g->keep, nullptr, g->tile_offsets, g->dag_rowptr,
         g->dag_col, g->batch.gid ? nullptr : g->rank, g->batch.gid ? nullptr : g->dag_rank,
         nullptr, 0, nullptr, g->tile_rows);

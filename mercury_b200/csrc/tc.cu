@@ -125,18 +125,17 @@ __device__ __forceinline__ bool cuckoo_insert(int *tab, int shift, int key) {
   return false;
 }
 
-// Membership in a bitmap over ranks [0, limit): an entry at or above the
-// owner's rank cannot be in N+(owner) and reads nothing.
-// The read is unconditional (an entry out of range reads word 0 and is
-// masked off), so a probe is straight-line code with no branch.
+// Membership in the owner's bitmap over ranks [0, R), by a clamped word
+// index and no range test: bits at or above R are never set, and word
+// `zero` (the first word of the quad cleared after the bitmap's own quads)
+// is all zero, so every rank at or above R -- kNoKey included -- reads a
+// zero bit.  The probe is straight-line code with no branch.
 struct BitmapProbe {
   const unsigned *bits;
-  unsigned limit;
+  unsigned zero;
   __device__ __forceinline__ unsigned operator()(int w) const {
-    const unsigned u = (unsigned)w;  // kNoKey (negative) is above every limit
-    const bool in = u < limit;
-    const unsigned c = in ? u : 0u;
-    return (bits[c >> 5] >> (c & 31)) & (unsigned)in;
+    const unsigned u = (unsigned)w;
+    return (bits[min(u >> 5, zero)] >> (u & 31)) & 1u;
   }
 };
 
@@ -618,7 +617,8 @@ __global__ void __launch_bounds__(kCountThreads, kStaged ? 4 : 5) tc_hub_kernel(
     // Clear the bitmap / table, then find the partners (their loads overlap).
     int4 *t4 = reinterpret_cast<int4 *>(table);
     if (bitmap) {
-      for (int i = threadIdx.x; i < (R + 127) >> 7; i += blockDim.x) t4[i] = make_int4(0, 0, 0, 0);
+      // The bitmap's quads and one more (the probe's zero word).
+      for (int i = threadIdx.x; i <= (R + 127) >> 7; i += blockDim.x) t4[i] = make_int4(0, 0, 0, 0);
     } else if (use_table) {
       for (int i = threadIdx.x; i < (1 << lg) / 4; i += blockDim.x) t4[i] = make_int4(-1, -1, -1, -1);
     }
@@ -663,7 +663,8 @@ __global__ void __launch_bounds__(kCountThreads, kStaged ? 4 : 5) tc_hub_kernel(
     if (bitmap)
       th = stream_partners<kStaged>(
           a.dag_rank, s_base, s_off, pt, &s_next, warp, lane,
-          BitmapProbe{reinterpret_cast<const unsigned *>(table), (unsigned)R}, sg,
+          BitmapProbe{reinterpret_cast<const unsigned *>(table), (unsigned)(((R + 127) >> 7) << 2)},
+          sg,
           reinterpret_cast<const unsigned *>(table), R, a.core);
     else if (use_table)
       th = stream_partners<kStaged>(a.dag_col, s_base, s_off, pt, &s_next, warp, lane,
@@ -873,7 +874,8 @@ int tc_count_launch(mc_dgraph *g, cudaEvent_t after_hub, int shard, int num_shar
   a.tasks = g->hub_tasks;
   a.ntasks = g->hub_off + g->n;
   a.queue = g->counters + 1;
-  a.bitmap_bits = (int)std::min<size_t>(small_smem * 8, (size_t)g->bitmap_bits_cap);
+  // (One quad of each bitmap's shared memory is the probe's zero word.)
+  a.bitmap_bits = (int)std::min<size_t>(small_smem * 8 - 128, (size_t)g->bitmap_bits_cap);
   a.stage_off = (int)(small_smem / sizeof(int));
   const int small_grid =
       g->num_sms * resident_blocks((const void *)kern, kCountThreads, small_smem + extra);
@@ -883,7 +885,7 @@ int tc_count_launch(mc_dgraph *g, cudaEvent_t after_hub, int shard, int num_shar
   a.tasks = g->mega_tasks;
   a.ntasks = g->mega_off + g->n;
   a.queue = g->counters + 6;
-  a.bitmap_bits = (int)std::min<size_t>(big_smem * 8, (size_t)g->bitmap_bits_cap);
+  a.bitmap_bits = (int)std::min<size_t>(big_smem * 8 - 128, (size_t)g->bitmap_bits_cap);
   a.stage_off = (int)(big_smem / sizeof(int));
   const int big_grid =
       g->num_sms * resident_blocks((const void *)kern, kCountThreads, big_smem + extra);

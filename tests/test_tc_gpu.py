@@ -32,8 +32,12 @@ def test_tc_matches_golden(name):
         assert d.tc_count() == GOLD[name]["TC"]  # second call on the same handle
 
 
+@pytest.mark.parametrize("stage", ["1", "0"])
 @pytest.mark.parametrize("name", ["rmat10", "cl3000", "dense400", "isolated"])
-def test_device_dag_equals_oracle_orientation(name):
+def test_device_dag_equals_oracle_orientation(name, stage, monkeypatch):
+    """Pass B with each tile's entries staged in shared memory (the default)
+    or written by each thread directly (MERCURY_DAG_STAGE=0)."""
+    monkeypatch.setenv("MERCURY_DAG_STAGE", stage)
     g = fixture(name)
     rp, col = np.array(g.rowptr), np.array(g.col)
     with DeviceGraph(g) as d:
@@ -55,6 +59,21 @@ def test_tc_rmat_vs_oracle(scale, ef, seed):
         st = d.tc_stats()
     assert got == orc.tc(g.rowptr, g.col)
     assert st["hub_tasks"] + st["leaf_tasks"] > 0
+
+
+def test_dag_write_forms_give_the_same_counts(monkeypatch):
+    """The hub kernel probes the DAG ranks that pass B writes: both pass-B
+    forms give the oracle's count on a graph with hub tasks, in core and
+    with host columns (chunked passes)."""
+    g = Graph.rmat(16, 16, seed=4)
+    want = orc.tc(g.rowptr, g.col)
+    for stage in ("0", "1"):
+        monkeypatch.setenv("MERCURY_DAG_STAGE", stage)
+        with DeviceGraph(g) as d:
+            assert d.tc_count() == want, stage
+            assert d.tc_stats()["hub_tasks"] > 0
+        with DeviceGraph(g, host_columns=True) as h:
+            assert h.tc_count() == want, stage
 
 
 @pytest.mark.parametrize("n,cap,seed", [(20000, 2000, 3), (200000, 50000, 1)])
