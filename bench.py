@@ -84,12 +84,27 @@ def parse_args():
     return p.parse_args()
 
 
-def workload_config(a):
+L2_BYTES = 126 * 2**20
+
+
+def l2_note(n=None, m=None):
+    """Whether the step's input (the symmetric CSR: 8(n+1) + 8m bytes) is
+    larger than the 126 MB L2, so that no flush is needed between steps."""
+    if n is None or m is None:
+        return "no flush: inputs larger than L2 (symmetric CSR > 126 MB per step)"
+    mb = (8 * (n + 1) + 8 * m) / 1e6
+    if 8 * (n + 1) + 8 * m > L2_BYTES:
+        return f"no flush: inputs larger than L2 (symmetric CSR {mb:.0f} MB per step)"
+    return (f"no flush: the symmetric CSR ({mb:.0f} MB) fits in L2, so steps after the "
+            f"first read it from L2 (a small case, not the benchmark workload)")
+
+
+def workload_config(a, n=None, m=None):
     cfg = {
         "workload": f"plain TC, RMAT scale {a.scale} edge factor {a.edge_factor} "
                     f"(0.57,0.19,0.19,0.05) seed {a.seed}, device orientation + count",
         "scale": a.scale, "edge_factor": a.edge_factor, "seed": a.seed,
-        "l2": "no flush: inputs larger than L2 (symmetric CSR > 126 MB per step)",
+        "l2": l2_note(n, m),
     }
     if getattr(a, "host_columns", False) or getattr(a, "host_dag", False):
         cfg["workload"] += ", column array in pinned host memory read through the device mapping"
@@ -101,7 +116,88 @@ def workload_config(a):
 
 
 # ---------------------------------------------------------------- clocks
-class ClockSampler:
+REASON_BITS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40),
+               ("sw_thermal_slowdown", 0x20), ("sw_power_cap", 0x4))
+
+
+def clock_summary(rows, sm_max_default=None, source=""):
+    """Median SM clock under load (samples at >= half the highest seen), the
+    highest max clock, and every throttle reason seen active. rows: (sm MHz,
+    max MHz, reason names)."""
+    sm = [r[0] for r in rows if r[0] is not None]
+    smax = [r[1] for r in rows if r[1] is not None]
+    if not sm:
+        return {"sm_mhz": None, "sm_max_mhz": sm_max_default, "reasons": ["unsampled"]}
+    top = max(sm)
+    loaded = [s for s in sm if s >= 0.5 * top]
+    reasons = sorted({x for r in rows for x in r[2]})
+    return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(smax) if smax else sm_max_default,
+            "samples": len(rows), "samples_under_load": len(loaded), "reasons": reasons,
+            "source": source}
+
+
+class NvmlClockSampler:
+    """SM clock, max clock and throttle reasons of the bench's GPU read through
+    NVML every 5 ms by a background thread while the timed region runs (the
+    launching thread spends that time in library calls and synchronisations,
+    which release the GIL). The board is found by the CUDA device's UUID, so a
+    restricted CUDA_VISIBLE_DEVICES still names the right one."""
+
+    PERIOD_S = 0.005
+
+    def __init__(self, device: int):
+        import threading
+
+        import pynvml
+        import torch
+        self.nv = pynvml
+        pynvml.nvmlInit()
+        uuid = str(torch.cuda.get_device_properties(device).uuid)
+        self.h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+        self.rows = []
+        self.stop = threading.Event()
+        self.thread = threading.Thread(target=self._run, daemon=True)
+
+    def _sample(self):
+        nv = self.nv
+        sm = float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+        bits = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+        self.rows.append((sm, self.max_mhz, [n for n, b in REASON_BITS if bits & b]))
+
+    def _run(self):
+        while not self.stop.is_set():
+            try:
+                self._sample()
+            except Exception:  # a failed read ends sampling, never the bench
+                return
+            self.stop.wait(self.PERIOD_S)
+
+    def __enter__(self):
+        self.thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self.stop.set()
+        self.thread.join(timeout=5)
+        try:
+            self.nv.nvmlShutdown()
+        except Exception:
+            pass
+
+    def summary(self, sm_max_default=None):
+        return clock_summary(self.rows, sm_max_default, "nvml every 5 ms")
+
+
+def ClockSampler(device: int):
+    """The NVML sampler, or nvidia-smi every 50 ms where NVML cannot be used."""
+    try:
+        return NvmlClockSampler(device)
+    except Exception:
+        return SmiClockSampler(device)
+
+
+class SmiClockSampler:
     """nvidia-smi clocks/throttle reasons sampled every 50 ms in the background."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -154,15 +250,10 @@ class ClockSampler:
                 return float(x)
             except ValueError:
                 return None
-        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
-        smax = [num(r[2]) for r in rows if num(r[2]) is not None]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
-        top = max(sm) if sm else None
-        loaded = [s for s in sm if top and s >= 0.5 * top] or sm
-        return {"sm_mhz": statistics.median(loaded) if loaded else None,
-                "sm_max_mhz": max(smax) if smax else sm_max_default,
-                "samples": len(rows), "reasons": reasons}
+        names = [n for n, _ in REASON_BITS]
+        return clock_summary([(num(r[1]), num(r[2]),
+                               [names[i] for i in range(4) if r[5 + i].lower() == "active"])
+                              for r in rows], sm_max_default, "nvidia-smi every 50 ms")
 
 
 # ---------------------------------------------------------------- roofline
@@ -363,7 +454,7 @@ def run_reference(a, rank, world):
         "mean_ms_per_step": statistics.mean(times) * 1e3,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic",
-        "config": {**workload_config(a), "n": n, "m": m,
+        "config": {**workload_config(a, n, m), "n": n, "m": m,
                    "parallelism": f"task-shard x{world}" if world > 1 else "1 GPU"},
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "edges/s", "cores": orc.num_threads(),
@@ -525,7 +616,7 @@ def run_ours(a, rank, world, local_rank):
         "metric": "TC edges/s", "value": value, "unit": "edges/s", "n_gpus": world,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_per_step,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "int32",
-        "data": "synthetic", "config": {**workload_config(a), "n": n, "m": m,
+        "data": "synthetic", "config": {**workload_config(a, n, m), "n": n, "m": m,
                                         "parallelism": f"task-shard x{world}" if world > 1 else "1 GPU"},
         "triangles": count,
         "phases_ms": {"orient": statistics.mean(orient_ms), "count": cnt_avg, "hub_kernel": hub_avg,

@@ -55,6 +55,9 @@ struct CountArgs {
   int shard, num_shards;  // this call counts tasks shard, shard + num_shards, ...
   BatchView bv;           // per-graph table factor and counts of a batch
   int stage_off;          // staged hub kernel: start of the copy slots (ints)
+  int64_t nnz;            // entries of col (the row prefetch never copies past them)
+  int short_ranges;       // short stream: one contiguous range per warp (else windows)
+  int long_classes;       // long lists of one batch placed before the longer ones
 };
 
 // log2 of the table slots per key of owner x's graph (4 slots per key by
@@ -166,14 +169,15 @@ __device__ __forceinline__ bool owns(int x, int px, int y, int py) {
 constexpr int kLongList = 64;
 
 // Partners of one hub task, compacted in row order.  Thread t examines
-// neighbours 2t and 2t+1 of the chunk; one block scan of (long partners,
-// short partners, dense partners, short list lengths) packed in 64 bits
-// (16 bits each: a chunk has at most 512 partners and the short lengths sum
-// to at most 512 x 63) places every partner.  Long list j (j < nl): start
-// base[j], length off[j].  Short list j: elements [off[nl+j], off[nl+j+1])
-// of the short stream, element f of it at lists[base[nl+j] + f] (base =
-// list start - offset).  Dense partner j (j < nd): its rank at
-// base[kHubChunk - 1 - j], above every long and short entry.
+// neighbours 2t and 2t+1 of the chunk; one block scan of (long partners of
+// one batch, longer long partners, short partners, dense partners, short
+// list lengths) packed in 64 bits places every partner: four 11-bit counts
+// (a chunk has at most 1024 partners) and a 16-bit length sum (at most
+// 1024 x 63).  Long list j (j < nl): start base[j], length off[j].  Short
+// list j: elements [off[nl+j], off[nl+j+1]) of the short stream, element f
+// of it at lists[base[nl+j] + f] (base = list start - offset).  Dense
+// partner j (j < nd): its rank at base[kHubChunk - 1 - j], above every long
+// and short entry.
 //
 // A long partner y is dense when the owner keeps a bitmap (owner_bits, its
 // rank) and y has a core bitmap whose AND with it over the words below both
@@ -182,11 +186,28 @@ struct Partners {
   int nl;     // long lists
   int total;  // elements of the short stream
   int nd;     // dense partners
+  int ns;     // short lists
+};
+
+// Fields of the partner scan's 64-bit word.
+constexpr int kLenShift = 0, kDenseShift = 16, kShortShift = 27, kLongAShift = 38,
+              kLongBShift = 49;
+constexpr unsigned long long kLenMask = 0xffffull, kCountMask = 0x7ffull;
+static_assert(kLongBShift + 11 <= 64 && kHubChunk <= 1024 && kHubChunk * 63 <= 0xffff,
+              "partner scan fields hold a chunk's counts and short lengths");
+
+// The chunk's neighbours come from the row prefetch in shared memory where
+// it holds them (entries [ca, cend) of col at s_col[0 ..)), else from global
+// memory.
+struct ChunkSource {
+  const int *s_col;  // null: every neighbour from global memory
+  long long ca, cend;
 };
 
 __device__ __forceinline__ Partners find_partners(const CountArgs &a, int x, int px, int64_t e0,
                                                   int nc, long long *s_base, int *s_off,
-                                                  unsigned long long *s_warp, int owner_bits) {
+                                                  unsigned long long *s_warp, int owner_bits,
+                                                  ChunkSource src = ChunkSource{nullptr, 0, 0}) {
   constexpr int kR = kHubChunk / kCountThreads;  // neighbours per thread
   static_assert(kR * kCountThreads == kHubChunk && kHubChunk <= 1024,
                 "whole neighbours per thread; 16-bit scan fields");
@@ -199,7 +220,8 @@ __device__ __forceinline__ Partners find_partners(const CountArgs &a, int x, int
   for (int r = 0; r < kR; ++r) {
     const int i = kR * threadIdx.x + r;
     if (i < nc) {
-      const int y = __ldg(a.col + e0 + i);
+      const long long e = e0 + i;
+      const int y = src.s_col && e < src.cend ? src.s_col[e - src.ca] : __ldg(a.col + e);
       const int4 pi = __ldg(a.pinfo + y);
       const int py = pi.x;
       if (owns(x, px, y, py)) {
@@ -214,12 +236,19 @@ __device__ __forceinline__ Partners find_partners(const CountArgs &a, int x, int
       }
     }
   }
+  // Long lists of one 128-entry batch (64..127 entries) take the slots
+  // before the longer ones, so a claimed pair mostly streams two lists of
+  // the same batch count (at RMAT scale 22, counted on the CPU: 22.8 M pair
+  // batches against 25.8 M in row order).  Off (long_classes 0): every long
+  // list in row order.
+  const bool classes = a.long_classes != 0;
   unsigned long long mine = 0;
 #pragma unroll
   for (int r = 0; r < kR; ++r) {
-    if (dense[r]) mine += 1ull << 16;
-    else if (len[r] >= kLongList) mine += 1ull << 48;
-    else if (len[r] > 0) mine += (1ull << 32) + (unsigned)len[r];
+    if (dense[r]) mine += 1ull << kDenseShift;
+    else if (len[r] >= kLongList)
+      mine += 1ull << (classes && len[r] >= 2 * kLongList ? kLongBShift : kLongAShift);
+    else if (len[r] > 0) mine += (1ull << kShortShift) + ((unsigned long long)len[r] << kLenShift);
   }
   unsigned long long incl = mine;
 #pragma unroll
@@ -237,20 +266,23 @@ __device__ __forceinline__ Partners find_partners(const CountArgs &a, int x, int
     all += v;
   }
   const unsigned long long excl = before + incl - mine;
-  const int nl = (int)(all >> 48), ns = (int)((all >> 32) & 0xffff);
-  const int nd = (int)((all >> 16) & 0xffff);
-  int lslot = (int)(excl >> 48);
-  int sslot = nl + (int)((excl >> 32) & 0xffff), off = (int)(excl & 0xffff);
-  int dslot = (int)((excl >> 16) & 0xffff);
+  auto field = [](unsigned long long v, int shift) { return (int)((v >> shift) & kCountMask); };
+  const int nla = field(all, kLongAShift);
+  const int nl = nla + field(all, kLongBShift), ns = field(all, kShortShift);
+  const int nd = field(all, kDenseShift);
+  int aslot = field(excl, kLongAShift), bslot = nla + field(excl, kLongBShift);
+  int sslot = nl + field(excl, kShortShift), off = (int)((excl >> kLenShift) & kLenMask);
+  int dslot = field(excl, kDenseShift);
 #pragma unroll
   for (int r = 0; r < kR; ++r) {
     if (dense[r]) {
       s_base[kHubChunk - 1 - dslot] = st[r];
       ++dslot;
     } else if (len[r] >= kLongList) {
-      s_base[lslot] = st[r];
-      s_off[lslot] = len[r];
-      ++lslot;
+      const bool b = classes && len[r] >= 2 * kLongList;
+      const int slot = b ? bslot++ : aslot++;
+      s_base[slot] = st[r];
+      s_off[slot] = len[r];
     } else if (len[r] > 0) {
       s_base[sslot] = st[r] - off;
       s_off[sslot] = off;
@@ -258,10 +290,10 @@ __device__ __forceinline__ Partners find_partners(const CountArgs &a, int x, int
       off += len[r];
     }
   }
-  const int total = (int)(all & 0xffff);
+  const int total = (int)((all >> kLenShift) & kLenMask);
   if (threadIdx.x == 0) s_off[nl + ns] = total;
   __syncthreads();
-  return Partners{nl, total, nd};
+  return Partners{nl, total, nd, ns};
 }
 
 // One warp streams N lists lists[st[i], st[i] + len[i]) together with
@@ -437,6 +469,49 @@ __device__ __forceinline__ unsigned stream_short(const int32_t *__restrict__ lis
   return hits;
 }
 
+// The short stream in contiguous ranges: warp w takes elements [lo, hi), an
+// eighth of the stream rounded to whole 128-element windows, so a lane's list
+// pointer only ever moves forward across the warp's windows.  (With the
+// windows w, w + 8, ... every warp steps over all lists of the task between
+// its windows: at RMAT scale 22, counted on the CPU, 81 M list steps against
+// 35 M inside the windows.)  The list holding lo is found by one binary
+// search over the ns + 1 offsets.
+template <class Probe>
+__device__ __forceinline__ unsigned stream_short_ranges(const int32_t *__restrict__ lists,
+                                                        const long long *s_base, const int *s_off,
+                                                        int total, int ns, int warp, int lane,
+                                                        const Probe &probe) {
+  constexpr int kU = 4;
+  constexpr int kWarps = kCountThreads / kWarp;
+  constexpr int kWin = kWarp * kU;
+  const int span = (total + kWarps * kWin - 1) / (kWarps * kWin) * kWin;
+  const int lo = warp * span, hi = min(total, lo + span);
+  unsigned hits = 0;
+  if (lo >= hi) return hits;
+  int l = 0, r = ns - 1;  // s_off[0] = 0 <= lo < total = s_off[ns]
+  while (l < r) {
+    const int m = (l + r + 1) >> 1;
+    if (s_off[m] <= lo) l = m;
+    else r = m - 1;
+  }
+  int jj = l;  // this lane's list, carried across the windows
+  for (int wb = lo; wb < hi; wb += kWin) {
+    int w[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const int f = wb + u * kWarp + lane;
+      w[u] = kNoKey;
+      if (f < hi) {
+        while (s_off[jj + 1] <= f) ++jj;
+        w[u] = __ldg(lists + s_base[jj] + f);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kU; ++u) hits += probe(w[u]);
+  }
+  return hits;
+}
+
 // |N+(owner) & N+(y)| summed over N dense partners y of ranks ry[i] (-1:
 // none): the AND of the owner's bitmap (shared memory, cleared to whole
 // quads past its rank) and each y's core bitmap over the quads below both
@@ -487,6 +562,7 @@ __device__ __forceinline__ unsigned long long stream_partners(const int32_t *__r
                                                               const int *s_off, Partners pt,
                                                               int *s_next, int warp, int lane,
                                                               const Probe &probe, Stage &sg,
+                                                              bool short_ranges,
                                                               const unsigned *bits = nullptr,
                                                               int owner_bits = 0,
                                                               const unsigned *core = nullptr) {
@@ -519,8 +595,13 @@ __device__ __forceinline__ unsigned long long stream_partners(const int32_t *__r
       hits += and_count_n<kND>(bits, owner_bits, core, ry, lane);
     }
   }
-  if (pt.total > 0)
-    hits += stream_short(lists, s_base + pt.nl, s_off + pt.nl, pt.total, warp, lane, probe);
+  if (pt.total > 0) {
+    if (short_ranges)
+      hits += stream_short_ranges(lists, s_base + pt.nl, s_off + pt.nl, pt.total, pt.ns, warp,
+                                  lane, probe);
+    else
+      hits += stream_short(lists, s_base + pt.nl, s_off + pt.nl, pt.total, warp, lane, probe);
+  }
   return hits;
 }
 
@@ -553,6 +634,53 @@ __device__ __forceinline__ unsigned long long stream_flat(const int32_t *__restr
 
 __device__ __forceinline__ int ceil_log2(int v) { return v <= 1 ? 0 : 32 - __clz(v - 1); }
 
+// A hub task as its CTA reads it: owner x with d+ d and rank R, the start a0
+// of N+(x), and the chunk [e0, e0 + nc) of x's symmetric row.  With the row
+// prefetch, [ca, cend) is the part of the chunk, widened to 16-byte bounds,
+// that a bulk copy brought into shared memory (cend <= ca: none).
+struct HubTask {
+  long long a0, e0, ca, cend;
+  int x, d, nc, R;
+};
+
+__device__ __forceinline__ HubTask hub_task(const CountArgs &a, unsigned long long t) {
+  HubTask h;
+  const uint64_t task = shard_task(a, t);
+  h.x = (int)(task >> 32);
+  const int chunk = (int)(task & 0xffffffffu);
+  h.a0 = a.dag_rowptr[h.x];
+  h.d = a.key[h.x].y;
+  h.e0 = a.rowptr[h.x] + (int64_t)chunk * kHubChunk;
+  h.nc = (int)min((long long)kHubChunk, (long long)(a.rowptr[h.x + 1] - h.e0));
+  h.R = a.rank ? __ldg(a.rank + h.x) : INT_MAX;
+  h.ca = h.cend = 0;
+  return h;
+}
+
+// Row prefetch: shared-memory ints for one chunk widened to 16-byte bounds
+// (at most kHubChunk + 4 after rounding both ends).
+constexpr int kRowStageInts = kHubChunk + 8;
+
+// Thread 0, one task ahead: task t's header into *s_hdr and its row chunk
+// into s_col by one cp.async.bulk (this GPU's own memory, no multicast)
+// completing on bar.  The copy starts at the chunk's first entry rounded
+// down to 16 bytes and ends at its last rounded up, but never past the
+// column array's last whole 16 bytes: entries after cend come from global
+// memory.
+__device__ __forceinline__ void row_prefetch(const CountArgs &a, unsigned long long t,
+                                             HubTask *s_hdr, int *s_col,
+                                             unsigned long long *bar) {
+  HubTask h = hub_task(a, t);
+  const long long ca = h.e0 & ~3LL;
+  const long long cend = min((long long)((h.e0 + h.nc + 3) & ~3LL), (long long)(a.nnz & ~3LL));
+  if (cend > ca) {
+    h.ca = ca;
+    h.cend = cend;
+    bulk_copy(s_col, a.col + ca, (unsigned)((cend - ca) * sizeof(int)), bar);
+  }
+  *s_hdr = h;
+}
+
 // One CTA per hub task: N+(owner) into shared memory; the chunk's partners
 // are found in one pass and compacted; then the whole CTA streams their
 // concatenated lists through it.  N+(owner) is kept as a bitmap over ranks
@@ -564,7 +692,14 @@ __device__ __forceinline__ int ceil_log2(int v) { return v <= 1 ? 0 : 32 - __clz
 // which follow the table in dynamic shared memory at a.stage_off ints.
 // (The copy slots' 16 KB leave room for 4 CTAs per SM, which the register
 // bound then follows.)
-template <bool kStaged>
+// kRowStage (MERCURY_TC_ROW_STAGE=1, off by default): thread 0 reads the
+// next task's header and bulk-copies its row chunk into shared memory while
+// the current task streams, so a task starts with its owner, offsets and
+// neighbour ids already on chip: the chain task -> owner row -> neighbours
+// -> partner records shrinks to its last load.  It measured slower (the
+// header loads hold warp 0 while the rest of the CTA waits for it at the
+// end-of-task barrier).
+template <bool kStaged, bool kRowStage>
 __global__ void __launch_bounds__(kCountThreads, kStaged ? 4 : 5) tc_hub_kernel(CountArgs a) {
   extern __shared__ __align__(128) int table[];
   __shared__ unsigned long long s_task;
@@ -573,6 +708,9 @@ __global__ void __launch_bounds__(kCountThreads, kStaged ? 4 : 5) tc_hub_kernel(
   __shared__ int s_off[kHubChunk + 1];
   __shared__ unsigned long long s_warp[kCountThreads / kWarp];
   __shared__ unsigned long long s_bar[kStaged ? kCountThreads / kWarp * 2 : 1];
+  __shared__ __align__(16) int s_col[kRowStage ? kRowStageInts : 4];
+  __shared__ HubTask s_hdr;
+  __shared__ unsigned long long s_cbar;
   const int lane = threadIdx.x & (kWarp - 1), warp = threadIdx.x / kWarp;
   const int64_t ntasks = shard_tasks(a);
   unsigned long long hits = 0;
@@ -588,10 +726,21 @@ __global__ void __launch_bounds__(kCountThreads, kStaged ? 4 : 5) tc_hub_kernel(
     }
     __syncwarp();
   }
+  // Parity of the row-prefetch barrier's next completion (the same on every
+  // thread: each waits once per copied chunk).
+  unsigned cphase = 0;
   // Thread 0 claims each task one task ahead, so the queue atomic's latency
   // overlaps the current task.
   unsigned long long t_next = 0;
-  if (threadIdx.x == 0) s_task = atomicAdd(a.queue, 1ull);
+  if (threadIdx.x == 0) {
+    const unsigned long long t0 = atomicAdd(a.queue, 1ull);
+    s_task = t0;
+    if constexpr (kRowStage) {
+      mbar_init(&s_cbar);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      if ((int64_t)t0 < ntasks) row_prefetch(a, t0, &s_hdr, s_col, &s_cbar);
+    }
+  }
   for (;;) {
     if (threadIdx.x == 0) {
       s_fail = 0;
@@ -601,14 +750,11 @@ __global__ void __launch_bounds__(kCountThreads, kStaged ? 4 : 5) tc_hub_kernel(
     const unsigned long long t = s_task;
     if ((int64_t)t >= ntasks) break;
     if (threadIdx.x == 0) t_next = atomicAdd(a.queue, 1ull);
-    const uint64_t task = shard_task(a, t);
-    const int x = (int)(task >> 32);
-    const int chunk = (int)(task & 0xffffffffu);
-    const int64_t a0 = a.dag_rowptr[x];
-    const int d = a.key[x].y;
-    const int64_t e0 = a.rowptr[x] + (int64_t)chunk * kHubChunk;
-    const int nc = (int)min((int64_t)kHubChunk, a.rowptr[x + 1] - e0);
-    const int R = a.rank ? __ldg(a.rank + x) : INT_MAX;
+    HubTask h;
+    if constexpr (kRowStage) h = s_hdr;
+    else h = hub_task(a, t);
+    const int x = h.x, d = h.d, nc = h.nc, R = h.R;
+    const int64_t a0 = h.a0, e0 = h.e0;
     const bool bitmap = R <= a.bitmap_bits;
     int lg = max(8, ceil_log2(d << table_factor_log2(a, x)));
     if (lg > a.table_log2_max && 2 * d <= (1 << a.table_log2_max)) lg = a.table_log2_max;
@@ -635,7 +781,21 @@ __global__ void __launch_bounds__(kCountThreads, kStaged ? 4 : 5) tc_hub_kernel(
     }
     // Dense partners need the owner's bitmap and the core bitmaps.
     const int owner_bits = bitmap && a.core ? R : 0;
-    const Partners pt = find_partners(a, x, d, e0, nc, s_base, s_off, s_warp, owner_bits);
+    ChunkSource src{nullptr, 0, 0};
+    if constexpr (kRowStage) {
+      if (h.cend > h.ca) {
+        // A wait that gives up raises kErrWaitTimeout (the call then fails),
+        // waits once more for the copy, and reads the chunk from global memory.
+        if (mbar_wait(&s_cbar, cphase)) {
+          src = ChunkSource{s_col, h.ca, h.cend};
+        } else {
+          atomicOr(a.err, kErrWaitTimeout);
+          mbar_wait(&s_cbar, cphase);
+        }
+        cphase ^= 1u;
+      }
+    }
+    const Partners pt = find_partners(a, x, d, e0, nc, s_base, s_off, s_warp, owner_bits, src);
     // N+(x) into shared memory.
     if (bitmap) {
       unsigned *bits = reinterpret_cast<unsigned *>(table);
@@ -658,20 +818,27 @@ __global__ void __launch_bounds__(kCountThreads, kStaged ? 4 : 5) tc_hub_kernel(
       if (!ok) s_fail = 1;
     }
     __syncthreads();
+    if constexpr (kRowStage) {
+      // Every thread has read this task's header and chunk (two barriers
+      // ago): the next task's may replace them.
+      if (threadIdx.x == 0 && (int64_t)t_next < ntasks)
+        row_prefetch(a, t_next, &s_hdr, s_col, &s_cbar);
+    }
     use_table = use_table && s_fail == 0;
+    const bool ranges = a.short_ranges != 0;
     unsigned long long th = 0;
     if (bitmap)
       th = stream_partners<kStaged>(
           a.dag_rank, s_base, s_off, pt, &s_next, warp, lane,
           BitmapProbe{reinterpret_cast<const unsigned *>(table), (unsigned)(((R + 127) >> 7) << 2)},
-          sg,
+          sg, ranges,
           reinterpret_cast<const unsigned *>(table), R, a.core);
     else if (use_table)
       th = stream_partners<kStaged>(a.dag_col, s_base, s_off, pt, &s_next, warp, lane,
-                                    CuckooProbe{table, shift}, sg);
+                                    CuckooProbe{table, shift}, sg, ranges);
     else
       th = stream_partners<false>(a.dag_col, s_base, s_off, pt, &s_next, warp, lane,
-                                  ListProbe{a.dag_col + a0, d}, sg);
+                                  ListProbe{a.dag_col + a0, d}, sg, ranges);
     hits += th;
     flush_task(a, x, th, lane);
     if (threadIdx.x == 0) s_task = t_next;  // every thread read s_task two barriers ago
@@ -866,7 +1033,24 @@ int tc_count_launch(mc_dgraph *g, cudaEvent_t after_hub, int shard, int num_shar
   const char *tma_env = std::getenv("MERCURY_TC_TMA");
   // (Lists in host memory, MC_HOST_DAG, always take the lane loads.)
   const bool staged = tma_env && std::atoi(tma_env) != 0 && !g->dag_host;
-  auto kern = staged ? tc_hub_kernel<true> : tc_hub_kernel<false>;
+  // MERCURY_TC_ROW_STAGE=1: the row prefetch, which bulk-copies chunks of
+  // the column array (device columns on a 16-byte boundary only).  Off by
+  // default: at RMAT scale 22 it took the hub kernel from 9.26 to 10.38 ms,
+  // as thread 0's header loads for the next task held warp 0 and the CTA's
+  // end-of-task barrier waited for it.
+  const char *row_env = std::getenv("MERCURY_TC_ROW_STAGE");
+  const bool row_stage = !staged && !g->col_host &&
+                         (reinterpret_cast<uintptr_t>(g->col) & 15u) == 0 && row_env &&
+                         std::atoi(row_env) != 0;
+  // MERCURY_TC_SHORT_RANGES=0: the short stream in interleaved windows.
+  const char *ranges_env = std::getenv("MERCURY_TC_SHORT_RANGES");
+  a.short_ranges = !(ranges_env && std::atoi(ranges_env) == 0);
+  // MERCURY_TC_LONG_CLASSES=0: long partner lists paired in row order.
+  const char *classes_env = std::getenv("MERCURY_TC_LONG_CLASSES");
+  a.long_classes = !(classes_env && std::atoi(classes_env) == 0);
+  a.nnz = g->nnz;
+  auto kern = staged ? tc_hub_kernel<true, false>
+                     : (row_stage ? tc_hub_kernel<false, true> : tc_hub_kernel<false, false>);
   const size_t extra = staged ? kStageBytes : 0;
   MC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)(big_smem + extra)));

@@ -169,3 +169,57 @@ def test_pattern_bytes_equal_the_loop_restatement(n, p, seed):
     want = loop_pattern_bytes(n, np.asarray(rp), np.asarray(col))
     for k, v in want.items():
         assert got[k] == pytest.approx(v, rel=1e-12), k
+
+
+def test_clock_summary_takes_the_median_under_load_and_every_reason():
+    rows = [(1965.0, 1965.0, []), (1950.0, 1965.0, ["sw_power_cap"]), (345.0, 1965.0, []),
+            (1965.0, 1965.0, ["hw_slowdown"])]
+    s = bench.clock_summary(rows)
+    assert s["sm_mhz"] == 1965.0 and s["sm_max_mhz"] == 1965.0
+    assert s["samples"] == 4 and s["samples_under_load"] == 3
+    assert s["reasons"] == ["hw_slowdown", "sw_power_cap"]
+    assert bench.clock_summary([], 1965.0)["reasons"] == ["unsampled"]
+
+
+def test_nvml_sampler_reads_the_board_of_the_cuda_device(monkeypatch):
+    """A fake NVML: the sampler finds the board by the CUDA device's UUID,
+    decodes the throttle-reason bits and samples until the region ends."""
+    import time
+    import torch
+
+    calls = {"uuid": None, "shutdown": 0}
+
+    class FakeNvml:
+        NVML_CLOCK_SM = 1
+
+        def nvmlInit(self):
+            pass
+
+        def nvmlShutdown(self):
+            calls["shutdown"] += 1
+
+        def nvmlDeviceGetHandleByUUID(self, uuid):
+            calls["uuid"] = uuid
+            return "h"
+
+        def nvmlDeviceGetMaxClockInfo(self, h, kind):
+            return 1965
+
+        def nvmlDeviceGetClockInfo(self, h, kind):
+            return 1900
+
+        def nvmlDeviceGetCurrentClocksEventReasons(self, h):
+            return 0x4 | 0x40  # sw_power_cap, hw_thermal_slowdown
+
+    monkeypatch.setitem(sys.modules, "pynvml", FakeNvml())
+    monkeypatch.setattr(torch.cuda, "get_device_properties",
+                        lambda d: SimpleNamespace(uuid="1234-abcd"))
+    s = bench.ClockSampler(0)
+    assert isinstance(s, bench.NvmlClockSampler)
+    with s:
+        time.sleep(0.05)
+    got = s.summary()
+    assert calls["uuid"] == "GPU-1234-abcd" and calls["shutdown"] == 1
+    assert got["sm_mhz"] == 1900.0 and got["sm_max_mhz"] == 1965.0
+    assert got["samples"] >= 2
+    assert got["reasons"] == ["hw_thermal_slowdown", "sw_power_cap"]

@@ -240,6 +240,56 @@ def test_hub_lists_staged_by_bulk_copies(monkeypatch, make, cap):
         assert sum(d.tc_count_shard(s, 3) for s in range(3)) == want
 
 
+@pytest.mark.parametrize("row_stage,ranges,classes", [("1", "1", "1"), ("0", "1", "1"),
+                                                      ("1", "0", "1"), ("1", "1", "0"),
+                                                      ("0", "0", "0")])
+@pytest.mark.parametrize("make", [lambda: Graph.rmat(16, 16, seed=51),
+                                  lambda: Graph.chung_lu(80000, 2.1, 24.0, 8000.0, seed=52),
+                                  lambda: fixture("dense400")])
+def test_hub_row_prefetch_and_stream_forms(monkeypatch, make, row_stage, ranges, classes):
+    """A hub task's row chunk reaches shared memory by a bulk copy issued one
+    task ahead (MERCURY_TC_ROW_STAGE=1) or by the partner scan's own loads
+    (the default); the short partner lists stream in one contiguous range per warp
+    (MERCURY_TC_SHORT_RANGES=1, the default) or in interleaved windows; long
+    lists of one 128-entry batch are paired before the longer ones
+    (MERCURY_TC_LONG_CLASSES=1, the default) or all in row order. Each form
+    gives the oracle's count on bitmap owners (cap 1000000) and table owners
+    (cap 0), whole and in shards."""
+    g = make()
+    want = orc.tc(g.rowptr, g.col)
+    monkeypatch.setenv("MERCURY_TC_ROW_STAGE", row_stage)
+    monkeypatch.setenv("MERCURY_TC_SHORT_RANGES", ranges)
+    monkeypatch.setenv("MERCURY_TC_LONG_CLASSES", classes)
+    for cap in ("0", "1000000"):
+        monkeypatch.setenv("MERCURY_TC_BITMAP_BITS", cap)
+        with DeviceGraph(g) as d:
+            assert d.tc_count() == want
+            assert d.tc_count() == want
+            assert sum(d.tc_count_shard(s, 3) for s in range(3)) == want
+
+
+@pytest.mark.parametrize("row_stage", ["1", "0"])
+def test_hub_row_prefetch_at_the_end_of_the_column_array(monkeypatch, row_stage):
+    """The hub owner with the largest d+ renamed to the last id, so its row
+    ends the column array, whose length is 2 mod 4: the prefetch copies the
+    chunk up to the array's last whole 16 bytes and the partner scan loads
+    the two entries after them. The count is the oracle's."""
+    g = Graph.rmat(12, 16, seed=2)
+    rp, col = np.array(g.rowptr), np.array(g.col)
+    assert len(col) % 4 == 2
+    n = len(rp) - 1
+    top = int(np.argmax(np.diff(orc.orient(rp, col)[0])))
+    perm = np.arange(n)
+    perm[top], perm[n - 1] = n - 1, top
+    rp2, col2 = relabel(rp, col, perm)
+    assert np.diff(orc.orient(rp2, col2)[0])[n - 1] > 64  # a hub owner
+    want = orc.tc(rp2, col2)
+    monkeypatch.setenv("MERCURY_TC_ROW_STAGE", row_stage)
+    with DeviceGraph(rp2, col2) as d:
+        assert d.tc_count() == want
+        assert sum(d.tc_count_shard(s, 2) for s in range(2)) == want
+
+
 def test_empty_and_edgeless_graphs():
     with DeviceGraph(np.zeros(1, dtype=np.int64), np.zeros(0, dtype=np.int32)) as d:
         assert d.tc_count() == 0
