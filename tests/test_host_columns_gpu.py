@@ -123,6 +123,23 @@ def test_small_device_budget_chooses_host_columns(monkeypatch):
     assert tc_count_host(g.rowptr, g.col) == want
 
 
+@pytest.mark.parametrize("placement", ["columns", "dag"])
+def test_forced_placement_counts_equal_device_placement(monkeypatch, placement):
+    """MERCURY_PLACEMENT=columns / dag forces the host placements that the
+    library otherwise chooses only when the graph does not fit; both give the
+    in-core counts."""
+    g = Graph.rmat(13, 16, seed=7)
+    want = orc.tc(g.rowptr, g.col)
+    with DeviceGraph(g) as d:
+        want_p5 = d.pattern_count(5)
+    monkeypatch.setenv("MERCURY_PLACEMENT", placement)
+    with DeviceGraph(g) as h:
+        assert h.columns_on_host
+        assert h.dag_on_host == (placement == "dag")
+        assert h.tc_count() == want
+        assert h.pattern_count(5) == want_p5
+
+
 def test_empty_and_edgeless_graphs_with_host_columns():
     with DeviceGraph(np.zeros(1, np.int64), np.zeros(0, np.int32), host_columns=True) as h:
         assert h.tc_count() == 0

@@ -56,6 +56,21 @@ def test_each_result_is_the_same_alone_and_in_the_mix():
     assert st["max_batch_seen"] > 1  # requests were coalesced
 
 
+def test_work_cap_of_one_runs_every_request_alone(monkeypatch):
+    """MERCURY_SERVE_BATCH_WORK=1: every request's estimated work is above
+    the cap, so each runs in a batch of its own; the results equal the plain
+    path's."""
+    monkeypatch.setenv("MERCURY_SERVE_BATCH_WORK", "1")
+    graphs, jobs = small_mix(5, 24)
+    want = [plain(g, j) for g, j in zip(graphs, jobs)]
+    with Server(8 << 30, max_batch=64, workers=2) as s:
+        tickets = [s.submit(g, j) for g, j in zip(graphs, jobs)]
+        got = [s.wait(t)[0] for t in tickets]
+        st = s.stats()
+    assert got == want
+    assert st["max_batch_seen"] == 1 and st["batches"] == 24
+
+
 def test_resident_cache_serves_keyed_graphs_without_arrays():
     g = Graph.rmat(10, 8, seed=5)
     want = plain(g, 0)

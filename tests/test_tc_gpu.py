@@ -209,6 +209,18 @@ def test_dense_partners_by_core_bitmap_and(monkeypatch, make, core):
         assert sum(d.tc_count_shard(s, 3) for s in range(3)) == want
 
 
+@pytest.mark.parametrize("factor", ["1", "8", "64"])
+def test_dense_factor_moves_the_and_boundary(monkeypatch, factor):
+    """MERCURY_TC_DENSE_FACTOR: words of a core-bitmap AND allowed per list
+    entry it replaces; every boundary gives the oracle's count."""
+    g = Graph.rmat(16, 16, seed=34)
+    want = orc.tc(g.rowptr, g.col)
+    monkeypatch.setenv("MERCURY_TC_DENSE_FACTOR", factor)
+    with DeviceGraph(g) as d:
+        assert d.tc_count() == want
+        assert sum(d.tc_count_shard(s, 2) for s in range(2)) == want
+
+
 @pytest.mark.parametrize("bits", ["0", "700", "5000"])
 def test_dense_partners_with_mixed_owner_kinds(monkeypatch, bits):
     """Owners above the bitmap cap use tables and never take the AND path;
