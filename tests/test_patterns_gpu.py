@@ -238,9 +238,9 @@ def test_pattern_bench_graph_counts_equal_committed_oracle():
 
 
 @pytest.mark.parametrize("route", ["default", "centers", "edge"])
-def test_survey_shape_graph_with_hubs_counts_equal_committed_oracle(monkeypatch, route):
-    """The survey's pattern graph shape (Chung-Lu gamma 2.1, mean 20, weight
-    cap 50,000) at 5,000 vertices, small enough for the literal oracle:
+def test_power_law_graph_with_hubs_counts_equal_committed_oracle(monkeypatch, route):
+    """The shape of the pattern benchmark graph (Chung-Lu gamma 2.1, mean 20,
+    weight cap 50,000) at 5,000 vertices, small enough for the literal oracle:
     hubs of degree 2,187, 1,525 and 1,173 (above the 1,024 limit of the
     bitmap kernels, P1's hub tasks included). All eight counts equal the
     oracle's, committed by tests/golden/make_pattern_golden.py, on every
