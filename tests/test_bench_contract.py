@@ -171,6 +171,14 @@ def test_pattern_bytes_equal_the_loop_restatement(n, p, seed):
         assert got[k] == pytest.approx(v, rel=1e-12), k
 
 
+def test_pattern_summary_records_an_error_instead_of_raising():
+    """The P1-P8 summary that the triangle bench appends never fails the
+    triangle-count line: without a device it returns the error."""
+    s = bench.pattern_summary(steps=1, n=2000, mean=6.0, cap=50.0)
+    if "error" not in s:  # a device is present
+        assert set(s["per_pattern"]) == {f"P{k}" for k in range(1, 9)}
+
+
 def test_clock_summary_takes_the_median_under_load_and_every_reason():
     rows = [(1965.0, 1965.0, []), (1950.0, 1965.0, ["sw_power_cap"]), (345.0, 1965.0, []),
             (1965.0, 1965.0, ["hw_slowdown"])]
