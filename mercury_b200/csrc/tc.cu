@@ -473,9 +473,9 @@ __device__ __forceinline__ unsigned stream_short(const int32_t *__restrict__ lis
 // eighth of the stream rounded to whole 128-element windows, so a lane's list
 // pointer only ever moves forward across the warp's windows.  (With the
 // windows w, w + 8, ... every warp steps over all lists of the task between
-// its windows: at RMAT scale 22, counted on the CPU, 81 M list steps against
-// 35 M inside the windows.)  The list holding lo is found by one binary
-// search over the ns + 1 offsets.
+// its windows: at RMAT scale 22, counted on the CPU, 78 M list steps between
+// windows and 24 M inside them, against 36 M for the ranges.)  The list
+// holding lo is found by one binary search over the ns + 1 offsets.
 template <class Probe>
 __device__ __forceinline__ unsigned stream_short_ranges(const int32_t *__restrict__ lists,
                                                         const long long *s_base, const int *s_off,
