@@ -122,3 +122,35 @@ def test_fast_p1_p4_restatement_on_fixtures_and_hubs():
     rp, col = orc.chung_lu(20000, 2.1, 12.0, 2000.0, seed=4)
     for k in (1, 4):
         assert orc.pattern_fast(rp, col, k, True) == orc.pattern(rp, col, k, True), k
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_p7_clique_restatement_equals_literal_oracle(seed):
+    """p7_cliques.cpp counts P7 as inclusion-exclusion over triangle, K4 and
+    K5 counts; it equals the literal restatement on random graphs of rising
+    density."""
+    n = 20 + 12 * seed
+    rp, col = csr_from_edges(n, random_graph(n, 0.12 + 0.08 * seed, 400 + seed))
+    assert orc.p7_cliques(rp, col) == orc.pattern(rp, col, 7)
+
+
+def test_p7_clique_restatement_on_fixtures_and_hubs():
+    """The golden fixtures, and the Chung-Lu graph with hubs of degree 2,187,
+    1,525 and 1,173 whose P7 the literal oracle committed."""
+    named = [name for name in sorted(GOLD) if "P7" in GOLD[name]]
+    assert len(named) >= 5
+    for name in named:
+        rp, col = load_fixture(name)
+        assert orc.p7_cliques(rp, col) == GOLD[name]["P7"], name
+    with open(os.path.join(GOLDEN, "pattern_counts.json")) as f:
+        rec = json.load(f)["chung_lu_n5000_mean20_cap50000_seed1"]
+    rp, col = orc.chung_lu(5000, 2.1, 20.0, 50000.0, seed=1)
+    assert orc.p7_cliques(rp, col) == rec["counts"]["P7"]
+
+
+def test_p7_clique_restatement_refuses_degrees_where_products_wrap():
+    """Above degree 46,340 the reference's 32-bit products can wrap and the
+    identity no longer holds: the restatement refuses (None)."""
+    n = 46342
+    rp, col = csr_from_edges(n, [(0, v) for v in range(1, n)])
+    assert orc.p7_cliques(rp, col) is None
