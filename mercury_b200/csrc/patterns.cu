@@ -2164,6 +2164,16 @@ int pattern_count_body(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12,
                        mc_timing_t *timing, int shard, int num_shards, double budget_ms,
                        double *progress) {
   NvtxRange range("pattern_count");
+  if (pattern < 1 || pattern > 8) return MC_ERR_ARG;
+  // P7 on graphs with hubs: by clique counts over the degree-ordered DAG
+  // (cliques.cu), which is built first; its time counts as the pattern's.
+  bool cliques = false;
+  int64_t dag_edges = 0;
+  if (pattern == 7) {
+    MC_CUDA_TRY(cudaEventRecord(g->ev[0], g->stream));
+    const int rc = p7_clique_prepare(g, &cliques, &dag_edges);
+    if (rc != MC_OK) return rc;
+  }
   // MERCURY_PATTERN_SLICE=1/0 forces slicing on/off (the tests compare both);
   // MERCURY_PATTERN_SLICE_MS sets the target slice length; MERCURY_TRACE_SLICES
   // prints each slice to stderr.
@@ -2204,9 +2214,11 @@ int pattern_count_body(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12,
     g->h_counters[6] = 0;
   }
   if (const char *env = std::getenv("MERCURY_PATTERN_SETS")) a.use_sets = std::atoi(env) != 0;
-  MC_CUDA_TRY(cudaEventRecord(g->ev[0], s));
+  if (!cliques) MC_CUDA_TRY(cudaEventRecord(g->ev[0], s));
   int rc = MC_OK;
-  if (g->n > 0 && g->nnz > 0) {
+  if (cliques) {
+    rc = p7_clique_launch(g, dag_edges, shard, num_shards, a.deadline, a.stop_flag);
+  } else if (g->n > 0 && g->nnz > 0) {
     // MERCURY_PATTERN_KERNEL=edge / =centers forces one route for every
     // pattern (the tests run all three settings; timing comparisons use it).
     const char *route = std::getenv("MERCURY_PATTERN_KERNEL");
@@ -2249,7 +2261,10 @@ int pattern_count_body(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12,
   if (sl.trace && g->h_counters[7])
     std::fprintf(stderr, "mercury: %llu centers built their outer rows per edge\n",
                  (unsigned long long)g->h_counters[7]);
-  if (budget_ms > 0 && g->h_counters[6]) return MC_ERR_TIMEOUT;  // a kernel stopped early
+  if (budget_ms > 0 && g->h_counters[6]) {  // a kernel stopped early
+    if (cliques && progress) *progress = 0.0;  // the clique route keeps no task fraction
+    return MC_ERR_TIMEOUT;
+  }
   const unsigned long long c1 = g->h_counters[0], c2 = g->h_counters[1];
   *out = (pattern == 4 || pattern == 6) ? c1 : c1 - c2;
   if (c12) {
