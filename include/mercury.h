@@ -267,12 +267,12 @@ int mc_dgraph_export_dag(const mc_dgraph_t *g, int64_t *rowptr_out,
  * kernels in subgraph_matching/pattern_kernels.cuh, combine at
  * sm_multigpu.cu:206-232): the same quantities over all 2m directed edges,
  * bit-exact, without MPI.  Uses per-warp frontier scratch of max_degree
- * entries per list, grown on first use and kept by the handle.  P7 on a
- * graph with a vertex of degree above 4,096 (and none above 46,340, where
- * the reference's 32-bit products could wrap) is counted from the
- * triangles, K4s and K5s of the degree-ordered DAG instead of the
- * per-edge formula: the same value, in time that grows with those clique
- * counts rather than with the cube of a hub's degree (MERCURY_P7_ROUTE=
+ * entries per list, grown on first use and kept by the handle.  P7 and P8
+ * on a graph with a vertex of degree above 4,096 (and none above 46,340,
+ * where the reference's 32-bit products could wrap) are counted from the
+ * triangles, K4s and K5s of the degree-ordered DAG instead of the per-edge
+ * formulas: the same values, in time that grows with those clique counts
+ * rather than with the cube of a hub's degree (MERCURY_CLIQUE_ROUTE=
  * cliques / formula forces either route). */
 int mc_pattern_count(mc_dgraph_t *g, int pattern, uint64_t *count,
                      mc_timing_t *timing);

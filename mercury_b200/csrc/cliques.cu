@@ -1,9 +1,9 @@
-// P7 by clique counts: a second device route for the reference's P7
-// (subgraph_matching/pattern_kernels.cuh:352-459, combined as in
-// subgraph_matching/sm_multigpu.cu:206-232) on graphs whose hubs make the
-// per-edge formula cubic in a hub's degree.
+// P7 and P8 by clique counts: a second device route for the reference's P7
+// and P8 (subgraph_matching/pattern_kernels.cuh:352-459 and :461-572,
+// combined as in subgraph_matching/sm_multigpu.cu:206-232) on graphs whose
+// hubs make the per-edge formulas cubic in a hub's degree.
 //
-// Per directed edge (v0, v1) the formula counts I3(A), the pairwise
+// P7.  Per directed edge (v0, v1) the formula counts I3(A), the pairwise
 // non-adjacent triples of A = N(v0) & N(v1).  By inclusion-exclusion over
 // the edges inside A,
 //   I3(A) = C(a, 3) - e_A (a - 2) + sum over x in A of C(d_A(x), 2) - t_A,
@@ -12,8 +12,13 @@
 // every edge (each triangle appears for its three edges, each K5 holds ten):
 //   P7 = 2 sum_e C(a_e, 3) - sum_tau k_tau (a_e1 + a_e2 + a_e3 - 6)
 //        + 6 sum_tau C(k_tau, 2) - 20 K5,
-// k_tau = |N(x) & N(y) & N(z)| for the triangle tau = {x, y, z}.  Every
-// term is a sum over edges or triangles, so each is accumulated modulo 2^64
+// k_tau = |N(x) & N(y) & N(z)| for the triangle tau = {x, y, z}.
+// P8.  The formula counts each induced tailed K4 (a K4 with a vertex hung on
+// one of its vertices alone) three times; inclusion-exclusion over the hung
+// vertex's neighbours, summed over every K4, gives
+//   P8 = sum_tau k_tau (d_x + d_y + d_z) - 3 sum_tau k_tau (a_e1 + a_e2 + a_e3)
+//        + 9 sum_tau k_tau^2 - 60 K5.
+// Every term is a sum over edges or triangles, so each is accumulated modulo 2^64
 // as the reference's u64 counter is, and shards of the edges sum to the
 // whole.  The identity holds while the reference's 32-bit products cannot
 // wrap: the route runs only for a maximum degree of at most 46,340.
@@ -50,6 +55,7 @@ struct CliqueArgs {
   int shard, num_shards;
   const unsigned long long *deadline;  // budgeted count: globaltimer ns, or null
   unsigned long long *stop_flag;
+  int pattern;  // 7 or 8
 };
 
 __device__ __forceinline__ unsigned long long clique_ns() {
@@ -106,7 +112,7 @@ __device__ __forceinline__ int64_t shard_edge(const CliqueArgs &a, unsigned long
 // Triangles per DAG edge (u -> v): a = |N(u) & N(v)| over the symmetric rows,
 // by walking the shorter row and searching the longer (warp per edge, every
 // edge: the triangle kernel reads the counts of all three edges of its
-// triangles).  Edges of this shard add 2 C(a, 3).
+// triangles).  For P7, edges of this shard add 2 C(a, 3).
 __global__ void __launch_bounds__(256) clique_edge_kernel(CliqueArgs a) {
   const int lane = threadIdx.x & (kWarp - 1);
   unsigned long long mine = 0;
@@ -130,7 +136,8 @@ __global__ void __launch_bounds__(256) clique_edge_kernel(CliqueArgs a) {
       hits = warp_sum_int(hits);
       if (lane == 0) {
         a.tri[i] = hits;
-        if (i % a.num_shards == a.shard) mine += 2ull * choose3((unsigned long long)hits);
+        if (a.pattern == 7 && i % a.num_shards == a.shard)
+          mine += 2ull * choose3((unsigned long long)hits);
       }
     }
   }
@@ -139,7 +146,8 @@ __global__ void __launch_bounds__(256) clique_edge_kernel(CliqueArgs a) {
 
 // The triangle terms of this shard's DAG edges (u -> v): for each w in
 // T = N+(u) & N+(v), the triangle's k = |N(u) & N(v) & N(w)|, its edges'
-// triangle counts, and the K5s on it as the first three of their DAG order.
+// triangle counts, its vertices' degrees (P8) and the K5s on it as the
+// first three of their DAG order.
 __global__ void __launch_bounds__(kCliqueWarps * kWarp) clique_triangle_kernel(CliqueArgs a) {
   __shared__ int32_t s_t[kCliqueWarps][kCliqueMaxOut];
   __shared__ int32_t s_s[kCliqueWarps][kCliqueMaxOut];
@@ -214,10 +222,17 @@ __global__ void __launch_bounds__(kCliqueWarps * kWarp) clique_triangle_kernel(C
         if (lane == 0) {
           const long long a_uw = __ldg(a.tri + a.drp[u] + lower_index(ou, lu, w));
           const long long a_vw = __ldg(a.tri + a.drp[v] + lower_index(ov, lv, w));
-          const long long k = kt;
-          mine += 6ull * choose2((unsigned long long)k);
-          mine -= (unsigned long long)(k * (a_uv + a_uw + a_vw - 6));
-          mine -= 20ull * (unsigned long long)k5;
+          const long long k = kt, sum_a = a_uv + a_uw + a_vw;
+          if (a.pattern == 7) {
+            mine += 6ull * choose2((unsigned long long)k);
+            mine -= (unsigned long long)(k * (sum_a - 6));
+            mine -= 20ull * (unsigned long long)k5;
+          } else {
+            mine += (unsigned long long)(k * ((long long)du + dv + dw));
+            mine -= (unsigned long long)(3 * k * sum_a);
+            mine += (unsigned long long)(9 * k * k);
+            mine -= 60ull * (unsigned long long)k5;
+          }
         }
       }
       __syncwarp();  // T is rewritten for the next edge
@@ -235,17 +250,18 @@ int resident(const void *kernel, int threads) {
 
 }  // namespace
 
-// MERCURY_P7_ROUTE=cliques sends P7 here whenever the graph allows it,
-// =formula never; unset, P7 takes this route on graphs with a vertex of
-// degree above 4,096 (where the formula's per-edge loops do not finish),
-// unless MERCURY_PATTERN_KERNEL forces a formula route.  The degree-ordered
+// MERCURY_CLIQUE_ROUTE=cliques sends P7 and P8 here whenever the graph
+// allows it, =formula never; unset, they take this route on graphs with a
+// vertex of degree above 4,096 (where the formulas' per-edge loops do not
+// finish), unless MERCURY_PATTERN_KERNEL forces a formula route.  The degree-ordered
 // DAG is built (or reused) here; *use is false when the graph does not
 // allow the route (a degree above 46,340, where the reference's products
 // wrap, or a DAG out-list longer than kCliqueMaxOut).
-int p7_clique_prepare(mc_dgraph *g, bool *use, int64_t *dag_edges) {
+int clique_prepare(mc_dgraph *g, int pattern, bool *use, int64_t *dag_edges) {
   *use = false;
   *dag_edges = 0;
-  const char *env = std::getenv("MERCURY_P7_ROUTE");
+  if (pattern != 7 && pattern != 8) return MC_OK;
+  const char *env = std::getenv("MERCURY_CLIQUE_ROUTE");
   const bool forced = env && std::strcmp(env, "cliques") == 0;
   if (env && std::strcmp(env, "formula") == 0) return MC_OK;
   if (!forced && (std::getenv("MERCURY_PATTERN_KERNEL") || g->max_degree <= 4096)) return MC_OK;
@@ -268,17 +284,18 @@ int p7_clique_prepare(mc_dgraph *g, bool *use, int64_t *dag_edges) {
   return MC_OK;
 }
 
-// Adds P7 of this shard's DAG edges to counters[0] (zeroed by the caller,
-// with counters[2] and counters[3], the kernels' queues).  The DAG and its
-// m entries come from p7_clique_prepare.
-int p7_clique_launch(mc_dgraph *g, int64_t m, int shard, int num_shards,
-                     const unsigned long long *deadline, unsigned long long *stop_flag) {
-  NvtxRange range("p7_cliques");
+// Adds P7 or P8 of this shard's DAG edges to counters[0] (zeroed by the
+// caller, with counters[2] and counters[3], the kernels' queues).  The DAG
+// and its m entries come from clique_prepare.
+int clique_launch(mc_dgraph *g, int pattern, int64_t m, int shard, int num_shards,
+                  const unsigned long long *deadline, unsigned long long *stop_flag) {
+  NvtxRange range("clique_patterns");
   cudaStream_t s = g->stream;
   int32_t *tri = nullptr;
   MC_CUDA_TRY(dev_alloc(reinterpret_cast<void **>(&tri), sizeof(int32_t) * (size_t)(m + 1), s));
   CliqueArgs a{g->rowptr, g->col, g->dag_rowptr, g->dag_col, g->n, m, tri,
-               g->counters + 0, g->counters + 2, shard, num_shards, deadline, stop_flag};
+               g->counters + 0, g->counters + 2, shard, num_shards, deadline, stop_flag,
+               pattern};
   const int edge_grid = g->num_sms * resident((const void *)clique_edge_kernel, 256);
   clique_edge_kernel<<<edge_grid, 256, 0, s>>>(a);
   cudaError_t e = cudaGetLastError();

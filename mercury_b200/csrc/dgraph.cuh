@@ -25,7 +25,7 @@ constexpr int kHubSmallTableLog2 = 12;
 // Least shared memory of a hub CTA (also the bitmap capacity: 8 bits per
 // byte, so owners of degree rank below 262144 use bitmaps).
 constexpr int kHubBitmapBytes = 32768;
-// Longest DAG out-list the P7 clique route stages in shared memory.
+// Longest DAG out-list the P7/P8 clique route stages in shared memory.
 constexpr int kCliqueMaxOut = 1024;
 // Core bitmaps: N+(v) as a bitmap over ranks [0, rank(v)) for the vertices
 // of the kCoreRanks lowest ranks (the highest degrees), so that a hub task
@@ -158,11 +158,12 @@ int64_t tc_device_bytes(int64_t n, int64_t nnz, bool col_host, bool dag_host = f
 // handle in chunks during the passes, each chunk checked against the CSR
 // contract first (the row offsets must have been checked: validate_rowptr).
 int tc_orient(mc_dgraph *g, const int32_t *upload = nullptr);
-// P7 by clique counts (cliques.cu): whether the route applies (building the
-// DAG if it does), and its launch, which adds the count to counters[0].
-int p7_clique_prepare(mc_dgraph *g, bool *use, int64_t *dag_edges);
-int p7_clique_launch(mc_dgraph *g, int64_t dag_edges, int shard, int num_shards,
-                     const unsigned long long *deadline, unsigned long long *stop_flag);
+// P7 and P8 by clique counts (cliques.cu): whether the route applies
+// (building the DAG if it does), and its launch, which adds the count to
+// counters[0].
+int clique_prepare(mc_dgraph *g, int pattern, bool *use, int64_t *dag_edges);
+int clique_launch(mc_dgraph *g, int pattern, int64_t dag_edges, int shard, int num_shards,
+                  const unsigned long long *deadline, unsigned long long *stop_flag);
 // Contract checks of the row offsets alone; sets max_degree.
 int validate_rowptr(mc_dgraph *g);
 int tc_partner_stats(mc_dgraph *g, unsigned long long *partner_edges, unsigned long long *work);

@@ -2165,13 +2165,13 @@ int pattern_count_body(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12,
                        double *progress) {
   NvtxRange range("pattern_count");
   if (pattern < 1 || pattern > 8) return MC_ERR_ARG;
-  // P7 on graphs with hubs: by clique counts over the degree-ordered DAG
-  // (cliques.cu), which is built first; its time counts as the pattern's.
+  // P7 and P8 on graphs with hubs: by clique counts over the degree-ordered
+  // DAG (cliques.cu), which is built first; its time counts as the pattern's.
   bool cliques = false;
   int64_t dag_edges = 0;
-  if (pattern == 7) {
+  if (pattern == 7 || pattern == 8) {
     MC_CUDA_TRY(cudaEventRecord(g->ev[0], g->stream));
-    const int rc = p7_clique_prepare(g, &cliques, &dag_edges);
+    const int rc = clique_prepare(g, pattern, &cliques, &dag_edges);
     if (rc != MC_OK) return rc;
   }
   // MERCURY_PATTERN_SLICE=1/0 forces slicing on/off (the tests compare both);
@@ -2217,7 +2217,7 @@ int pattern_count_body(mc_dgraph *g, int pattern, uint64_t *out, uint64_t *c12,
   if (!cliques) MC_CUDA_TRY(cudaEventRecord(g->ev[0], s));
   int rc = MC_OK;
   if (cliques) {
-    rc = p7_clique_launch(g, dag_edges, shard, num_shards, a.deadline, a.stop_flag);
+    rc = clique_launch(g, pattern, dag_edges, shard, num_shards, a.deadline, a.stop_flag);
   } else if (g->n > 0 && g->nnz > 0) {
     // MERCURY_PATTERN_KERNEL=edge / =centers forces one route for every
     // pattern (the tests run all three settings; timing comparisons use it).

@@ -1,9 +1,11 @@
 // ORACLE -- test infrastructure, not product code.
 //
-// A second CPU restatement of the reference's P7 formula
-// (subgraph_matching/pattern_kernels.cuh:352-459, combined as in
-// subgraph_matching/sm_multigpu.cu:206-232), for graphs whose hubs make the
-// literal restatement in patterns_oracle.cpp take days.  Per directed edge
+// A second CPU restatement of the reference's P7 and P8 formulas
+// (subgraph_matching/pattern_kernels.cuh:352-459 and :461-572, combined as
+// in subgraph_matching/sm_multigpu.cu:206-232), for graphs whose hubs make
+// the literal restatement in patterns_oracle.cpp take days.
+//
+// P7.  Per directed edge
 // (v0, v1) the formula counts the triples of A = N(v0) & N(v1) that are
 // pairwise non-adjacent, I3(A) (its frequency term less its correction).
 // By inclusion-exclusion over the edges inside A,
@@ -15,13 +17,27 @@
 // for its three edges and each K5 holds ten edges, so over the graph
 //   P7 = 2 [ sum_e C(a_e, 3) - sum_e k4_e (a_e - 2)
 //            + 3 sum_tau C(k4_tau, 2) - 10 K5 ].
+//
+// P8.  The formula counts, per directed edge (v0, v1), the pairs of
+// adjacent x < v2 in A with a v4 in N(v1) - N(v0) adjacent to neither: a K4
+// {v0, v1, v2, x} with a vertex hung on v1 alone, an induced tailed K4, once
+// for each of the three other K4 vertices as v0.  For a K4 Q and q in Q,
+// inclusion-exclusion over N(q) gives the vertices hung on q alone:
+//   d(q) - 3 - sum_p (a_qp - 2) + sum_{p,r} (k_qpr - 1) - k5_Q
+// (p, r the other vertices, a the triangles on an edge, k the K4s on a
+// triangle, k5_Q the K5s on Q).  Summed over q and over every K4 (a
+// triangle lies in k_tau K4s, an edge's K4s are half the k of its
+// triangles, a vertex's a third, a K5 holds five K4s):
+//   P8 = sum_tau k_tau (d_x + d_y + d_z) - 3 sum_tau k_tau (a_e1 + a_e2 + a_e3)
+//        + 9 sum_tau k_tau^2 - 60 K5.
+//
 // The counts come from listing every triangle, K4 and K5 once on the
 // degree-ordered DAG (u -> v iff d(v) > d(u), or equal and v > u).  The
-// reference multiplies two 32-bit ints per term (:411); the identity holds
-// while those products cannot wrap, i.e. for a maximum degree of at most
-// 46,340, and the function refuses larger graphs.  tests/test_oracle.py
-// checks it against the literal restatement on random graphs, the fixtures
-// and a graph with hubs.
+// reference multiplies two 32-bit ints per term (:411, :526); the
+// identities hold while those products cannot wrap, i.e. for a maximum
+// degree of at most 46,340, and the function refuses larger graphs.
+// tests/test_oracle.py checks both against the literal restatement on
+// random graphs, the fixtures and graphs with hubs.
 #include <omp.h>
 
 #include <algorithm>
@@ -40,11 +56,11 @@ inline int64_t index_in(const int32_t *b, const int32_t *e, int32_t v) {
 
 extern "C" {
 
-// Returns 0 and writes P7 (mod 2^64) to *result, or -1 when the maximum
-// degree exceeds 46,340.  terms (optional, 7 doubles): triangles, K4, K5,
-// sum_e C(a_e,3), sum_e k4_e (a_e - 2), 3 sum C(k4_tau,2), 10 K5.
-int orc_p7_cliques(int64_t n, const int64_t *rp, const int32_t *ci, uint64_t *result,
-                   double *terms) {
+// Returns 0 and writes P7 and P8 (mod 2^64) to result[0..1], or -1 when the
+// maximum degree exceeds 46,340.  terms (optional, 7 doubles): triangles,
+// K4, K5, sum_e C(a_e,3), sum_e k4_e (a_e - 2), 3 sum C(k4_tau,2), 10 K5.
+int orc_clique_patterns(int64_t n, const int64_t *rp, const int32_t *ci, uint64_t *result,
+                        double *terms) {
   for (int64_t v = 0; v < n; ++v)
     if (rp[v + 1] - rp[v] > 46340) return -1;
   auto keep = [&](int64_t u, int32_t v) {
@@ -150,9 +166,39 @@ int orc_p7_cliques(int64_t n, const int64_t *rp, const int32_t *ci, uint64_t *re
     if (k >= 2) s3 += 3 * (k * (k - 1) / 2);
   }
   const u128 s4 = 10 * (u128)(uint64_t)k5_total;
-  // The true value is non-negative; the reference's u64 result is it mod 2^64.
+  // The true values are non-negative; the reference's u64 result is each
+  // modulo 2^64.
   const u128 p7 = 2 * (s1 + s3 - s2 - s4);
-  *result = (uint64_t)p7;
+  // P8's triangle terms: k (d_x + d_y + d_z), 3 k (a_e1 + a_e2 + a_e3), 9 k^2.
+  u128 t_deg = 0, t_a = 0, t_k2 = 0;
+#pragma omp parallel
+  {
+    u128 dg = 0, ta = 0, k2 = 0;
+#pragma omp for schedule(dynamic, 256)
+    for (int64_t u = 0; u < n; ++u)
+      for (int64_t i = drp[u]; i < drp[u + 1]; ++i) {
+        const int32_t v = dcol[i];
+        for (int64_t j = toff[i]; j < toff[i + 1]; ++j) {
+          const int32_t w = tcol[j];
+          const u128 k = (u128)k4t[j];
+          if (k == 0) continue;
+          const u128 d = (u128)((rp[u + 1] - rp[u]) + (rp[v + 1] - rp[v]) + (rp[w + 1] - rp[w]));
+          const u128 s = (u128)(a[i] + a[eid(u, w)] + a[eid(v, w)]);
+          dg += k * d;
+          ta += k * s;
+          k2 += k * k;
+        }
+      }
+#pragma omp critical
+    {
+      t_deg += dg;
+      t_a += ta;
+      t_k2 += k2;
+    }
+  }
+  const u128 p8 = t_deg + 9 * t_k2 - 3 * t_a - 60 * (u128)(uint64_t)k5_total;
+  result[0] = (uint64_t)p7;
+  result[1] = (uint64_t)p8;
   if (terms) {
     const double v[] = {(double)ntri, k4_total, k5_total, (double)s1, (double)s2, (double)s3,
                         (double)s4};

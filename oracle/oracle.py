@@ -49,8 +49,8 @@ def lib() -> C.CDLL:
         L.orc_tc_by_label.restype = None
         L.orc_pattern_fast.argtypes = [C.c_int64, P, P, C.c_int, P]
         L.orc_pattern_fast.restype = C.c_uint64
-        L.orc_p7_cliques.argtypes = [C.c_int64, P, P, P, P]
-        L.orc_p7_cliques.restype = C.c_int
+        L.orc_clique_patterns.argtypes = [C.c_int64, P, P, P, P]
+        L.orc_clique_patterns.restype = C.c_int
         L.orc_csr_build.argtypes = [C.c_int64, C.c_int64, P, P, P, P]
         L.orc_csr_build.restype = C.c_int64
         L.orc_rmat_draws.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
@@ -176,22 +176,23 @@ def pattern_fast(rowptr, col, k: int, return_counters: bool = False):
     return r
 
 
-def p7_cliques(rowptr, col, return_terms: bool = False):
-    """P7 from its clique restatement (p7_cliques.cpp: inclusion-exclusion of
-    I3(N(v0) & N(v1)) over triangle, K4 and K5 counts), for graphs whose hubs
-    make pattern() take days; None when the maximum degree exceeds 46,340
-    (the reference's 32-bit products could wrap there)."""
+def clique_patterns(rowptr, col, return_terms: bool = False):
+    """{7: P7, 8: P8} from their clique restatement (clique_patterns.cpp:
+    inclusion-exclusion over triangle, K4 and K5 counts), for graphs whose
+    hubs make pattern() take days; None when the maximum degree exceeds
+    46,340 (the reference's 32-bit products could wrap there)."""
     rowptr, col = _csr(rowptr, col)
-    out = np.zeros(1, dtype=np.uint64)
+    out = np.zeros(2, dtype=np.uint64)
     terms = np.zeros(7)
-    rc = lib().orc_p7_cliques(len(rowptr) - 1, rowptr.ctypes.data, col.ctypes.data,
-                              out.ctypes.data, terms.ctypes.data)
+    rc = lib().orc_clique_patterns(len(rowptr) - 1, rowptr.ctypes.data, col.ctypes.data,
+                                   out.ctypes.data, terms.ctypes.data)
     if rc != 0:
         return None
+    counts = {7: int(out[0]), 8: int(out[1])}
     if return_terms:
         keys = ("triangles", "k4", "k5", "sum_c_a3", "sum_k4e_a2", "sum_3_c_k4t2", "ten_k5")
-        return int(out[0]), {k: float(v) for k, v in zip(keys, terms)}
-    return int(out[0])
+        return counts, {k: float(v) for k, v in zip(keys, terms)}
+    return counts
 
 
 def csr_from_edges(src, dst, n: int):

@@ -11,13 +11,13 @@ counts against it.
   python tests/golden/make_pattern_golden.py [--n 100000 --mean 10 --cap 200]
 
 With --fast, P1 and P4 come from the second restatement
-(oracle/patterns_fast.cpp) and P7 from its clique restatement
-(oracle/p7_cliques.cpp), both pinned to the literal one by
+(oracle/patterns_fast.cpp) and P7 and P8 from their clique restatement
+(oracle/clique_patterns.cpp), both pinned to the literal one by
 tests/test_oracle.py, which count graphs with hubs in minutes; the Chung-Lu
 graph with n 1,000,000, mean 20 and cap 50,000 is counted that way:
 
   python tests/golden/make_pattern_golden.py --n 1000000 --mean 20 --cap 50000 \
-      --patterns 1,4,7 --fast
+      --patterns 1,4,7,8 --fast
 
 The same shape at 5,000 vertices (hubs of degree 2,187, 1,525 and 1,173)
 is small enough for the literal restatement, all eight patterns (P3, whose
@@ -49,13 +49,13 @@ def main():
     ap.add_argument("--cap", type=float, default=200.0)
     ap.add_argument("--patterns", default="1,2,3,4,5,6,7,8")
     ap.add_argument("--fast", action="store_true",
-                    help="P1/P4 by patterns_fast.cpp, P7 by p7_cliques.cpp")
+                    help="P1/P4 by patterns_fast.cpp, P7/P8 by clique_patterns.cpp")
     a = ap.parse_args()
     rp, col = orc.chung_lu(a.n, 2.1, a.mean, a.cap, seed=1)
     rec = json.load(open(OUT)) if os.path.exists(OUT) else {}
     entry = rec.setdefault(key(a.n, a.mean, a.cap), {})
     entry.update({"n": a.n, "m": int(len(col) // 2), "max_degree": int((rp[1:] - rp[:-1]).max()),
-                  "source": ("oracle/patterns_fast.cpp (P1, P4) and oracle/p7_cliques.cpp (P7)"
+                  "source": ("oracle/patterns_fast.cpp (P1, P4) and oracle/clique_patterns.cpp (P7, P8)"
                              if a.fast else "oracle/patterns_oracle.cpp") +
                             " on the oracle's generator restatement"})
     counts = entry.setdefault("counts", {})
@@ -64,8 +64,8 @@ def main():
         t0 = time.time()
         if not a.fast:
             counts[f"P{k}"] = orc.pattern(rp, col, k)
-        elif k == 7:
-            counts[f"P{k}"] = orc.p7_cliques(rp, col)
+        elif k in (7, 8):
+            counts[f"P{k}"] = orc.clique_patterns(rp, col)[k]
         else:
             counts[f"P{k}"] = orc.pattern_fast(rp, col, k)
         seconds[f"P{k}"] = round(time.time() - t0, 1)

@@ -125,32 +125,43 @@ def test_fast_p1_p4_restatement_on_fixtures_and_hubs():
 
 
 @pytest.mark.parametrize("seed", range(6))
-def test_p7_clique_restatement_equals_literal_oracle(seed):
-    """p7_cliques.cpp counts P7 as inclusion-exclusion over triangle, K4 and
-    K5 counts; it equals the literal restatement on random graphs of rising
-    density."""
+def test_clique_restatement_equals_literal_oracle(seed):
+    """clique_patterns.cpp counts P7 and P8 as inclusion-exclusion over
+    triangle, K4 and K5 counts; both equal the literal restatement on random
+    graphs of rising density."""
     n = 20 + 12 * seed
     rp, col = csr_from_edges(n, random_graph(n, 0.12 + 0.08 * seed, 400 + seed))
-    assert orc.p7_cliques(rp, col) == orc.pattern(rp, col, 7)
+    c = orc.clique_patterns(rp, col)
+    assert c[7] == orc.pattern(rp, col, 7) and c[8] == orc.pattern(rp, col, 8)
 
 
-def test_p7_clique_restatement_on_fixtures_and_hubs():
-    """The golden fixtures, and the Chung-Lu graph with hubs of degree 2,187,
-    1,525 and 1,173 whose P7 the literal oracle committed."""
+def test_clique_restatement_on_fixtures_and_hubs():
+    """The golden fixtures, the Chung-Lu graph with hubs of degree 2,187,
+    1,525 and 1,173 and the graph with a vertex of degree 20,000, whose P7 and
+    P8 the literal oracle committed."""
     named = [name for name in sorted(GOLD) if "P7" in GOLD[name]]
     assert len(named) >= 5
     for name in named:
         rp, col = load_fixture(name)
-        assert orc.p7_cliques(rp, col) == GOLD[name]["P7"], name
+        c = orc.clique_patterns(rp, col)
+        assert (c[7], c[8]) == (GOLD[name]["P7"], GOLD[name]["P8"]), name
     with open(os.path.join(GOLDEN, "pattern_counts.json")) as f:
         rec = json.load(f)["chung_lu_n5000_mean20_cap50000_seed1"]
     rp, col = orc.chung_lu(5000, 2.1, 20.0, 50000.0, seed=1)
-    assert orc.p7_cliques(rp, col) == rec["counts"]["P7"]
+    c = orc.clique_patterns(rp, col)
+    assert (c[7], c[8]) == (rec["counts"]["P7"], rec["counts"]["P8"])
+    import sys
+    sys.path.insert(0, GOLDEN)
+    from make_hub_golden import hub_graph
+    with open(os.path.join(GOLDEN, "hub_counts.json")) as f:
+        hub = json.load(f)["counts"]
+    c = orc.clique_patterns(*hub_graph())
+    assert (c[7], c[8]) == (hub["P7"], hub["P8"])
 
 
-def test_p7_clique_restatement_refuses_degrees_where_products_wrap():
+def test_clique_restatement_refuses_degrees_where_products_wrap():
     """Above degree 46,340 the reference's 32-bit products can wrap and the
     identity no longer holds: the restatement refuses (None)."""
     n = 46342
     rp, col = csr_from_edges(n, [(0, v) for v in range(1, n)])
-    assert orc.p7_cliques(rp, col) is None
+    assert orc.clique_patterns(rp, col) is None

@@ -308,49 +308,54 @@ def test_p1_large_centers_by_bitmap_tasks(monkeypatch, hub, lane_scan):
         assert sum(d.pattern_count_shard(1, s, 3) for s in range(3)) % (1 << 64) == want
 
 
-P7_FIXTURES = sorted(k for k in GOLD if "P7" in GOLD[k])
+CLIQUE_FIXTURES = sorted(k for k in GOLD if "P7" in GOLD[k] and "P8" in GOLD[k])
 
 
-def test_p7_clique_route_on_fixtures_and_random_graphs(monkeypatch):
-    """MERCURY_P7_ROUTE=cliques: P7 from triangle, K4 and K5 counts listed on
-    the degree-ordered DAG (inclusion-exclusion of I3(N(v0) & N(v1))) equals
-    the golden counts, the oracle on random graphs of rising density, and the
-    sum of its shards (mod 2^64)."""
-    monkeypatch.setenv("MERCURY_P7_ROUTE", "cliques")
-    for name in P7_FIXTURES:
+def test_clique_route_on_fixtures_and_random_graphs(monkeypatch):
+    """MERCURY_CLIQUE_ROUTE=cliques: P7 and P8 from triangle, K4 and K5 counts
+    listed on the degree-ordered DAG (inclusion-exclusion of the formulas'
+    per-edge sets) equal the golden counts, the oracle on random graphs of
+    rising density, and the sum of their shards (mod 2^64)."""
+    monkeypatch.setenv("MERCURY_CLIQUE_ROUTE", "cliques")
+    for name in CLIQUE_FIXTURES:
         g = Graph(os.path.join(GOLDEN, "graphs", name, "graph"))
         with DeviceGraph(g) as d:
-            assert d.pattern_count(7) == GOLD[name]["P7"], name
-            parts = [d.pattern_count_shard(7, s, 3) for s in range(3)]
-            assert sum(parts) % (1 << 64) == GOLD[name]["P7"], name
+            for k in (7, 8):
+                assert d.pattern_count(k) == GOLD[name][f"P{k}"], (name, k)
+                parts = [d.pattern_count_shard(k, s, 3) for s in range(3)]
+                assert sum(parts) % (1 << 64) == GOLD[name][f"P{k}"], (name, k)
     for seed in range(4):
         n = 30 + 20 * seed
         rp, col = csr_from_edges(n, random_graph(n, 0.2 + 0.1 * seed, 700 + seed))
         with DeviceGraph(rp, col) as d:
-            assert d.pattern_count(7) == orc.pattern(rp, col, 7), seed
+            for k in (7, 8):
+                assert d.pattern_count(k) == orc.pattern(rp, col, k), (seed, k)
 
 
-def test_p7_clique_route_on_graphs_with_hubs(monkeypatch):
-    """The route P7 takes by itself on graphs with a vertex above degree
-    4,096 (the graph with one vertex of degree 20,000), and forced on the
-    Chung-Lu graph with hubs of degree 2,187, 1,525 and 1,173: both equal
+def test_clique_route_on_graphs_with_hubs(monkeypatch):
+    """The route P7 and P8 take by themselves on graphs with a vertex above
+    degree 4,096 (the graph with one vertex of degree 20,000), and forced on
+    the Chung-Lu graph with hubs of degree 2,187, 1,525 and 1,173: both equal
     the counts the literal oracle committed, and the formula route agrees."""
     sys.path.insert(0, GOLDEN)
     from make_hub_golden import hub_graph
     with open(os.path.join(GOLDEN, "hub_counts.json")) as f:
-        hub_want = json.load(f)["counts"]["P7"]
+        hub_want = json.load(f)["counts"]
     rp, col = hub_graph()
     with DeviceGraph(rp, col) as d:
-        assert d.pattern_count(7) == hub_want
-        assert sum(d.pattern_count_shard(7, s, 2) for s in range(2)) % (1 << 64) == hub_want
-    monkeypatch.setenv("MERCURY_P7_ROUTE", "formula")
+        for k in (7, 8):
+            assert d.pattern_count(k) == hub_want[f"P{k}"], k
+            parts = [d.pattern_count_shard(k, s, 2) for s in range(2)]
+            assert sum(parts) % (1 << 64) == hub_want[f"P{k}"], k
+    monkeypatch.setenv("MERCURY_CLIQUE_ROUTE", "formula")
     with DeviceGraph(rp, col) as d:
-        assert d.pattern_count(7) == hub_want
+        assert d.pattern_count(7) == hub_want["P7"]
     with open(os.path.join(GOLDEN, "pattern_counts.json")) as f:
-        want = json.load(f)["chung_lu_n5000_mean20_cap50000_seed1"]["counts"]["P7"]
-    monkeypatch.setenv("MERCURY_P7_ROUTE", "cliques")
+        want = json.load(f)["chung_lu_n5000_mean20_cap50000_seed1"]["counts"]
+    monkeypatch.setenv("MERCURY_CLIQUE_ROUTE", "cliques")
     g = Graph.chung_lu(5000, 2.1, 20.0, 50000.0, seed=1)
     with DeviceGraph(g) as d:
-        assert d.pattern_count(7) == want
-        count, frac = d.pattern_count_budget(7, 60000.0)
-        assert count == want and frac == 1.0
+        for k in (7, 8):
+            assert d.pattern_count(k) == want[f"P{k}"], k
+            count, frac = d.pattern_count_budget(k, 60000.0)
+            assert count == want[f"P{k}"] and frac == 1.0
