@@ -253,8 +253,8 @@ int resident(const void *kernel, int threads) {
 // MERCURY_CLIQUE_ROUTE=cliques sends P7 and P8 here whenever the graph
 // allows it, =formula never; unset, they take this route on graphs with a
 // vertex of degree above 4,096 (where the formulas' per-edge loops do not
-// finish), unless MERCURY_PATTERN_KERNEL forces a formula route.  The degree-ordered
-// DAG is built (or reused) here; *use is false when the graph does not
+// finish), unless MERCURY_PATTERN_KERNEL forces a formula route.  The
+// degree-ordered DAG is built here; *use is false when the graph does not
 // allow the route (a degree above 46,340, where the reference's products
 // wrap, or a DAG out-list longer than kCliqueMaxOut).
 int clique_prepare(mc_dgraph *g, int pattern, bool *use, int64_t *dag_edges) {
