@@ -136,3 +136,45 @@ def test_restated_forms_equal_the_oracle(n, p, seed, k):
     rp, col = np.asarray(rp), np.asarray(col)
     N = neighbourhoods(rp, col)
     assert FORMS[k](N, list(directed_edges(rp, col))) == orc.pattern(rp, col, k)
+
+
+def clique_form(rp, col, k):
+    """P7 or P8 as the clique route of mercury_b200/csrc/cliques.cu computes
+    them, restated literally: triangles listed once on the degree-ordered DAG
+    (u -> v -> w), a_e = |N(x) & N(y)| per edge, k_tau = |N(u) & N(v) & N(w)|
+    per triangle, and the K5s (u, v, w, x, y) with x, y in N+(u) & N+(v) &
+    N+(w) and y in N+(x); every term added modulo 2^64."""
+    N = neighbourhoods(rp, col)
+    n = len(N)
+    deg = [len(s) for s in N]
+    out = [{w for w in N[u] if deg[w] > deg[u] or (deg[w] == deg[u] and w > u)}
+           for u in range(n)]
+    a = {}
+    for u in range(n):
+        for v in out[u]:
+            a[frozenset((u, v))] = len(N[u] & N[v])
+    acc = 0
+    if k == 7:
+        acc += sum(2 * (t * (t - 1) * (t - 2) // 6) for t in a.values())
+    for u in range(n):
+        for v in out[u]:
+            for w in out[u] & out[v]:
+                kt = len(N[u] & N[v] & N[w])
+                sum_a = a[frozenset((u, v))] + a[frozenset((u, w))] + a[frozenset((v, w))]
+                S = out[u] & out[v] & out[w]
+                k5 = sum(len(S & out[x]) for x in S)
+                if k == 7:
+                    acc += 6 * (kt * (kt - 1) // 2) - kt * (sum_a - 6) - 20 * k5
+                else:
+                    acc += kt * (deg[u] + deg[v] + deg[w]) - 3 * kt * sum_a + 9 * kt * kt - 60 * k5
+    return acc & MASK64
+
+
+@pytest.mark.parametrize("n,p,seed", [(14, 0.5, 31), (22, 0.4, 32), (30, 0.35, 33),
+                                      (40, 0.25, 34)])
+@pytest.mark.parametrize("k", [7, 8])
+def test_clique_route_forms_equal_the_oracle(n, p, seed, k):
+    """The clique route's per-edge and per-triangle terms give the oracle's
+    P7 and P8 on random graphs (the GPU tests check the kernels too)."""
+    rp, col = csr_from_edges(n, random_graph(n, p, seed))
+    assert clique_form(rp, col, k) == orc.pattern(rp, col, k)
